@@ -1,0 +1,396 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 lmp platform on the 3-D Q1 128^3 variable-coefficient system.
+
+One step = one complete mixed-precision solve to a 1e-10 relative residual:
+FP64 outer defect correction (MPIR) around an FP32 Jacobi-CG with tolerance
+1e-4, on the 128^3-cell trilinear Q1 operator with k = exp(GRF), sigma = 1,
+correlation length 0.1 (2,146,689 DoFs, 57,066,625 stored nonzeros).
+`value` is whole-job solves/s with the system resident in HBM; the line also
+carries the plain FP64 Jacobi-CG time to the same tolerance, the speed-up of
+the mixed form over it, the SpMV bandwidth against the measured HBM peak,
+the end-to-end rate through the C ABI with host buffers, and the reference's
+CPU code timed on this host.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--N 128]
+
+For N > 1 (torchrun, one rank per GPU) every rank solves its own replica of
+the system: the path has no data-parallel exchange (replicas only), and the
+time is the maximum over ranks.
+"""
+import argparse
+import datetime
+import importlib.util
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "3D Q1 128³ CG time-to-1e-10: mixed vs FP64; SpMV HBM GB/s; serving p50/p99"
+UNIT = "solves/s"
+
+
+def load_platform():
+    name = "hiflow3_b200"
+    if name in sys.modules:
+        return sys.modules[name]
+    path = os.path.join(ROOT, "hiflow3_2.0_b200", "__init__.py")
+    spec = importlib.util.spec_from_file_location(name, path, submodule_search_locations=[os.path.dirname(path)])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def load_workloads():
+    load_platform()
+    import importlib
+    return importlib.import_module("hiflow3_b200.workloads")
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu):
+        self.gpu, self.rows, self.proc = gpu, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+                for k, nm in enumerate(names):
+                    if r[5 + k].lower().startswith("active"):
+                        reasons.add(nm)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def spmv_bytes(n, nnz, vbytes):
+    """Algorithmic bytes of one SpMV: values + column indices + row pointer,
+    x read once, y written once."""
+    return vbytes * nnz + 4 * nnz + 4 * (n + 1) + 2 * vbytes * n
+
+
+# --------------------------------------------------------------- CPU baseline
+
+def cpu_counts(N):
+    p = os.path.join(ROOT, "tests", "golden", "c3_counts.json" if N == 128 else f"c3_counts_{N}.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return None
+
+
+def cpu_baseline(row, col, val, b, outer, inner_total, fp64_iters):
+    """The reference's own CPU code (oracle/_ref: HiFlow3's CPUopenmp lmp
+    objects driving the restated MPIR and CG loops), timed on a bounded sample
+    and scaled to the full solve's iteration counts."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    threads = len(os.sched_getaffinity(0))
+    if not os.path.exists(pyoracle.REF_SO):
+        return None
+    ref = pyoracle.Ref()
+    s1, s2 = 4, 16
+    a = pyoracle.ref_mpir(ref, row, col, val, b, threads, sample_inner=s1)
+    c = pyoracle.ref_mpir(ref, row, col, val, b, threads, sample_inner=s2)
+    per_inner = max((c["seconds"] - a["seconds"]) / (s2 - s1), 1e-9)
+    per_outer = max(a["seconds"] - s1 * per_inner, 0.0)   # residuals, casts, update of one correction
+    est = outer * per_outer + inner_total * per_inner
+    p = pyoracle.ref_pcg_timed(ref, row, col, val, b, threads, maxits=16)
+    fp64_est = p["seconds"] / max(p["iters"], 1) * fp64_iters
+    return dict(value=1.0 / est, unit=UNIT, cores=threads, kind="reference",
+                sample=(f"reference CPUopenmp lmp MPIR: first correction cut at {s1} and {s2} FP32 inner "
+                        f"iterations (linear fit: {per_inner * 1e3:.1f} ms/inner iteration, "
+                        f"{per_outer * 1e3:.1f} ms/correction overhead) scaled to {outer} corrections and "
+                        f"{inner_total} inner iterations"),
+                est_solve_s=est, fp64_cg_est_s=fp64_est, fp64_cg_sample_iters=p["iters"])
+
+
+def run_reference(args):
+    wl = load_workloads()
+    b200 = load_platform()
+    row, col, val, b, _ = wl.system(b200, "c3", N=args.N)
+    counts = cpu_counts(args.N)
+    if counts is None:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle
+        ref = pyoracle.Ref()
+        m = pyoracle.ref_mpir(ref, row, col, val, b, len(os.sched_getaffinity(0)))
+        counts = dict(mpir_outer=m["outer"], mpir_inner_total=m["inner_total"], fp64_cg_iters=0)
+    ests = []
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(row, col, val, b, counts["mpir_outer"], counts["mpir_inner_total"],
+                          counts["fp64_cg_iters"])
+        if cb is None:
+            return {"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU lmp build) is missing"}
+        if k >= args.warmup:
+            ests.append(cb["est_solve_s"])
+    est = statistics.median(ests)
+    v = 1.0 / est
+    cb["value"] = v
+    return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": est * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic (seeded)", "impl": "reference",
+            "config": {"workload": wl.CONFIGS["c3"]["desc"], "cells": args.N ** 3},
+            "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+# --------------------------------------------------------------- B200 arm
+
+def run_b200(args, rank, world, local_rank, dist):
+    import torch
+    b200 = load_platform()
+    wl = load_workloads()
+    torch.cuda.set_device(local_rank)
+    pf = b200.Platform(local_rank)
+    t0 = time.time()
+    row, col, val, b, _ = wl.system(b200, "c3", N=args.N)
+    t_asm = time.time() - t0
+    n, nnz = len(row) - 1, len(col)
+    t0 = time.time()
+    A64 = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    A32 = A64.CastFrom(b200.F32)
+    pf.sync()
+    t_up = time.time() - t0
+    bv, x = pf.vector(b), pf.vector(n)
+
+    mp = b200.MPIR(pf, max_outer=50)
+    mp.SetupOperator(A64)
+    mp.SetupLowPrecisionOperator(A32)
+    mp.InitControl(50, 0.0, 1e-10, 1e6)
+    mp.InitInnerControl(100000, 0.0, 1e-4, 1e6)
+
+    def step():
+        x.Zeros()
+        mp.Solve(bv, x)
+        return mp.result
+
+    for _ in range(args.warmup):
+        step()
+    if world > 1:
+        dist.barrier()
+    pf.sync()
+    launches = 0
+    with Clocks(local_rank) as clk:
+        pf.timer_start()
+        for _ in range(args.steps):
+            r = step()
+            launches += r.launches
+        ms = pf.timer_stop()
+    res_mixed = dict(outer=r.outer, inner_total=r.iters, res0=r.res0, res=r.res, status=r.status)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_step = ms / args.steps
+    value = world * args.steps / (ms / 1e3)
+    x_mixed = x.numpy()
+
+    # true residual of the mixed solution, in FP64 on the device
+    rv = pf.vector(n)
+    relres = float(np.sqrt(A64.Residual(bv, x, rv)) / np.linalg.norm(b))
+
+    # plain FP64 Jacobi-CG to the same tolerance (the comparison)
+    cg = b200.CG(pf)
+    cg.SetupOperator(A64)
+    J64 = b200.Preconditioner.Jacobi(pf, A64)
+    cg.SetupPreconditioner(J64)
+    cg.InitControl(200000, 0.0, 1e-10, 1e6)
+    x64 = pf.vector(n)
+    cg.Solve(bv, x64)          # warm-up
+    k64 = max(1, min(3, args.steps))
+    pf.sync()
+    pf.timer_start()
+    for _ in range(k64):
+        x64.Zeros()
+        cg.Solve(bv, x64)
+    fp64_ms = pf.timer_stop() / k64
+    fp64_iters = cg.iter()
+    # FP64 reference solution at 1e-12 for the error of the mixed result
+    cg.InitControl(400000, 0.0, 1e-12, 1e6)
+    xr = pf.vector(n)
+    cg.Solve(bv, xr)
+    xr_h = xr.numpy()
+    err = float(np.linalg.norm(x_mixed - xr_h) / np.linalg.norm(xr_h))
+    err64 = float(np.linalg.norm(x64.numpy() - xr_h) / np.linalg.norm(xr_h))
+
+    # SpMV bandwidth: the fused SpMV+dot kernel of the CG iteration, FP64 and
+    # FP32, events on the library's stream around back-to-back launches
+    # (matrix 0.5-0.7 GB, well above L2)
+    def spmv_rate(A, vbytes):
+        dt = b200.F64 if vbytes == 8 else b200.F32
+        xx, yy = pf.vector(np.random.default_rng(1).uniform(-1, 1, n), dt), pf.vector(n, dt)
+        import ctypes
+        d = torch.zeros(1, dtype=torch.float64, device="cuda")
+        L = b200.lib()
+        for _ in range(3):
+            L.b200la_spmv_dot(pf.h, A.h, xx.ptr, yy.ptr, ctypes.c_void_p(d.data_ptr()))
+        reps = 40
+        pf.sync()
+        pf.timer_start()
+        for _ in range(reps):
+            L.b200la_spmv_dot(pf.h, A.h, xx.ptr, yy.ptr, ctypes.c_void_p(d.data_ptr()))
+        t_ms = pf.timer_stop() / reps
+        by = spmv_bytes(n, nnz, vbytes)
+        return by, t_ms, by / (t_ms * 1e-3) / 1e9
+
+    by64, t64, gbs64 = spmv_rate(A64, 8)
+    by32, t32, gbs32 = spmv_rate(A32, 4)
+    peak, peak_kind = measured_peaks()
+
+    # end to end through the C ABI: host b in, host x out, per step
+    import ctypes
+    L = b200.lib()
+    hb = pf.host_alloc(8 * n)
+    hx = pf.host_alloc(8 * n)
+    ctypes.memmove(hb, b.ctypes.data, 8 * n)
+    ctl = b200.Control(50, 0.0, 1e-10, 1e6)
+    ictl = b200.Control(100000, 0.0, 1e-4, 1e6)
+    db, dx = ctypes.c_void_p(), ctypes.c_void_p()
+    pf.check(L.b200la_malloc(pf.h, 8 * n, ctypes.byref(db)))
+    pf.check(L.b200la_malloc(pf.h, 8 * n, ctypes.byref(dx)))
+    res = b200.Result()
+
+    def e2e_step():
+        pf.check(L.b200la_memcpy_h2d(pf.h, db, hb, 8 * n))
+        pf.check(L.b200la_memset_zero(pf.h, dx, 8 * n))
+        pf.check(L.b200la_mpir(pf.h, A64.h, A32.h, db, dx, ctypes.byref(ctl), ctypes.byref(ictl), 50,
+                               ctypes.byref(res)))
+        pf.check(L.b200la_memcpy_d2h(pf.h, hx, dx, 8 * n))
+
+    for _ in range(min(args.warmup, 2)):
+        e2e_step()
+    if world > 1:
+        dist.barrier()
+    pf.sync()
+    pf.timer_start()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_ms = pf.timer_stop()
+    if world > 1:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    xh = np.ctypeslib.as_array(ctypes.cast(hx, ctypes.POINTER(ctypes.c_double)), (n,)).copy()
+    e2e_ok = bool(np.array_equal(xh, x_mixed))
+    L.b200la_free(pf.h, db)
+    L.b200la_free(pf.h, dx)
+    pf.host_free(hb)
+    pf.host_free(hx)
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic (seeded GRF coefficient and RHS)",
+        "config": {"workload": wl.CONFIGS["c3"]["desc"], "cells": args.N ** 3, "dofs": n, "nnz": nnz,
+                   "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
+                   "l2": "inputs larger than L2 (matrix 0.46-0.69 GB)"},
+        "mixed": {"ms": ms_step, "outer": res_mixed["outer"], "inner_iters": res_mixed["inner_total"],
+                  "relres_true": relres, "err_vs_fp64_solution": err},
+        "fp64_cg": {"ms": fp64_ms, "iters": fp64_iters, "err_vs_fp64_solution": err64},
+        "mixed_speedup_vs_fp64": fp64_ms / ms_step,
+        "spmv": {"fp64_gbs": gbs64, "fp64_us": t64 * 1e3, "fp64_bytes": by64,
+                 "fp32_gbs": gbs32, "fp32_us": t32 * 1e3, "fp32_bytes": by32,
+                 "fp64_frac_of_peak": gbs64 / peak},
+        "roofline": {"bound": "hbm", "kernel": "spmv_tile_kernel<float, EPI_DOT_X> (FP32 SpMV + p.Ap of the inner CG)",
+                     "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,
+                     "peak_source": peak_kind, "traffic": None},
+        "gpu_launches": launches,
+        "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * n,
+                "d2h_bytes_per_step": 8 * n, "matches_device_run": e2e_ok},
+        "setup_s": {"assembly": t_asm, "upload_and_cast": t_up},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(row, col, val, b, res_mixed["outer"], res_mixed["inner_total"], fp64_iters)
+        line["cpu_baseline"] = cb if cb else {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                              "sample": "oracle/_ref missing"}
+    pf.close()
+    return line
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--N", type=int, default=128)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        backend = "gloo" if args.impl == "reference" else "nccl"
+        if backend == "nccl":
+            import torch
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    try:
+        if args.impl == "reference":
+            if rank == 0:
+                print(json.dumps(run_reference(args)), flush=True)
+        else:
+            line = run_b200(args, rank, world, local_rank, dist)
+            if rank == 0:
+                print(json.dumps(line), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

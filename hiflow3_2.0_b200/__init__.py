@@ -1,0 +1,633 @@
+"""B200 lmp platform for HiFlow3 -- Python mirror of the reference's operator API.
+
+The product is ``libb200la.so`` (this directory), a C-ABI library of
+hand-written sm_100a kernels and their host orchestration; this module binds it
+with ctypes so tests and benchmarks read like the reference's own
+(``test/LinearAlgebra/cg.cc``, ``gmres.cc``): ``CSR_lMatrix.VectorMult``,
+``lVector.Dot / Axpy / ScaleAdd``, ``CG.SetupOperator / InitControl / Solve``.
+Device memory is owned by PyTorch CUDA tensors (plumbing only); every
+arithmetic operation runs in the library's kernels.  There is no CPU fallback:
+constructing a ``Platform`` without a B200 raises.
+
+The directory name is not a Python identifier; load it with
+``importlib.util.spec_from_file_location``.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libb200la.so")
+
+F64, F32 = 0, 1
+PRECOND_JACOBI, PRECOND_MCSGS, PRECOND_ILU0_LS, PRECOND_ILU0_MC = 1, 2, 3, 4
+ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS = range(5)
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "allocation failed",
+          4: "no usable sm_100 device", 5: "malformed CSR", 6: "refused by memory budget",
+          7: "bounded device wait gave up", 8: "preconditioner setup failed", 9: "unknown request"}
+
+
+class B200Error(RuntimeError):
+    def __init__(self, code, msg=""):
+        self.code = code
+        super().__init__(f"b200la error {code} ({STATUS.get(code, '?')}){': ' + msg if msg else ''}")
+
+
+class Control(C.Structure):
+    """IterateControl (src/common/iterate_control.h)."""
+    _fields_ = [("maxits", C.c_int), ("abstol", C.c_double), ("reltol", C.c_double), ("divtol", C.c_double)]
+
+
+class Result(C.Structure):
+    _fields_ = [("iters", C.c_int), ("status", C.c_int), ("res0", C.c_double), ("res", C.c_double),
+                ("outer", C.c_int), ("launches", C.c_int), ("solve_ms", C.c_double)]
+
+
+def build(force=False):
+    """Compile libb200la.so in place (nvcc, sm_100a)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-C", HERE, "-j8"], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+_P = C.c_void_p
+_I = C.c_int
+_D = C.c_double
+
+
+def lib():
+    """Load libb200la.so, declaring every entry point of include/b200la.h."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `make -C {HERE}` (no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    sig = {
+        "b200la_create": ([_I, C.POINTER(_P)], _I),
+        "b200la_destroy": ([_P], _I),
+        "b200la_set_stream": ([_P, _P], _I),
+        "b200la_get_stream": ([_P], _P),
+        "b200la_sync": ([_P], _I),
+        "b200la_last_error": ([_P], C.c_char_p),
+        "b200la_status_string": ([_I], C.c_char_p),
+        "b200la_num_sms": ([_P], _I),
+        "b200la_malloc": ([_P, C.c_size_t, C.POINTER(_P)], _I),
+        "b200la_free": ([_P, _P], _I),
+        "b200la_memcpy_h2d": ([_P, _P, _P, C.c_size_t], _I),
+        "b200la_memcpy_d2h": ([_P, _P, _P, C.c_size_t], _I),
+        "b200la_memcpy_d2d": ([_P, _P, _P, C.c_size_t], _I),
+        "b200la_memset_zero": ([_P, _P, C.c_size_t], _I),
+        "b200la_host_alloc": ([_P, C.c_size_t, C.POINTER(_P)], _I),
+        "b200la_host_free": ([_P, _P], _I),
+        "b200la_timer_start": ([_P], _I),
+        "b200la_timer_stop": ([_P, C.POINTER(_D)], _I),
+        "b200la_csr_create": ([_P, _I, _I, _I, _P, _P, _P, _I, C.POINTER(_P)], _I),
+        "b200la_csr_create_segmented": ([_P, _I, _I, _I, _P, _P, _P, _I, _I, _P, C.POINTER(_P)], _I),
+        "b200la_csr_destroy": ([_P], _I),
+        "b200la_csr_cast": ([_P, _P, _I, C.POINTER(_P)], _I),
+        "b200la_csr_info": ([_P] + [C.POINTER(_I)] * 7, _I),
+        "b200la_csr_download": ([_P, _P, _P, _P, _P], _I),
+        "b200la_csr_format": ([_P, C.POINTER(_I), C.POINTER(_I)], _I),
+        "b200la_csr_set_values": ([_P, _P, _P], _I),
+        "b200la_csr_invdiag": ([_P, _P, _P], _I),
+        "b200la_spmv": ([_P, _P, _P, _P], _I),
+        "b200la_spmv_add": ([_P, _P, _P, _P], _I),
+        "b200la_spmv_dot": ([_P, _P, _P, _P, _P], _I),
+        "b200la_residual": ([_P, _P, _P, _P, _P, _P], _I),
+        "b200la_dot": ([_P, _I, _I, _P, _P, C.POINTER(_D)], _I),
+        "b200la_nrm2": ([_P, _I, _I, _P, C.POINTER(_D)], _I),
+        "b200la_dot_dev": ([_P, _I, _I, _P, _P, _P], _I),
+        "b200la_axpy": ([_P, _I, _I, _D, _P, _P], _I),
+        "b200la_scaleadd": ([_P, _I, _I, _D, _P, _P], _I),
+        "b200la_scale": ([_P, _I, _I, _D, _P], _I),
+        "b200la_ewmul": ([_P, _I, _I, _P, _P], _I),
+        "b200la_cast": ([_P, _I, _P, _I, _P, _I], _I),
+        "b200la_gather": ([_P, _I, _I, _P, _P, _P], _I),
+        "b200la_scatter": ([_P, _I, _I, _P, _P, _P], _I),
+        "b200la_permute": ([_P, _I, _I, _P, _P, _P], _I),
+        "b200la_coo_to_csr": ([_I, _I, _P, _P, _P, _P, _P, _P], _I),
+        "b200la_add_values": ([_P, _P, _P, _P, _I, _P, _I, _P], _I),
+        "b200la_zero_rows": ([_P, _P, _P, _P, _I, _D], _I),
+        "b200la_multicoloring": ([_I, _P, _P, C.POINTER(_I), _P, _P], _I),
+        "b200la_levelscheduling": ([_I, _P, _P, C.POINTER(_I), _P, _P], _I),
+        "b200la_reorder_csr": ([_I, _P, _P, _P, _P, _P, _P, _P], _I),
+        "b200la_ilu0": ([_I, _P, _P, _P], _I),
+        "b200la_q1_sizes": ([_I, _I, C.POINTER(_I), C.POINTER(C.c_int64)], _I),
+        "b200la_q1_assemble": ([_I, _I, _I, _P, _D, _P, _P, _P, _P], _I),
+        "b200la_q1_rhs": ([C.c_uint64, _I, _I, _P], _I),
+        "b200la_precond_jacobi": ([_P, _P, C.POINTER(_P)], _I),
+        "b200la_precond_mcsgs": ([_P, _I, _P, _P, _P, _D, _I, C.POINTER(_P), C.POINTER(_P)], _I),
+        "b200la_precond_ilu0": ([_P, _I, _P, _P, _P, _I, _I, C.POINTER(_P), C.POINTER(_P)], _I),
+        "b200la_precond_info": ([_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), _P, _P], _I),
+        "b200la_precond_apply": ([_P, _P, _P, _P], _I),
+        "b200la_precond_destroy": ([_P], _I),
+        "b200la_cg": ([_P, _P, _P, _P, _P, C.POINTER(Control), C.POINTER(Result)], _I),
+        "b200la_cg_hist": ([_P, _P, _P, _P, _P, C.POINTER(Control), C.POINTER(Result), _P, _I], _I),
+        "b200la_gmres": ([_P, _P, _P, _I, _P, _P, C.POINTER(Control), C.POINTER(Result)], _I),
+        "b200la_mpir": ([_P, _P, _P, _P, _P, C.POINTER(Control), C.POINTER(Control), _I, C.POINTER(Result)], _I),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    """Names of the entry points declared in include/b200la.h."""
+    import re
+    hdr = open(os.path.join(HERE, "..", "include", "b200la.h")).read()
+    decl = r"^\s*(?:int|void|const char)\s*\*?\s*(b200la_[a-z0-9_]+)\s*\("
+    return sorted(set(re.findall(decl, hdr, flags=re.M)))
+
+
+def _np_ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+# ----------------------------------------------------------------- host setup
+# The one-time host algorithms of the platform (results identical to the
+# reference's: CSR assembly, colouring, level scheduling, ILU(0)).
+
+def _check(rc, what=""):
+    if rc != 0:
+        raise B200Error(rc, what)
+
+
+def q1_sizes(dim, N):
+    n, nnz = C.c_int(), C.c_int64()
+    _check(lib().b200la_q1_sizes(dim, N, C.byref(n), C.byref(nnz)), "q1_sizes")
+    return n.value, nnz.value
+
+
+def q1_assemble(dim, N, kind=0, kcell=None, nu=1.0, beta=(0.0, 0.0, 0.0)):
+    n, nnz = q1_sizes(dim, N)
+    row, col, val = np.empty(n + 1, np.int32), np.empty(nnz, np.int32), np.empty(nnz)
+    kc = _f64(kcell) if kcell is not None else None
+    b3 = _f64(list(beta) + [0.0] * (3 - len(beta)))
+    _check(lib().b200la_q1_assemble(dim, N, kind, _np_ptr(kc) if kc is not None else None, nu, _np_ptr(b3),
+                                    _np_ptr(row), _np_ptr(col), _np_ptr(val)), "q1_assemble")
+    return row, col, val
+
+
+def q1_rhs(seed, dim, N):
+    n, _ = q1_sizes(dim, N)
+    b = np.empty(n)
+    _check(lib().b200la_q1_rhs(seed, dim, N, _np_ptr(b)), "q1_rhs")
+    return b
+
+
+def coo_to_csr(n, coo_row, coo_col, coo_val=None):
+    coo_row, coo_col = _i32(coo_row), _i32(coo_col)
+    nnz = coo_row.size
+    row, col = np.empty(n + 1, np.int32), np.empty(nnz, np.int32)
+    if coo_val is None:
+        _check(lib().b200la_coo_to_csr(n, nnz, _np_ptr(coo_row), _np_ptr(coo_col), None, _np_ptr(row),
+                                       _np_ptr(col), None), "coo_to_csr")
+        return row, col
+    cv, val = _f64(coo_val), np.empty(nnz)
+    _check(lib().b200la_coo_to_csr(n, nnz, _np_ptr(coo_row), _np_ptr(coo_col), _np_ptr(cv), _np_ptr(row),
+                                   _np_ptr(col), _np_ptr(val)), "coo_to_csr")
+    return row, col, val
+
+
+def add_values(row, col, val, rows, cols, values):
+    row, col, val = _i32(row), _i32(col), _f64(val).copy()
+    rows, cols, values = _i32(rows), _i32(cols), _f64(values)
+    _check(lib().b200la_add_values(_np_ptr(row), _np_ptr(col), _np_ptr(val), _np_ptr(rows), rows.size,
+                                   _np_ptr(cols), cols.size, _np_ptr(values)), "add_values")
+    return val
+
+
+def zero_rows(row, col, val, idx, alpha=1.0):
+    row, col, val, idx = _i32(row), _i32(col), _f64(val).copy(), _i32(idx)
+    _check(lib().b200la_zero_rows(_np_ptr(row), _np_ptr(col), _np_ptr(val), _np_ptr(idx), idx.size, alpha))
+    return val
+
+
+def multicoloring(row, col):
+    row, col = _i32(row), _i32(col)
+    n = row.size - 1
+    nc, sizes, perm = C.c_int(), np.empty(n, np.int32), np.empty(n, np.int32)
+    _check(lib().b200la_multicoloring(n, _np_ptr(row), _np_ptr(col), C.byref(nc), _np_ptr(sizes), _np_ptr(perm)),
+           "multicoloring")
+    return nc.value, sizes[:nc.value].copy(), perm
+
+
+def levelscheduling(row, col):
+    row, col = _i32(row), _i32(col)
+    n = row.size - 1
+    nl, sizes, perm = C.c_int(), np.empty(n, np.int32), np.empty(n, np.int32)
+    _check(lib().b200la_levelscheduling(n, _np_ptr(row), _np_ptr(col), C.byref(nl), _np_ptr(sizes),
+                                        _np_ptr(perm)), "levelscheduling")
+    return nl.value, sizes[:nl.value].copy(), perm
+
+
+def reorder_csr(row, col, val, perm):
+    row, col, val, perm = _i32(row), _i32(col), _f64(val), _i32(perm)
+    n = row.size - 1
+    r2, c2, v2 = np.empty(n + 1, np.int32), np.empty(col.size, np.int32), np.empty(col.size)
+    _check(lib().b200la_reorder_csr(n, _np_ptr(row), _np_ptr(col), _np_ptr(val), _np_ptr(perm), _np_ptr(r2),
+                                    _np_ptr(c2), _np_ptr(v2)), "reorder_csr")
+    return r2, c2, v2
+
+
+def ilu0(row, col, val):
+    row, col, v = _i32(row), _i32(col), _f64(val).copy()
+    _check(lib().b200la_ilu0(row.size - 1, _np_ptr(row), _np_ptr(col), _np_ptr(v)), "ilu0")
+    return v
+
+
+# ----------------------------------------------------------------- device side
+
+def _torch():
+    import torch
+    return torch
+
+
+class Platform:
+    """init_platform for the B200 (src/linear_algebra/lmp/platform_management.cc:135-185)."""
+
+    def __init__(self, device=0):
+        torch = _torch()
+        if not torch.cuda.is_available():
+            raise B200Error(4, "no CUDA device visible (the B200 platform has no CPU fallback)")
+        torch.cuda.set_device(device)
+        torch.cuda.init()
+        self.device = device
+        h = C.c_void_p()
+        _check(lib().b200la_create(device, C.byref(h)), "b200la_create")
+        self.h = h
+
+    def check(self, rc, what=""):
+        if rc != 0:
+            msg = lib().b200la_last_error(self.h).decode()
+            raise B200Error(rc, f"{what}: {msg}" if what else msg)
+
+    def sync(self):
+        self.check(lib().b200la_sync(self.h), "sync")
+
+    def num_sms(self):
+        return lib().b200la_num_sms(self.h)
+
+    def timer_start(self):
+        self.check(lib().b200la_timer_start(self.h), "timer_start")
+
+    def timer_stop(self):
+        ms = C.c_double()
+        self.check(lib().b200la_timer_stop(self.h, C.byref(ms)), "timer_stop")
+        return ms.value
+
+    def host_alloc(self, nbytes):
+        """A page-locked host buffer (returned as a ctypes pointer; free with host_free)."""
+        p = C.c_void_p()
+        self.check(lib().b200la_host_alloc(self.h, nbytes, C.byref(p)), "host_alloc")
+        return p
+
+    def host_free(self, p):
+        self.check(lib().b200la_host_free(self.h, p), "host_free")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().b200la_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # vectors are torch CUDA tensors
+    def vector(self, data_or_n, dtype=F64):
+        torch = _torch()
+        td = torch.float64 if dtype == F64 else torch.float32
+        if isinstance(data_or_n, int):
+            return lVector(self, torch.zeros(data_or_n, dtype=td, device=f"cuda:{self.device}"))
+        a = np.ascontiguousarray(data_or_n, dtype=np.float64 if dtype == F64 else np.float32)
+        return lVector(self, torch.from_numpy(a).to(f"cuda:{self.device}"))
+
+
+def _dt(t):
+    torch = _torch()
+    if t.dtype == torch.float64:
+        return F64
+    if t.dtype == torch.float32:
+        return F32
+    raise TypeError("vectors are float64 or float32")
+
+
+class lVector:
+    """lVector<T> on the B200 (src/linear_algebra/lmp/lvector.h:39-335)."""
+
+    def __init__(self, platform, tensor):
+        self.pf, self.t = platform, tensor
+        self.dtype = _dt(tensor)
+
+    @property
+    def ptr(self):
+        return C.c_void_p(self.t.data_ptr())
+
+    def get_size(self):
+        return self.t.numel()
+
+    def numpy(self):
+        self.pf.sync()
+        return self.t.cpu().numpy()
+
+    def Zeros(self):
+        self.pf.check(lib().b200la_memset_zero(self.pf.h, self.ptr, self.t.numel() * self.t.element_size()))
+
+    def CopyFrom(self, other):
+        self.pf.check(lib().b200la_memcpy_d2d(self.pf.h, self.ptr, other.ptr, self.t.numel() * self.t.element_size()))
+
+    def CloneWithoutContent(self):
+        return lVector(self.pf, _torch().zeros_like(self.t))
+
+    def Dot(self, other):
+        out = C.c_double()
+        self.pf.check(lib().b200la_dot(self.pf.h, self.dtype, self.get_size(), self.ptr, other.ptr, C.byref(out)),
+                      "Dot")
+        return out.value
+
+    def Norm2(self):
+        out = C.c_double()
+        self.pf.check(lib().b200la_nrm2(self.pf.h, self.dtype, self.get_size(), self.ptr, C.byref(out)), "Norm2")
+        return out.value
+
+    def Axpy(self, vec, scalar):
+        self.pf.check(lib().b200la_axpy(self.pf.h, self.dtype, self.get_size(), scalar, vec.ptr, self.ptr), "Axpy")
+
+    def ScaleAdd(self, scalar, vec):
+        self.pf.check(lib().b200la_scaleadd(self.pf.h, self.dtype, self.get_size(), scalar, vec.ptr, self.ptr),
+                      "ScaleAdd")
+
+    def Scale(self, scalar):
+        self.pf.check(lib().b200la_scale(self.pf.h, self.dtype, self.get_size(), scalar, self.ptr), "Scale")
+
+    def ElementWiseMult(self, vec):
+        self.pf.check(lib().b200la_ewmul(self.pf.h, self.dtype, self.get_size(), vec.ptr, self.ptr),
+                      "ElementWiseMult")
+
+    def CastFrom(self, vec):
+        self.pf.check(lib().b200la_cast(self.pf.h, vec.dtype, vec.ptr, self.dtype, self.ptr, self.get_size()),
+                      "CastFrom")
+
+    def GetIndexedValues(self, idx):
+        torch = _torch()
+        idx_t = torch.as_tensor(_i32(idx), device=self.t.device)
+        out = torch.empty(idx_t.numel(), dtype=self.t.dtype, device=self.t.device)
+        self.pf.check(lib().b200la_gather(self.pf.h, self.dtype, idx_t.numel(), C.c_void_p(idx_t.data_ptr()),
+                                          self.ptr, C.c_void_p(out.data_ptr())), "GetIndexedValues")
+        self.pf.sync()
+        return out.cpu().numpy()
+
+    def SetIndexedValues(self, idx, values):
+        torch = _torch()
+        idx_t = torch.as_tensor(_i32(idx), device=self.t.device)
+        v = torch.as_tensor(np.asarray(values), dtype=self.t.dtype, device=self.t.device)
+        self.pf.check(lib().b200la_scatter(self.pf.h, self.dtype, idx_t.numel(), C.c_void_p(idx_t.data_ptr()),
+                                           C.c_void_p(v.data_ptr()), self.ptr), "SetIndexedValues")
+        self.pf.sync()
+
+    def Reorder(self, perm):
+        """out[i] = in[perm[i]] (CPU_lVector::Reorder, lvector_cpu.cc:75-94)."""
+        torch = _torch()
+        p = torch.as_tensor(_i32(perm), device=self.t.device)
+        out = torch.empty_like(self.t)
+        self.pf.check(lib().b200la_permute(self.pf.h, self.dtype, self.get_size(), C.c_void_p(p.data_ptr()),
+                                           self.ptr, C.c_void_p(out.data_ptr())), "Reorder")
+        self.pf.sync()
+        self.t = out
+
+
+class CSR_lMatrix:
+    """CSR_lMatrix<T> on the B200 (src/linear_algebra/lmp/lmatrix_csr.h)."""
+
+    def __init__(self, platform, handle, n, m, nnz, dtype):
+        self.pf, self.h, self.n, self.m, self.nnz, self.dtype = platform, handle, n, m, nnz, dtype
+
+    @classmethod
+    def from_csr(cls, platform, row, col, val, n_cols=None, dtype=F64, segments=None):
+        row, col = _i32(row), _i32(col)
+        n = row.size - 1
+        m = n if n_cols is None else n_cols
+        v = np.ascontiguousarray(val, dtype=np.float64 if dtype == F64 else np.float32)
+        h = C.c_void_p()
+        if segments is None:
+            rc = lib().b200la_csr_create(platform.h, n, m, col.size, _np_ptr(row), _np_ptr(col), _np_ptr(v),
+                                         dtype, C.byref(h))
+        else:
+            so = _i32(segments)
+            rc = lib().b200la_csr_create_segmented(platform.h, n, m, col.size, _np_ptr(row), _np_ptr(col),
+                                                   _np_ptr(v), dtype, so.size - 1, _np_ptr(so), C.byref(h))
+        platform.check(rc, "csr_create")
+        return cls(platform, h, n, m, col.size, dtype)
+
+    def info(self):
+        vals = [C.c_int() for _ in range(7)]
+        self.pf.check(lib().b200la_csr_info(self.h, *[C.byref(v) for v in vals]))
+        keys = ["n_rows", "n_cols", "nnz", "dtype", "lanes_per_row", "n_tiles", "n_long_rows"]
+        out = dict(zip(keys, [v.value for v in vals]))
+        npat, uses = C.c_int(), C.c_int()
+        self.pf.check(lib().b200la_csr_format(self.h, C.byref(npat), C.byref(uses)))
+        out["row_patterns"], out["uses_pattern_dictionary"] = npat.value, bool(uses.value)
+        return out
+
+    def CastFrom(self, dtype):
+        """A copy of this matrix in another precision (lMatrix::CastFrom)."""
+        h = C.c_void_p()
+        self.pf.check(lib().b200la_csr_cast(self.pf.h, self.h, dtype, C.byref(h)), "CastFrom")
+        return CSR_lMatrix(self.pf, h, self.n, self.m, self.nnz, dtype)
+
+    def download(self):
+        row = np.empty(self.n + 1, np.int32)
+        col = np.empty(self.nnz, np.int32)
+        val = np.empty(self.nnz, np.float64 if self.dtype == F64 else np.float32)
+        self.pf.check(lib().b200la_csr_download(self.pf.h, self.h, _np_ptr(row), _np_ptr(col), _np_ptr(val)))
+        return row, col, val
+
+    def VectorMult(self, x, y):
+        self.pf.check(lib().b200la_spmv(self.pf.h, self.h, x.ptr, y.ptr), "VectorMult")
+
+    def VectorMultAdd(self, x, y):
+        self.pf.check(lib().b200la_spmv_add(self.pf.h, self.h, x.ptr, y.ptr), "VectorMultAdd")
+
+    def VectorMultDot(self, x, y):
+        torch = _torch()
+        d = torch.zeros(1, dtype=torch.float64, device=x.t.device)
+        self.pf.check(lib().b200la_spmv_dot(self.pf.h, self.h, x.ptr, y.ptr, C.c_void_p(d.data_ptr())),
+                      "VectorMultDot")
+        self.pf.sync()
+        return float(d.item())
+
+    def Residual(self, b, x, r):
+        torch = _torch()
+        d = torch.zeros(1, dtype=torch.float64, device=x.t.device)
+        self.pf.check(lib().b200la_residual(self.pf.h, self.h, b.ptr, x.ptr, r.ptr, C.c_void_p(d.data_ptr())),
+                      "Residual")
+        self.pf.sync()
+        return float(d.item())
+
+    def extract_invdiagelements(self, out):
+        self.pf.check(lib().b200la_csr_invdiag(self.pf.h, self.h, out.ptr), "invdiag")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().b200la_csr_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Preconditioner:
+    """lPreconditioner on the B200: Jacobi, MC-SGS or ILU(0) (level-scheduled / coloured)."""
+
+    def __init__(self, platform, handle, kind, n, A_perm=None):
+        self.pf, self.h, self.kind, self.n, self.A_perm = platform, handle, kind, n, A_perm
+        kind_c, n_c, nb = C.c_int(), C.c_int(), C.c_int()
+        sizes = np.zeros(n, np.int32)
+        perm = np.arange(n, dtype=np.int32)
+        lib().b200la_precond_info(handle, C.byref(kind_c), C.byref(n_c), C.byref(nb), _np_ptr(sizes),
+                                  _np_ptr(perm))
+        self.nblocks = nb.value
+        self.block_sizes = sizes[:nb.value].copy()
+        self.perm = perm if nb.value else None
+
+    @classmethod
+    def Jacobi(cls, platform, A):
+        h = C.c_void_p()
+        platform.check(lib().b200la_precond_jacobi(platform.h, A.h, C.byref(h)), "precond_jacobi")
+        return cls(platform, h, PRECOND_JACOBI, A.n)
+
+    @classmethod
+    def MultiColoringSGS(cls, platform, row, col, val, omega=1.0, dtype=F64):
+        row, col, val = _i32(row), _i32(col), _f64(val)
+        n = row.size - 1
+        h, Ap = C.c_void_p(), C.c_void_p()
+        platform.check(lib().b200la_precond_mcsgs(platform.h, n, _np_ptr(row), _np_ptr(col), _np_ptr(val), omega,
+                                                  dtype, C.byref(h), C.byref(Ap)), "precond_mcsgs")
+        A = CSR_lMatrix(platform, Ap, n, n, col.size, dtype)
+        return cls(platform, h, PRECOND_MCSGS, n, A)
+
+    @classmethod
+    def ILU0(cls, platform, row, col, val, mode=PRECOND_ILU0_LS, dtype=F64):
+        row, col, val = _i32(row), _i32(col), _f64(val)
+        n = row.size - 1
+        h, Ap = C.c_void_p(), C.c_void_p()
+        platform.check(lib().b200la_precond_ilu0(platform.h, n, _np_ptr(row), _np_ptr(col), _np_ptr(val), mode,
+                                                 dtype, C.byref(h), C.byref(Ap)), "precond_ilu0")
+        A = CSR_lMatrix(platform, Ap, n, n, col.size, dtype)
+        return cls(platform, h, mode, n, A)
+
+    def ApplyPreconditioner(self, r, z):
+        self.pf.check(lib().b200la_precond_apply(self.pf.h, self.h, r.ptr, z.ptr), "ApplyPreconditioner")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().b200la_precond_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Solver:
+    def __init__(self, platform):
+        self.pf = platform
+        self.op = None
+        self.precond = None
+        self.ctl = Control(1000, 0.0, 1e-10, 1e6)
+        self.result = Result()
+
+    def SetupOperator(self, A):
+        self.op = A
+
+    def SetupPreconditioner(self, P):
+        self.precond = P
+
+    def InitControl(self, maxits, abstol, reltol, divtol):
+        self.ctl = Control(maxits, abstol, reltol, divtol)
+
+    def iter(self):
+        return self.result.iters
+
+    def res(self):
+        return self.result.res
+
+
+class CG(_Solver):
+    """CG<LAD> (src/linear_solver/cg.cc) on the device."""
+
+    def Solve(self, b, x, history=0):
+        P = self.precond.h if self.precond is not None else None
+        if history:
+            hist = np.zeros(history)
+            rc = lib().b200la_cg_hist(self.pf.h, self.op.h, P, b.ptr, x.ptr, C.byref(self.ctl),
+                                      C.byref(self.result), _np_ptr(hist), history)
+            self.history = hist[:self.result.iters + 1]
+        else:
+            rc = lib().b200la_cg(self.pf.h, self.op.h, P, b.ptr, x.ptr, C.byref(self.ctl), C.byref(self.result))
+        self.pf.check(rc, "CG::Solve")
+        return self.result.status
+
+
+class GMRES(_Solver):
+    """GMRES<LAD>::SolveRight (src/linear_solver/gmres.cc) on the device."""
+
+    def __init__(self, platform, size_basis=30):
+        super().__init__(platform)
+        self.size_basis = size_basis
+
+    def Solve(self, b, x):
+        P = self.precond.h if self.precond is not None else None
+        rc = lib().b200la_gmres(self.pf.h, self.op.h, P, self.size_basis, b.ptr, x.ptr, C.byref(self.ctl),
+                                C.byref(self.result))
+        self.pf.check(rc, "GMRES::Solve")
+        return self.result.status
+
+
+class MPIR(_Solver):
+    """MPIR<LAD_high, LAD_low> (src/linear_solver/mpir.cc): FP64 defect correction
+    around an FP32 Jacobi-CG."""
+
+    def __init__(self, platform, max_outer=50):
+        super().__init__(platform)
+        self.inner = Control(10000, 0.0, 1e-4, 1e6)
+        self.max_outer = max_outer
+        self.op32 = None
+
+    def SetupLowPrecisionOperator(self, A32):
+        self.op32 = A32
+
+    def InitInnerControl(self, maxits, abstol, reltol, divtol):
+        self.inner = Control(maxits, abstol, reltol, divtol)
+
+    def Solve(self, b, x):
+        A32 = self.op32.h if self.op32 is not None else None
+        rc = lib().b200la_mpir(self.pf.h, self.op.h, A32, b.ptr, x.ptr, C.byref(self.ctl), C.byref(self.inner),
+                               self.max_outer, C.byref(self.result))
+        self.pf.check(rc, "MPIR::Solve")
+        return self.result.status

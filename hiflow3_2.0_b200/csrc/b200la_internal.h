@@ -1,0 +1,100 @@
+// b200la_internal.h -- objects behind the opaque handles of include/b200la.h.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "host_setup.h"
+#include "kernels.cuh"
+
+struct GraphEntry {
+    std::vector<const void *> key;
+    cudaGraphExec_t exec = nullptr;
+    int launches = 0;
+};
+
+struct b200la_ctx {
+    int device = 0;
+    int num_sms = 148;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    double *partials = nullptr;     // grid-reduction partials [8][kMaxGrid]
+    unsigned *ticket = nullptr;     // last-CTA tickets
+    int *dev_err = nullptr;         // device error flag (bounded waits)
+    b200::DevState *st = nullptr;   // device solver state
+    b200::DevState *st_host = nullptr;   // pinned mirror
+    double *dscal = nullptr;        // device scalars (256)
+    double *hscal = nullptr;        // pinned host scalars (256)
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;     // solver-internal timing
+    cudaEvent_t tev0 = nullptr, tev1 = nullptr;   // b200la_timer_start / stop
+    void *work = nullptr;           // solver workspace
+    size_t work_bytes = 0;
+    long long launches = 0;         // kernels launched through this context
+    std::vector<GraphEntry> graphs; // captured solver iteration batches
+    std::string msg;
+};
+
+struct b200la_csr {
+    int n = 0, m = 0, nnz = 0, dtype = 0, lg = 0, cfg = 0;
+    int *row = nullptr, *col = nullptr;
+    void *val = nullptr;
+    b200::Tile *tiles = nullptr;
+    int *long_rows = nullptr;
+    int ntiles = 0, nlong = 0;
+    b200::Seg all{};                  // whole-matrix schedule
+    std::vector<b200::Seg> segs;      // segs[0] = all, then one per row segment
+    std::vector<int> seg_off;         // row offsets of the segments (if any)
+    std::vector<int> h_row;           // host copy of the row pointer
+    size_t bytes = 0;
+    // row-pattern dictionary (null when the matrix has too many patterns)
+    uint16_t *pid = nullptr;
+    int *pat_off = nullptr, *pat_delta = nullptr;
+    int npat = 0, ndelta = 0;
+    bool use_pat = false;             // SpMV runs on the dictionary
+};
+
+struct b200la_precond {
+    int kind = 0, n = 0, dtype = 0;
+    void *invd = nullptr;             // Jacobi: 1/a_ii
+    // block sweeps (colours / levels) in the permuted numbering
+    int nblocks = 0;
+    std::vector<int> block_off;
+    std::vector<int> perm;            // perm[new] = old
+    b200la_csr *L = nullptr;          // entries left of the row's block (no diagonal)
+    b200la_csr *U = nullptr;          // entries right of the row's block (no diagonal)
+    void *Dv = nullptr, *iDv = nullptr;
+    int *perm_dev = nullptr;
+    // level-scheduled sync-free sweeps
+    int use_syncfree = 0;
+    unsigned *flags = nullptr;        // per-row completion epochs
+    unsigned *sync = nullptr;         // [epoch, fwd counter, bwd counter, done]
+    void *syncfree_plan = nullptr;    // chunk lists of the two sweeps
+};
+
+// shared helpers (capi.cu)
+int ctx_fail(const b200la_ctx *ctx, int code, const char *what, cudaError_t e);
+b200::Scratch ctx_scratch(const b200la_ctx *ctx);
+b200::CsrView csr_view(const b200la_csr *A);
+int ctx_work(b200la_ctx *ctx, size_t bytes, void **out);
+int ctx_check_device_error(b200la_ctx *ctx);
+int spmv_run(b200la_ctx *ctx, const b200la_csr *A, const b200::Seg &seg, b200::SpmvOp op);
+int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row, const int *col, const void *val,
+               int dtype, int n_seg, const int *seg_off, b200la_csr **out);
+// precond.cu
+int precond_apply_async(b200la_ctx *ctx, const b200la_precond *P, const void *r, void *z, const int *gate);
+int syncfree_setup(b200la_ctx *ctx, b200la_precond *P);
+int syncfree_apply(b200la_ctx *ctx, const b200la_precond *P, const void *r, void *z, const int *gate);
+void syncfree_free(b200la_precond *P);
+// solvers.cu
+void graph_cache_clear(b200la_ctx *ctx);
+
+namespace b200 {
+cudaError_t sweeps_configure();
+cudaError_t launch_invdiag(int dtype, int n, const int *row, const int *col, const void *val, void *out,
+                           cudaStream_t st);
+cudaError_t launch_jacobi(int dtype, int n, const void *invd, const void *r, void *z, const int *gate,
+                          cudaStream_t st);
+}  // namespace b200

@@ -1,0 +1,826 @@
+// capi.cu -- the C ABI of the B200 lmp platform (declared in include/b200la.h).
+//
+// Host orchestration only: argument checks, device memory, tile schedules,
+// preconditioner setup and the device-resident solver loops.  Every
+// arithmetic operation on vectors and matrices runs in a kernel of
+// kernels.cu / sweeps.cu; there is no host fallback.
+#include "b200la.h"
+#include "b200la_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace b200;
+
+// ------------------------------------------------------------------ helpers
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_CUDA, #call, e_);         \
+    } while (0)
+
+int ctx_fail(const b200la_ctx *ctx, int code, const char *what, cudaError_t e)
+{
+    if (ctx) {
+        char buf[512];
+        std::snprintf(buf, sizeof buf, "%s: %s", what, e == cudaSuccess ? "" : cudaGetErrorString(e));
+        const_cast<b200la_ctx *>(ctx)->msg = buf;
+    }
+    return code;
+}
+
+static int ctx_msg(const b200la_ctx *ctx, int code, const std::string &m)
+{
+    if (ctx) const_cast<b200la_ctx *>(ctx)->msg = m;
+    return code;
+}
+
+static size_t dsize(int dtype) { return dtype == B200LA_F64 ? 8 : 4; }
+
+Scratch ctx_scratch(const b200la_ctx *ctx)
+{
+    Scratch s;
+    s.partials = ctx->partials;
+    s.ticket = ctx->ticket;
+    s.err = ctx->dev_err;
+    s.num_sms = ctx->num_sms;
+    return s;
+}
+
+// Whether SpMV on a matrix of this dtype runs on its row-pattern dictionary
+// (when the matrix has one).  B200LA_PATTERN = 0: never, 1: FP32 only
+// (default; FP64 operators keep explicit 32-bit column indices), 2: always.
+static bool pattern_policy(int dtype)
+{
+    const char *e = std::getenv("B200LA_PATTERN");
+    const int mode = e ? std::atoi(e) : 1;
+    return mode == 2 || (mode == 1 && dtype == B200LA_F32);
+}
+
+CsrView csr_view(const b200la_csr *A)
+{
+    CsrView v;
+    v.row = A->row;
+    v.col = A->col;
+    v.val = A->val;
+    v.tiles = A->tiles;
+    v.long_rows = A->long_rows;
+    v.lg = A->lg;
+    v.dtype = A->dtype;
+    v.cfg = A->cfg;
+    v.pid = A->pid;
+    v.pat_off = A->pat_off;
+    v.pat_delta = A->pat_delta;
+    v.npat = A->npat;
+    v.ndelta = A->ndelta;
+    v.use_pat = A->pid != nullptr && A->use_pat;
+    return v;
+}
+
+int ctx_work(b200la_ctx *ctx, size_t bytes, void **out)
+{
+    if (bytes > ctx->work_bytes) {
+        if (ctx->work) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ctx->work);
+            ctx->work = nullptr;
+            ctx->work_bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&ctx->work, bytes);
+        if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_ALLOC, "workspace", e);
+        ctx->work_bytes = bytes;
+    }
+    *out = ctx->work;
+    return B200LA_OK;
+}
+
+int ctx_check_device_error(b200la_ctx *ctx)
+{
+    int h = 0;
+    CK(cudaMemcpyAsync(&h, ctx->dev_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (h != kDevOk) {
+        cudaMemsetAsync(ctx->dev_err, 0, sizeof(int), ctx->stream);
+        return ctx_msg(ctx, B200LA_ERR_TIMEOUT, "a bounded device wait gave up (error flag " + std::to_string(h) + ")");
+    }
+    return B200LA_OK;
+}
+
+// ------------------------------------------------------------------ context
+
+extern "C" int b200la_create(int device, b200la_ctx **out)
+{
+    if (!out) return B200LA_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) return B200LA_ERR_DEVICE;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return B200LA_ERR_DEVICE;
+    if (prop.major != 10) return B200LA_ERR_DEVICE;   // sm_100 family only
+    if (cudaSetDevice(device) != cudaSuccess) return B200LA_ERR_DEVICE;
+    b200la_ctx *ctx = new b200la_ctx();
+    ctx->device = device;
+    ctx->num_sms = prop.multiProcessorCount;
+    if (ctx->num_sms * kCtasPerSm > kMaxGrid || ctx->num_sms * 8 > kMaxGrid) ctx->num_sms = kMaxGrid / 8;
+    cudaError_t e;
+    if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) ||
+        (e = cudaMalloc(&ctx->partials, sizeof(double) * 8 * kMaxGrid)) ||
+        (e = cudaMalloc(&ctx->ticket, sizeof(unsigned) * 4)) || (e = cudaMalloc(&ctx->dev_err, sizeof(int))) ||
+        (e = cudaMalloc(&ctx->st, sizeof(DevState))) || (e = cudaMalloc(&ctx->dscal, sizeof(double) * 256)) ||
+        (e = cudaMallocHost(&ctx->st_host, sizeof(DevState))) ||
+        (e = cudaMallocHost(&ctx->hscal, sizeof(double) * 256)) || (e = cudaEventCreate(&ctx->ev0)) ||
+        (e = cudaEventCreate(&ctx->ev1)) || (e = cudaMemset(ctx->ticket, 0, sizeof(unsigned) * 4)) ||
+        (e = cudaMemset(ctx->dev_err, 0, sizeof(int))) || (e = spmv_configure()) || (e = sweeps_configure())) {
+        ctx->stream = ctx->own_stream;
+        b200la_destroy(ctx);
+        return B200LA_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    *out = ctx;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_destroy(b200la_ctx *ctx)
+{
+    if (!ctx) return B200LA_OK;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    graph_cache_clear(ctx);
+    if (ctx->work) cudaFree(ctx->work);
+    if (ctx->partials) cudaFree(ctx->partials);
+    if (ctx->ticket) cudaFree(ctx->ticket);
+    if (ctx->dev_err) cudaFree(ctx->dev_err);
+    if (ctx->st) cudaFree(ctx->st);
+    if (ctx->dscal) cudaFree(ctx->dscal);
+    if (ctx->st_host) cudaFreeHost(ctx->st_host);
+    if (ctx->hscal) cudaFreeHost(ctx->hscal);
+    if (ctx->ev0) cudaEventDestroy(ctx->ev0);
+    if (ctx->ev1) cudaEventDestroy(ctx->ev1);
+    if (ctx->tev0) cudaEventDestroy(ctx->tev0);
+    if (ctx->tev1) cudaEventDestroy(ctx->tev1);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_set_stream(b200la_ctx *ctx, void *s)
+{
+    if (!ctx) return B200LA_ERR_ARG;
+    cudaStreamSynchronize(ctx->stream);
+    graph_cache_clear(ctx);
+    ctx->stream = s ? static_cast<cudaStream_t>(s) : ctx->own_stream;
+    return B200LA_OK;
+}
+
+extern "C" void *b200la_get_stream(b200la_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
+
+extern "C" int b200la_sync(b200la_ctx *ctx)
+{
+    if (!ctx) return B200LA_ERR_ARG;
+    CK(cudaStreamSynchronize(ctx->stream));
+    return ctx_check_device_error(ctx);
+}
+
+extern "C" const char *b200la_last_error(const b200la_ctx *ctx) { return ctx ? ctx->msg.c_str() : "no context"; }
+
+extern "C" const char *b200la_status_string(int s)
+{
+    switch (s) {
+    case B200LA_OK: return "ok";
+    case B200LA_ERR_ARG: return "invalid argument";
+    case B200LA_ERR_CUDA: return "CUDA error";
+    case B200LA_ERR_ALLOC: return "allocation failed";
+    case B200LA_ERR_DEVICE: return "no usable sm_100 device";
+    case B200LA_ERR_CSR: return "malformed CSR";
+    case B200LA_ERR_BUDGET: return "refused by memory budget";
+    case B200LA_ERR_TIMEOUT: return "bounded device wait gave up";
+    case B200LA_ERR_SETUP: return "preconditioner setup failed";
+    case B200LA_ERR_NOTFOUND: return "unknown request";
+    default: return "unknown status";
+    }
+}
+
+extern "C" int b200la_num_sms(const b200la_ctx *ctx) { return ctx ? ctx->num_sms : 0; }
+
+// ------------------------------------------------------------------ memory
+
+extern "C" int b200la_malloc(b200la_ctx *ctx, size_t bytes, void **dptr)
+{
+    if (!ctx || !dptr) return B200LA_ERR_ARG;
+    cudaError_t e = cudaMalloc(dptr, bytes ? bytes : 16);
+    if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_ALLOC, "cudaMalloc", e);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_free(b200la_ctx *ctx, void *dptr)
+{
+    if (!ctx) return B200LA_ERR_ARG;
+    if (!dptr) return B200LA_OK;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFree(dptr));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_memcpy_h2d(b200la_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    if (!ctx || (bytes && (!dst || !src))) return B200LA_ERR_ARG;
+    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_memcpy_d2h(b200la_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    if (!ctx || (bytes && (!dst || !src))) return B200LA_ERR_ARG;
+    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_memcpy_d2d(b200la_ctx *ctx, void *dst, const void *src, size_t bytes)
+{
+    if (!ctx || (bytes && (!dst || !src))) return B200LA_ERR_ARG;
+    if (bytes) CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_memset_zero(b200la_ctx *ctx, void *dptr, size_t bytes)
+{
+    if (!ctx || (bytes && !dptr)) return B200LA_ERR_ARG;
+    if (bytes) CK(cudaMemsetAsync(dptr, 0, bytes, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_host_alloc(b200la_ctx *ctx, size_t bytes, void **hptr)
+{
+    if (!ctx || !hptr) return B200LA_ERR_ARG;
+    cudaError_t e = cudaMallocHost(hptr, bytes ? bytes : 16);
+    if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_ALLOC, "cudaMallocHost", e);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_host_free(b200la_ctx *ctx, void *hptr)
+{
+    if (!ctx) return B200LA_ERR_ARG;
+    if (!hptr) return B200LA_OK;
+    CK(cudaStreamSynchronize(ctx->stream));
+    CK(cudaFreeHost(hptr));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_timer_start(b200la_ctx *ctx)
+{
+    if (!ctx) return B200LA_ERR_ARG;
+    if (!ctx->tev0) {
+        CK(cudaEventCreate(&ctx->tev0));
+        CK(cudaEventCreate(&ctx->tev1));
+    }
+    CK(cudaEventRecord(ctx->tev0, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_timer_stop(b200la_ctx *ctx, double *ms)
+{
+    if (!ctx || !ms || !ctx->tev0) return B200LA_ERR_ARG;
+    CK(cudaEventRecord(ctx->tev1, ctx->stream));
+    CK(cudaEventSynchronize(ctx->tev1));
+    float f = 0.f;
+    CK(cudaEventElapsedTime(&f, ctx->tev0, ctx->tev1));
+    *ms = f;
+    return B200LA_OK;
+}
+
+// ------------------------------------------------------------------ matrix
+
+static int lanes_log2(int n, long long nnz)
+{
+    if (const char *e = std::getenv("B200LA_LANES")) {
+        const int l = std::atoi(e);
+        for (int lg = 0; lg <= 5; ++lg)
+            if ((1 << lg) == l) return lg;
+    }
+    const double mean = n > 0 ? (double)nnz / n : 0.0;
+    int lg = 0;
+    while (lg < 5 && (double)(8 << lg) < mean) ++lg;
+    return lg;
+}
+
+// SpMV variant for new matrices: B200LA_SPMV = wide | small | direct.
+static int spmv_cfg_choice()
+{
+    if (const char *e = std::getenv("B200LA_SPMV")) {
+        if (!std::strcmp(e, "small")) return kSpmvTileSmall;
+        if (!std::strcmp(e, "direct")) return kSpmvDirect;
+        if (!std::strcmp(e, "wide")) return kSpmvTileWide;
+    }
+    // measured on B200 (128^3 Q1, 27 nonzeros per row): the direct variant
+    // reaches 72% of HBM peak in FP64, the staged tiles 67%
+    return kSpmvDirect;
+}
+
+// Tile schedule of rows [s0, s1): runs of whole rows of at most kBlock >> lg
+// rows and `cap` nonzeros; longer rows go to the warp-per-row list.
+static void build_segment(const int *row, int s0, int s1, int lg, int cap, std::vector<Tile> &tiles,
+                          std::vector<int> &longs, std::vector<Seg> &segs)
+{
+    const int kTileCap = cap;
+    Seg sg;
+    sg.r0 = s0;
+    sg.r1 = s1;
+    sg.t0 = (int)tiles.size();
+    sg.l0 = (int)longs.size();
+    const int rows_max = kBlock >> lg;
+    int r = s0;
+    while (r < s1) {
+        if (row[r + 1] - row[r] > kTileCap) {
+            longs.push_back(r++);
+            continue;
+        }
+        const int r0 = r;
+        while (r < s1 && r - r0 < rows_max && row[r + 1] - row[r] <= kTileCap && row[r + 1] - row[r0] <= kTileCap)
+            ++r;
+        Tile t;
+        t.r0 = r0;
+        t.r1 = r;
+        t.a0 = row[r0] & ~3;
+        t.a1 = (row[r] + 3) & ~3;
+        tiles.push_back(t);
+    }
+    sg.t1 = (int)tiles.size();
+    sg.l1 = (int)longs.size();
+    segs.push_back(sg);
+}
+
+int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row, const int *col,
+               const void *val, int dtype, int n_seg, const int *seg_off, b200la_csr **out)
+{
+    if (!ctx || !out || !row || (nnz && (!col || !val)) || n_rows < 0 || n_cols < 0 || nnz < 0 ||
+        (dtype != B200LA_F64 && dtype != B200LA_F32))
+        return ctx_msg(ctx, B200LA_ERR_ARG, "csr_create: invalid argument");
+    long long bad = -1;
+    const int v = host::validate_csr(n_rows, n_cols, nnz, row, col, &bad);
+    if (v) return ctx_msg(ctx, B200LA_ERR_CSR, "csr_create: malformed CSR (code " + std::to_string(v) + " at " +
+                                                   std::to_string(bad) + ")");
+    if (n_seg > 0) {
+        if (!seg_off || seg_off[0] != 0 || seg_off[n_seg] != n_rows)
+            return ctx_msg(ctx, B200LA_ERR_ARG, "csr_create: bad segment offsets");
+        for (int s = 0; s < n_seg; ++s)
+            if (seg_off[s + 1] < seg_off[s]) return ctx_msg(ctx, B200LA_ERR_ARG, "csr_create: bad segment offsets");
+    }
+    b200la_csr *A = new b200la_csr();
+    A->n = n_rows;
+    A->m = n_cols;
+    A->nnz = nnz;
+    A->dtype = dtype;
+    A->lg = lanes_log2(n_rows, nnz);
+    A->cfg = spmv_cfg_choice();
+    const int cap = spmv_tile_cap(A->cfg);
+    A->h_row.assign(row, row + n_rows + 1);
+    std::vector<Tile> tiles;
+    std::vector<int> longs;
+    build_segment(row, 0, n_rows, A->lg, cap, tiles, longs, A->segs);   // segs[0] = whole matrix
+    A->all = A->segs[0];
+    if (n_seg > 0) {
+        // per-segment schedules follow the whole-matrix schedule
+        for (int s = 0; s < n_seg; ++s) build_segment(row, seg_off[s], seg_off[s + 1], A->lg, cap, tiles, longs, A->segs);
+        A->seg_off.assign(seg_off, seg_off + n_seg + 1);
+    }
+    A->ntiles = (int)tiles.size();
+    A->nlong = (int)longs.size();
+    const size_t pad = 8;
+    const size_t es = dsize(dtype);
+    cudaError_t e;
+    size_t bytes = sizeof(int) * (n_rows + 1) + (sizeof(int) + es) * (nnz + pad) + sizeof(Tile) * tiles.size() +
+                   sizeof(int) * (longs.size() + 1);
+    // row pointers, columns and values are padded by 8 entries: the bulk
+    // copies move whole 16-byte units past the last row / nonzero
+    if ((e = cudaMalloc(&A->row, sizeof(int) * (n_rows + 1 + pad))) ||
+        (e = cudaMalloc(&A->col, sizeof(int) * (nnz + pad))) ||
+        (e = cudaMalloc(&A->val, es * (nnz + pad))) ||
+        (e = cudaMalloc(&A->tiles, sizeof(Tile) * std::max<size_t>(tiles.size(), 1))) ||
+        (e = cudaMalloc(&A->long_rows, sizeof(int) * std::max<size_t>(longs.size(), 1)))) {
+        b200la_csr_destroy(A);
+        return ctx_fail(ctx, B200LA_ERR_ALLOC, "csr_create: device allocation", e);
+    }
+    A->bytes = bytes;
+    cudaStream_t s = ctx->stream;
+    if ((e = cudaMemsetAsync(A->row + n_rows + 1, 0, sizeof(int) * pad, s)) ||
+        (e = cudaMemcpyAsync(A->row, row, sizeof(int) * (n_rows + 1), cudaMemcpyHostToDevice, s)) ||
+        (e = cudaMemsetAsync(A->col + nnz, 0, sizeof(int) * pad, s)) ||
+        (e = cudaMemsetAsync(static_cast<char *>(A->val) + es * nnz, 0, es * pad, s)) ||
+        (nnz && (e = cudaMemcpyAsync(A->col, col, sizeof(int) * nnz, cudaMemcpyHostToDevice, s))) ||
+        (nnz && (e = cudaMemcpyAsync(A->val, val, es * nnz, cudaMemcpyHostToDevice, s))) ||
+        (!tiles.empty() && (e = cudaMemcpyAsync(A->tiles, tiles.data(), sizeof(Tile) * tiles.size(),
+                                                cudaMemcpyHostToDevice, s))) ||
+        (!longs.empty() &&
+         (e = cudaMemcpyAsync(A->long_rows, longs.data(), sizeof(int) * longs.size(), cudaMemcpyHostToDevice, s))) ||
+        (e = cudaStreamSynchronize(s))) {
+        b200la_csr_destroy(A);
+        return ctx_fail(ctx, B200LA_ERR_CUDA, "csr_create: upload", e);
+    }
+    // row-pattern dictionary (kept beside the explicit indices) when the
+    // matrix has few distinct row patterns, as stencil operators do
+    std::vector<uint16_t> pid;
+    std::vector<int> poff, pdel;
+    if (n_rows > 0 && host::row_patterns(n_rows, row, col, kMaxPatterns, kMaxPatternDeltas, pid, poff, pdel)) {
+        A->npat = (int)poff.size() - 1;
+        A->ndelta = (int)pdel.size();
+        if ((e = cudaMalloc(&A->pid, sizeof(uint16_t) * n_rows)) ||
+            (e = cudaMalloc(&A->pat_off, sizeof(int) * poff.size())) ||
+            (e = cudaMalloc(&A->pat_delta, sizeof(int) * std::max<size_t>(pdel.size(), 1))) ||
+            (e = cudaMemcpy(A->pid, pid.data(), sizeof(uint16_t) * n_rows, cudaMemcpyHostToDevice)) ||
+            (e = cudaMemcpy(A->pat_off, poff.data(), sizeof(int) * poff.size(), cudaMemcpyHostToDevice)) ||
+            (!pdel.empty() &&
+             (e = cudaMemcpy(A->pat_delta, pdel.data(), sizeof(int) * pdel.size(), cudaMemcpyHostToDevice)))) {
+            b200la_csr_destroy(A);
+            return ctx_fail(ctx, B200LA_ERR_ALLOC, "csr_create: pattern dictionary", e);
+        }
+        A->bytes += sizeof(uint16_t) * n_rows + sizeof(int) * (poff.size() + pdel.size());
+        A->use_pat = pattern_policy(dtype);
+    }
+    *out = A;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_csr_create(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row, const int *col,
+                                 const void *val, int dtype, b200la_csr **out)
+{
+    return csr_upload(ctx, n_rows, n_cols, nnz, row, col, val, dtype, 0, nullptr, out);
+}
+
+extern "C" int b200la_csr_create_segmented(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row,
+                                           const int *col, const void *val, int dtype, int n_seg, const int *seg_off,
+                                           b200la_csr **out)
+{
+    if (n_seg < 1) return ctx_msg(ctx, B200LA_ERR_ARG, "csr_create_segmented: n_seg < 1");
+    return csr_upload(ctx, n_rows, n_cols, nnz, row, col, val, dtype, n_seg, seg_off, out);
+}
+
+extern "C" int b200la_csr_destroy(b200la_csr *A)
+{
+    if (!A) return B200LA_OK;
+    cudaDeviceSynchronize();
+    if (A->row) cudaFree(A->row);
+    if (A->col) cudaFree(A->col);
+    if (A->val) cudaFree(A->val);
+    if (A->tiles) cudaFree(A->tiles);
+    if (A->long_rows) cudaFree(A->long_rows);
+    if (A->pid) cudaFree(A->pid);
+    if (A->pat_off) cudaFree(A->pat_off);
+    if (A->pat_delta) cudaFree(A->pat_delta);
+    delete A;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, b200la_csr **out)
+{
+    if (!ctx || !A || !out || (dtype != B200LA_F64 && dtype != B200LA_F32)) return B200LA_ERR_ARG;
+    b200la_csr *B = new b200la_csr(*A);
+    B->dtype = dtype;
+    B->row = nullptr;
+    B->col = nullptr;
+    B->val = nullptr;
+    B->tiles = nullptr;
+    B->long_rows = nullptr;
+    B->pid = nullptr;
+    B->pat_off = nullptr;
+    B->pat_delta = nullptr;
+    const size_t pad = 8, es = dsize(dtype);
+    cudaError_t e;
+    if (A->pid) {
+        if ((e = cudaMalloc(&B->pid, sizeof(uint16_t) * A->n)) ||
+            (e = cudaMalloc(&B->pat_off, sizeof(int) * (A->npat + 1))) ||
+            (e = cudaMalloc(&B->pat_delta, sizeof(int) * std::max(A->ndelta, 1))) ||
+            (e = cudaMemcpy(B->pid, A->pid, sizeof(uint16_t) * A->n, cudaMemcpyDeviceToDevice)) ||
+            (e = cudaMemcpy(B->pat_off, A->pat_off, sizeof(int) * (A->npat + 1), cudaMemcpyDeviceToDevice)) ||
+            (e = cudaMemcpy(B->pat_delta, A->pat_delta, sizeof(int) * std::max(A->ndelta, 1),
+                            cudaMemcpyDeviceToDevice))) {
+            b200la_csr_destroy(B);
+            return ctx_fail(ctx, B200LA_ERR_ALLOC, "csr_cast: pattern dictionary", e);
+        }
+        B->use_pat = pattern_policy(dtype);
+    }
+    if ((e = cudaMalloc(&B->row, sizeof(int) * (A->n + 1 + pad))) ||
+        (e = cudaMalloc(&B->col, sizeof(int) * (A->nnz + pad))) ||
+        (e = cudaMalloc(&B->val, es * (A->nnz + pad))) ||
+        (e = cudaMalloc(&B->tiles, sizeof(Tile) * std::max(A->ntiles, 1))) ||
+        (e = cudaMalloc(&B->long_rows, sizeof(int) * std::max(A->nlong, 1)))) {
+        b200la_csr_destroy(B);
+        return ctx_fail(ctx, B200LA_ERR_ALLOC, "csr_cast: allocation", e);
+    }
+    B->bytes = sizeof(int) * (A->n + 1) + (sizeof(int) + es) * (A->nnz + pad) + sizeof(Tile) * A->ntiles +
+               sizeof(int) * (A->nlong + 1);
+    cudaStream_t s = ctx->stream;
+    if ((e = cudaMemcpyAsync(B->row, A->row, sizeof(int) * (A->n + 1 + pad), cudaMemcpyDeviceToDevice, s)) ||
+        (e = cudaMemcpyAsync(B->col, A->col, sizeof(int) * (A->nnz + pad), cudaMemcpyDeviceToDevice, s)) ||
+        (e = launch_cast(A->dtype, A->val, dtype, B->val, (int)(A->nnz + pad), s)) ||
+        (e = cudaMemcpyAsync(B->tiles, A->tiles, sizeof(Tile) * std::max(A->ntiles, 1), cudaMemcpyDeviceToDevice, s)) ||
+        (e = cudaMemcpyAsync(B->long_rows, A->long_rows, sizeof(int) * std::max(A->nlong, 1), cudaMemcpyDeviceToDevice,
+                             s)) ||
+        (e = cudaStreamSynchronize(s))) {
+        b200la_csr_destroy(B);
+        return ctx_fail(ctx, B200LA_ERR_CUDA, "csr_cast", e);
+    }
+    *out = B;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_csr_info(const b200la_csr *A, int *n_rows, int *n_cols, int *nnz, int *dtype, int *lanes,
+                               int *n_tiles, int *n_long)
+{
+    if (!A) return B200LA_ERR_ARG;
+    if (n_rows) *n_rows = A->n;
+    if (n_cols) *n_cols = A->m;
+    if (nnz) *nnz = A->nnz;
+    if (dtype) *dtype = A->dtype;
+    if (lanes) *lanes = 1 << A->lg;
+    if (n_tiles) *n_tiles = A->all.t1 - A->all.t0;
+    if (n_long) *n_long = A->all.l1 - A->all.l0;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_csr_format(const b200la_csr *A, int *npat, int *uses_dict)
+{
+    if (!A) return B200LA_ERR_ARG;
+    if (npat) *npat = A->pid ? A->npat : 0;
+    if (uses_dict) *uses_dict = (A->pid && A->use_pat) ? 1 : 0;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_csr_download(b200la_ctx *ctx, const b200la_csr *A, int *row, int *col, void *val)
+{
+    if (!ctx || !A) return B200LA_ERR_ARG;
+    cudaStream_t s = ctx->stream;
+    if (row) CK(cudaMemcpyAsync(row, A->row, sizeof(int) * (A->n + 1), cudaMemcpyDeviceToHost, s));
+    if (col && A->nnz) CK(cudaMemcpyAsync(col, A->col, sizeof(int) * A->nnz, cudaMemcpyDeviceToHost, s));
+    if (val && A->nnz) CK(cudaMemcpyAsync(val, A->val, dsize(A->dtype) * A->nnz, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_csr_set_values(b200la_ctx *ctx, b200la_csr *A, const void *val)
+{
+    if (!ctx || !A || (A->nnz && !val)) return B200LA_ERR_ARG;
+    if (A->nnz) CK(cudaMemcpyAsync(A->val, val, dsize(A->dtype) * A->nnz, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_csr_invdiag(b200la_ctx *ctx, const b200la_csr *A, void *out)
+{
+    if (!ctx || !A || !out || A->n != A->m) return B200LA_ERR_ARG;
+    CK(launch_invdiag(A->dtype, A->n, A->row, A->col, A->val, out, ctx->stream));
+    return B200LA_OK;
+}
+
+// ------------------------------------------------------------------- SpMV
+
+int spmv_run(b200la_ctx *ctx, const b200la_csr *A, const Seg &seg, SpmvOp op)
+{
+    CK(launch_spmv(ctx_scratch(ctx), csr_view(A), seg, op, ctx->stream));
+    ctx->launches += 1;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_spmv(b200la_ctx *ctx, const b200la_csr *A, const void *x, void *y)
+{
+    if (!ctx || !A || !x || !y || x == y) return ctx_msg(ctx, B200LA_ERR_ARG, "spmv: invalid argument");
+    SpmvOp op;
+    op.epi = EPI_SET;
+    op.x = x;
+    op.y = y;
+    return spmv_run(ctx, A, A->all, op);
+}
+
+extern "C" int b200la_spmv_add(b200la_ctx *ctx, const b200la_csr *A, const void *x, void *y)
+{
+    if (!ctx || !A || !x || !y || x == y) return ctx_msg(ctx, B200LA_ERR_ARG, "spmv_add: invalid argument");
+    SpmvOp op;
+    op.epi = EPI_ADD;
+    op.x = x;
+    op.y = y;
+    return spmv_run(ctx, A, A->all, op);
+}
+
+extern "C" int b200la_spmv_dot(b200la_ctx *ctx, const b200la_csr *A, const void *x, void *y, double *dot_dev)
+{
+    if (!ctx || !A || !x || !y || !dot_dev || x == y || A->n != A->m)
+        return ctx_msg(ctx, B200LA_ERR_ARG, "spmv_dot: invalid argument");
+    SpmvOp op;
+    op.epi = EPI_DOT_X;
+    op.fin = FIN_STORE;
+    op.x = x;
+    op.y = y;
+    op.dot_out = dot_dev;
+    return spmv_run(ctx, A, A->all, op);
+}
+
+extern "C" int b200la_residual(b200la_ctx *ctx, const b200la_csr *A, const void *b, const void *x, void *r,
+                               double *nrm2sq_dev)
+{
+    if (!ctx || !A || !b || !x || !r || !nrm2sq_dev || x == r || A->n != A->m)
+        return ctx_msg(ctx, B200LA_ERR_ARG, "residual: invalid argument");
+    SpmvOp op;
+    op.epi = EPI_RESID;
+    op.fin = FIN_STORE;
+    op.x = x;
+    op.y = r;
+    op.b = b;
+    op.dot_out = nrm2sq_dev;
+    return spmv_run(ctx, A, A->all, op);
+}
+
+// ------------------------------------------------------------------ BLAS1
+
+static bool dt_ok(int dtype) { return dtype == B200LA_F64 || dtype == B200LA_F32; }
+
+extern "C" int b200la_dot_dev(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, double *out)
+{
+    if (!ctx || !dt_ok(dtype) || n < 0 || (n && (!x || !y)) || !out) return B200LA_ERR_ARG;
+    CK(launch_dot(ctx_scratch(ctx), dtype, n, x, y, out, false, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_dot(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, double *result)
+{
+    if (!ctx || !result) return B200LA_ERR_ARG;
+    int rc = b200la_dot_dev(ctx, dtype, n, x, y, ctx->dscal);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(ctx->hscal, ctx->dscal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *result = ctx->hscal[0];
+    return B200LA_OK;
+}
+
+extern "C" int b200la_nrm2(b200la_ctx *ctx, int dtype, int n, const void *x, double *result)
+{
+    if (!ctx || !result || !dt_ok(dtype) || n < 0 || (n && !x)) return B200LA_ERR_ARG;
+    CK(launch_dot(ctx_scratch(ctx), dtype, n, x, x, ctx->dscal, true, ctx->stream));
+    CK(cudaMemcpyAsync(ctx->hscal, ctx->dscal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    *result = ctx->hscal[0];
+    return B200LA_OK;
+}
+
+#define VEC_ARGS_OK (ctx && dt_ok(dtype) && n >= 0)
+
+extern "C" int b200la_axpy(b200la_ctx *ctx, int dtype, int n, double alpha, const void *x, void *y)
+{
+    if (!VEC_ARGS_OK || (n && (!x || !y))) return B200LA_ERR_ARG;
+    if (n) CK(launch_axpy(dtype, n, alpha, x, y, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_scaleadd(b200la_ctx *ctx, int dtype, int n, double alpha, const void *x, void *y)
+{
+    if (!VEC_ARGS_OK || (n && (!x || !y))) return B200LA_ERR_ARG;
+    if (n) CK(launch_scaleadd(dtype, n, alpha, x, y, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_scale(b200la_ctx *ctx, int dtype, int n, double alpha, void *y)
+{
+    if (!VEC_ARGS_OK || (n && !y)) return B200LA_ERR_ARG;
+    if (n) CK(launch_scale(dtype, n, alpha, y, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_ewmul(b200la_ctx *ctx, int dtype, int n, const void *x, void *y)
+{
+    if (!VEC_ARGS_OK || (n && (!x || !y))) return B200LA_ERR_ARG;
+    if (n) CK(launch_ewmul(dtype, n, x, y, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_cast(b200la_ctx *ctx, int src_dtype, const void *src, int dst_dtype, void *dst, int n)
+{
+    if (!ctx || !dt_ok(src_dtype) || !dt_ok(dst_dtype) || n < 0 || (n && (!src || !dst))) return B200LA_ERR_ARG;
+    if (n) CK(launch_cast(src_dtype, src, dst_dtype, dst, n, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_gather(b200la_ctx *ctx, int dtype, int n_idx, const int *idx, const void *x, void *out)
+{
+    if (!ctx || !dt_ok(dtype) || n_idx < 0 || (n_idx && (!idx || !x || !out))) return B200LA_ERR_ARG;
+    if (n_idx) CK(launch_gather(dtype, n_idx, idx, x, out, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_scatter(b200la_ctx *ctx, int dtype, int n_idx, const int *idx, const void *vals, void *x)
+{
+    if (!ctx || !dt_ok(dtype) || n_idx < 0 || (n_idx && (!idx || !x || !vals))) return B200LA_ERR_ARG;
+    if (n_idx) CK(launch_scatter(dtype, n_idx, idx, vals, x, ctx->stream));
+    return B200LA_OK;
+}
+
+extern "C" int b200la_permute(b200la_ctx *ctx, int dtype, int n, const int *perm, const void *in, void *out)
+{
+    if (!ctx || !dt_ok(dtype) || n < 0 || (n && (!perm || !in || !out)) || in == out) return B200LA_ERR_ARG;
+    if (n) CK(launch_gather(dtype, n, perm, in, out, ctx->stream));
+    return B200LA_OK;
+}
+
+// ------------------------------------------------------- host-side setup
+
+extern "C" int b200la_coo_to_csr(int n_rows, int nnz, const int *coo_row, const int *coo_col, const double *coo_val,
+                                 int *row, int *col, double *val)
+{
+    if (n_rows < 0 || nnz < 0 || !row || (nnz && (!coo_row || !coo_col || !col)) || (coo_val && !val))
+        return B200LA_ERR_ARG;
+    for (int e = 0; e < nnz; ++e)
+        if (coo_row[e] < 0 || coo_row[e] >= n_rows) return B200LA_ERR_CSR;
+    host::coo_to_csr(n_rows, nnz, coo_row, coo_col, coo_val, row, col, val);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_add_values(const int *row, const int *col, double *val, const int *rows, int num_rows,
+                                 const int *cols, int num_cols, const double *values)
+{
+    if (!row || !col || !val || num_rows < 0 || num_cols < 0 || (num_rows && (!rows || !values)) ||
+        (num_cols && !cols))
+        return B200LA_ERR_ARG;
+    host::add_values(row, col, val, rows, num_rows, cols, num_cols, values);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_zero_rows(const int *row, const int *col, double *val, const int *idx, int size, double alpha)
+{
+    if (!row || !col || !val || size < 0 || (size && !idx)) return B200LA_ERR_ARG;
+    host::zero_rows(row, col, val, idx, size, alpha);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_multicoloring(int n, const int *row, const int *col, int *ncolors, int *sizes, int *perm)
+{
+    if (n < 0 || !row || !col || !ncolors || !sizes || !perm) return B200LA_ERR_ARG;
+    std::vector<int> s, p;
+    if (host::multicoloring(n, row, col, ncolors, s, p)) return B200LA_ERR_SETUP;
+    std::copy(s.begin(), s.end(), sizes);
+    std::copy(p.begin(), p.end(), perm);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_levelscheduling(int n, const int *row, const int *col, int *nlevels, int *sizes, int *perm)
+{
+    if (n < 0 || !row || !col || !nlevels || !sizes || !perm) return B200LA_ERR_ARG;
+    std::vector<int> s, p;
+    if (host::levelscheduling(n, row, col, nlevels, s, p)) return B200LA_ERR_SETUP;
+    std::copy(s.begin(), s.end(), sizes);
+    std::copy(p.begin(), p.end(), perm);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_reorder_csr(int n, const int *row, const int *col, const double *val, const int *perm,
+                                  int *row_out, int *col_out, double *val_out)
+{
+    if (n < 0 || !row || !col || !val || !perm || !row_out || !col_out || !val_out) return B200LA_ERR_ARG;
+    host::Csr A, B;
+    A.n = A.m = n;
+    A.row.assign(row, row + n + 1);
+    A.col.assign(col, col + row[n]);
+    A.val.assign(val, val + row[n]);
+    std::vector<int> p(perm, perm + n);
+    host::reorder(A, p, B);
+    std::copy(B.row.begin(), B.row.end(), row_out);
+    std::copy(B.col.begin(), B.col.end(), col_out);
+    std::copy(B.val.begin(), B.val.end(), val_out);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_ilu0(int n, const int *row, const int *col, double *val)
+{
+    if (n < 0 || !row || !col || !val) return B200LA_ERR_ARG;
+    for (int i = 0; i < n; ++i) {
+        bool diag = false;
+        for (int j = row[i]; j < row[i + 1]; ++j) diag |= (col[j] == i);
+        if (!diag) return B200LA_ERR_CSR;   // the factorisation walks each row up to its diagonal
+    }
+    host::ilu0(n, row, col, val);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_q1_sizes(int dim, int N, int *n, int64_t *nnz)
+{
+    if (!n || !nnz) return B200LA_ERR_ARG;
+    return host::q1_sizes(dim, N, n, nnz) ? B200LA_ERR_ARG : B200LA_OK;
+}
+
+extern "C" int b200la_q1_assemble(int dim, int N, int kind, const double *kcell, double nu, const double *beta,
+                                  int *row, int *col, double *val)
+{
+    if (!row || !col || !val || (kind == 1 && !beta) || (kind != 0 && kind != 1)) return B200LA_ERR_ARG;
+    return host::q1_assemble(dim, N, kind, kcell, nu, beta, row, col, val) ? B200LA_ERR_ARG : B200LA_OK;
+}
+
+extern "C" int b200la_q1_rhs(uint64_t seed, int dim, int N, double *b)
+{
+    int n;
+    int64_t nnz;
+    if (!b || host::q1_sizes(dim, N, &n, &nnz)) return B200LA_ERR_ARG;
+    host::q1_rhs(seed, dim, N, b);
+    return B200LA_OK;
+}

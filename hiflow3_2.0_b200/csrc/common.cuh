@@ -1,0 +1,164 @@
+// common.cuh -- device helpers shared by the B200 lmp platform kernels.
+//
+// * PTX wrappers for mbarrier + cp.async.bulk (the bulk-copy engine streams
+//   CSR tiles into shared memory without occupying registers or threads),
+// * warp/block reductions,
+// * a deterministic grid reduction: every CTA writes one partial per quantity,
+//   the last CTA to finish (atomic ticket) sums the partials in CTA order and
+//   runs a caller-supplied finaliser on thread 0.  The result depends only on
+//   the grid size, never on CTA timing.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#ifndef B200LA_BLOCK
+#define B200LA_BLOCK 256
+#endif
+
+namespace b200 {
+
+constexpr int kBlock = B200LA_BLOCK;
+constexpr int kMaxGrid = 148 * 8;           // partial slots per reduction quantity
+constexpr long long kSpinLimit = 1LL << 28; // bounded waits: ~seconds, never forever
+
+// Error flags written by kernels (ctx->dev_err); the host reads them after sync.
+enum DevErr : int { kDevOk = 0, kDevWaitTimeout = 1, kDevBadIndex = 2 };
+
+__device__ __forceinline__ unsigned smem_u32(const void *p)
+{
+    return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init()
+{
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait on an mbarrier phase.  Returns false (and records the error)
+// if the phase does not complete within kSpinLimit polls.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, int *err)
+{
+    for (long long i = 0; i < kSpinLimit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    if (err) atomicExch(err, kDevWaitTimeout);
+    return false;
+}
+
+__device__ __forceinline__ uint64_t l2_evict_first_policy()
+{
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+// Global -> shared bulk copy completing on an mbarrier.  dst, src 16-byte
+// aligned; bytes a multiple of 16.  The L2 policy marks the streamed matrix
+// as evict-first so the gathered vector stays resident in L2.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *bar,
+                                         uint64_t policy)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint"
+        " [%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
+        : "memory");
+}
+
+template <typename T>
+__device__ __forceinline__ T warp_sum(T v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum of NQ values over the block; result valid on thread 0.  sm must hold
+// NQ * (kBlock / 32) doubles.
+template <int NQ>
+__device__ __forceinline__ void block_sum(double (&v)[NQ], double *sm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int nw = kBlock / 32;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) {
+        const double w = warp_sum(v[q]);
+        if (lane == 0) sm[q * nw + warp] = w;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += sm[q * nw + w];
+            v[q] = s;
+        }
+    }
+    __syncthreads();
+}
+
+// Grid-wide deterministic reduction tail.  Each CTA passes its per-thread
+// values; partials is [NQ][kMaxGrid]; ticket is reset to 0 by the last CTA.
+// Returns true on thread 0 of the last CTA, with out[] holding the totals
+// summed in CTA order.
+template <int NQ>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NQ], double *partials, unsigned *ticket,
+                                            double (&out)[NQ])
+{
+    __shared__ double sm[NQ * (kBlock / 32)];
+    __shared__ bool last;
+    block_sum<NQ>(v, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) partials[q * kMaxGrid + blockIdx.x] = v[q];
+        __threadfence();
+        const unsigned t = atomicAdd(ticket, 1u);
+        last = (t == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    // last CTA: every thread sums a fixed strided subset of the partials
+    // (loads issued together, through L2), then a fixed block tree -- the
+    // summation order depends only on the grid size
+    __threadfence();
+    double w[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) w[q] = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += kBlock) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) w[q] += __ldcg(partials + q * kMaxGrid + b);
+    }
+    block_sum<NQ>(w, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) out[q] = w[q];
+        *ticket = 0u;
+    }
+    return threadIdx.x == 0;
+}
+
+}  // namespace b200

@@ -1,0 +1,356 @@
+// kernels.cu -- BLAS1 and Krylov-step kernels of the B200 lmp platform
+// (the CSR SpMV kernels are in spmv.cu).
+#include "common.cuh"
+#include "kernels.cuh"
+
+#include <cmath>
+
+namespace b200 {
+
+namespace {
+
+// ------------------------------------------------------------------ BLAS1
+
+inline int stream_grid(const Scratch *s, int n, int per_thread = 4)
+{
+    int g = (n + kBlock * per_thread - 1) / (kBlock * per_thread);
+    const int cap = (s ? s->num_sms : 148) * 8;
+    if (g > cap) g = cap;
+    if (g > kMaxGrid) g = kMaxGrid;
+    return g < 1 ? 1 : g;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) dot_kernel(int n, const T *__restrict__ x, const T *__restrict__ y,
+                                                     double *out, bool sqrt_out, const int *gate, Scratch sc)
+{
+    if (gate && *reinterpret_cast<const volatile int *>(gate) != 0) return;
+    T a = T(0);
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) a += x[i] * y[i];
+    double v[1] = {(double)a}, o[1];
+    if (grid_reduce<1>(v, sc.partials, sc.ticket, o)) *out = sqrt_out ? sqrt(o[0]) : o[0];
+}
+
+template <typename T>
+__global__ void axpy_kernel(int n, T a, const T *__restrict__ x, T *__restrict__ y)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] += a * x[i];
+}
+
+template <typename T>
+__global__ void scaleadd_kernel(int n, T a, const T *__restrict__ x, T *__restrict__ y)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] = a * y[i] + x[i];
+}
+
+template <typename T>
+__global__ void scale_kernel(int n, T a, T *__restrict__ y)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] *= a;
+}
+
+template <typename T>
+__global__ void fill_kernel(int n, T a, T *__restrict__ y)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] = a;
+}
+
+template <typename T>
+__global__ void ewmul_kernel(int n, const T *__restrict__ x, T *__restrict__ y)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] *= x[i];
+}
+
+template <typename S, typename D>
+__global__ void cast_kernel(int n, const S *__restrict__ s, D *__restrict__ d)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) d[i] = (D)s[i];
+}
+
+template <typename T>
+__global__ void gather_kernel(int n, const int *__restrict__ idx, const T *__restrict__ x, T *__restrict__ out)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) out[i] = x[idx[i]];
+}
+
+template <typename T>
+__global__ void scatter_kernel(int n, const int *__restrict__ idx, const T *__restrict__ v, T *__restrict__ x)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) x[idx[i]] = v[i];
+}
+
+// ------------------------------------------------------------------ Krylov
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) cg_update_kernel(int n, int precond, T *__restrict__ x, T *__restrict__ r,
+                                                           const T *__restrict__ p, const T *__restrict__ Ap,
+                                                           const T *__restrict__ invd, DevState *st, Scratch sc)
+{
+    if (*reinterpret_cast<volatile int *>(&st->status) != kIterate) return;
+    const T alpha = (T)st->alpha;
+    double rr = 0.0, rz = 0.0;
+    T prr = T(0), prz = T(0);
+    int cnt = 0;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        x[i] += alpha * p[i];
+        const T ri = r[i] - alpha * Ap[i];
+        r[i] = ri;
+        prr += ri * ri;
+        if (precond == 1) prz += ri * (ri * invd[i]);
+        // FP32 partial sums are folded into double every 8 elements
+        if (sizeof(T) == 4 && ++cnt == 8) {
+            rr += (double)prr; rz += (double)prz;
+            prr = prz = T(0);
+            cnt = 0;
+        }
+    }
+    rr += (double)prr;
+    rz += (double)prz;
+    double v[2] = {rr, rz}, o[2];
+    if (grid_reduce<2>(v, sc.partials, sc.ticket, o)) {
+        const int it = st->iter + 1;
+        st->iter = it;
+        st->rr = o[0];
+        const double res = sqrt(o[0]);
+        st->res = res;
+        if (st->hist && it < st->hist_len) st->hist[it] = res;
+        const int status = check_state(st, it, res);
+        st->status = status;
+        if (status == kIterate && precond != 2) {
+            const double g = (precond == 1) ? o[1] : o[0];
+            st->beta = g / st->rho;
+            st->rho = g;
+        }
+    }
+}
+
+template <typename T>
+__global__ void cg_pupdate_kernel(int n, int precond, T *__restrict__ p, const T *__restrict__ r,
+                                  const T *__restrict__ invd, const T *__restrict__ z, DevState *st)
+{
+    if (*reinterpret_cast<volatile int *>(&st->status) != kIterate) return;
+    const T beta = (T)st->beta;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        const T zi = (precond == 1) ? r[i] * invd[i] : (precond == 0 ? r[i] : z[i]);
+        p[i] = beta * p[i] + zi;
+    }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) cg_start_kernel(int n, int precond, const T *__restrict__ r,
+                                                          const T *__restrict__ invd, const T *__restrict__ z,
+                                                          T *__restrict__ p, DevState *st, Scratch sc)
+{
+    double a = 0.0;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        const T ri = r[i];
+        const T zi = (precond == 1) ? ri * invd[i] : (precond == 0 ? ri : z[i]);
+        p[i] = zi;
+        a += (double)(ri * zi);
+    }
+    double v[1] = {a}, o[1];
+    if (grid_reduce<1>(v, sc.partials, sc.ticket, o)) st->rho = o[0];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kBlock) cg_rz_kernel(int n, const T *__restrict__ r, const T *__restrict__ z,
+                                                       DevState *st, Scratch sc)
+{
+    if (*reinterpret_cast<volatile int *>(&st->status) != kIterate) return;
+    double a = 0.0;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) a += (double)(r[i] * z[i]);
+    double v[1] = {a}, o[1];
+    if (grid_reduce<1>(v, sc.partials, sc.ticket, o)) {
+        st->rz = o[0];
+        st->beta = o[0] / st->rho;
+        st->rho = o[0];
+    }
+}
+
+__global__ void cast_residual_kernel(int n, const double *__restrict__ r, float *__restrict__ rl,
+                                     float *__restrict__ xl)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        rl[i] = (float)r[i];
+        xl[i] = 0.0f;
+    }
+}
+
+__global__ void add_correction_kernel(int n, const float *__restrict__ cl, double *__restrict__ x)
+{
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) x[i] += (double)cl[i];
+}
+
+template <typename T>
+__global__ void axpy_dev_kernel(int n, const double *coef, double sign, const T *__restrict__ x, T *__restrict__ y,
+                                const int *gate)
+{
+    if (gate && *reinterpret_cast<const volatile int *>(gate) != 0) return;
+    const T a = (T)(sign * *coef);
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] += a * x[i];
+}
+
+template <typename T>
+__global__ void scale_dev_kernel(int n, const double *coef, bool reciprocal, const T *__restrict__ x,
+                                 T *__restrict__ y, const int *gate)
+{
+    if (gate && *reinterpret_cast<const volatile int *>(gate) != 0) return;
+    const T a = (T)(reciprocal ? 1.0 / *coef : *coef);
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] = a * x[i];
+}
+
+}  // namespace
+
+#define B200_DISPATCH(dtype, ...)                 \
+    do {                                          \
+        if ((dtype) == 0) {                       \
+            using T = double;                     \
+            __VA_ARGS__;                          \
+        } else {                                  \
+            using T = float;                      \
+            __VA_ARGS__;                          \
+        }                                         \
+    } while (0)
+
+cudaError_t launch_dot(const Scratch &s, int dtype, int n, const void *x, const void *y, double *out, bool sqrt_out,
+                       cudaStream_t st)
+{
+    const int g = stream_grid(&s, n);
+    B200_DISPATCH(dtype, dot_kernel<T><<<g, kBlock, 0, st>>>(n, (const T *)x, (const T *)y, out, sqrt_out,
+                                                             nullptr, s));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dot_to(const Scratch &s, int dtype, int n, const void *x, const void *y, double *out,
+                          const int *gate, cudaStream_t st)
+{
+    const int g = stream_grid(&s, n);
+    B200_DISPATCH(dtype, dot_kernel<T><<<g, kBlock, 0, st>>>(n, (const T *)x, (const T *)y, out, false, gate, s));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_dot_norm_to(const Scratch &s, int dtype, int n, const void *x, double *out, const int *gate,
+                               cudaStream_t st)
+{
+    const int g = stream_grid(&s, n);
+    B200_DISPATCH(dtype, dot_kernel<T><<<g, kBlock, 0, st>>>(n, (const T *)x, (const T *)x, out, true, gate, s));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_axpy(int dtype, int n, double a, const void *x, void *y, cudaStream_t st)
+{
+    B200_DISPATCH(dtype, axpy_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, (T)a, (const T *)x, (T *)y));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scaleadd(int dtype, int n, double a, const void *x, void *y, cudaStream_t st)
+{
+    B200_DISPATCH(dtype,
+                  scaleadd_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, (T)a, (const T *)x, (T *)y));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale(int dtype, int n, double a, void *y, cudaStream_t st)
+{
+    B200_DISPATCH(dtype, scale_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, (T)a, (T *)y));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fill(int dtype, int n, double v, void *y, cudaStream_t st)
+{
+    B200_DISPATCH(dtype, fill_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, (T)v, (T *)y));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_ewmul(int dtype, int n, const void *x, void *y, cudaStream_t st)
+{
+    B200_DISPATCH(dtype, ewmul_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, (const T *)x, (T *)y));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cast(int src_dtype, const void *src, int dst_dtype, void *dst, int n, cudaStream_t st)
+{
+    const int g = stream_grid(nullptr, n);
+    if (src_dtype == 0 && dst_dtype == 1) cast_kernel<double, float><<<g, kBlock, 0, st>>>(n, (const double *)src, (float *)dst);
+    else if (src_dtype == 1 && dst_dtype == 0) cast_kernel<float, double><<<g, kBlock, 0, st>>>(n, (const float *)src, (double *)dst);
+    else if (src_dtype == 0) cast_kernel<double, double><<<g, kBlock, 0, st>>>(n, (const double *)src, (double *)dst);
+    else cast_kernel<float, float><<<g, kBlock, 0, st>>>(n, (const float *)src, (float *)dst);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather(int dtype, int n, const int *idx, const void *x, void *out, cudaStream_t st)
+{
+    B200_DISPATCH(dtype, gather_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, idx, (const T *)x, (T *)out));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(int dtype, int n, const int *idx, const void *vals, void *x, cudaStream_t st)
+{
+    B200_DISPATCH(dtype,
+                  scatter_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, idx, (const T *)vals, (T *)x));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_update(const Scratch &s, int dtype, int n, int precond, void *x, void *r, const void *p,
+                             const void *Ap, const void *invd, DevState *st, cudaStream_t stm)
+{
+    const int g = stream_grid(&s, n);
+    B200_DISPATCH(dtype, cg_update_kernel<T><<<g, kBlock, 0, stm>>>(n, precond, (T *)x, (T *)r, (const T *)p,
+                                                                    (const T *)Ap, (const T *)invd, st, s));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_pupdate(int dtype, int n, int precond, void *p, const void *r, const void *invd, const void *z,
+                              DevState *st, cudaStream_t stm)
+{
+    B200_DISPATCH(dtype, cg_pupdate_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, stm>>>(
+                             n, precond, (T *)p, (const T *)r, (const T *)invd, (const T *)z, st));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_start(const Scratch &s, int dtype, int n, int precond, const void *r, const void *invd,
+                            const void *z, void *p, DevState *st, cudaStream_t stm)
+{
+    const int g = stream_grid(&s, n);
+    B200_DISPATCH(dtype, cg_start_kernel<T><<<g, kBlock, 0, stm>>>(n, precond, (const T *)r, (const T *)invd,
+                                                                   (const T *)z, (T *)p, st, s));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cg_rz(const Scratch &s, int dtype, int n, const void *r, const void *z, DevState *st,
+                         cudaStream_t stm)
+{
+    const int g = stream_grid(&s, n);
+    B200_DISPATCH(dtype, cg_rz_kernel<T><<<g, kBlock, 0, stm>>>(n, (const T *)r, (const T *)z, st, s));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cast_residual(int n, const double *r, float *rl, float *xl, cudaStream_t st)
+{
+    cast_residual_kernel<<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, r, rl, xl);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_add_correction(int n, const float *cl, double *x, cudaStream_t st)
+{
+    add_correction_kernel<<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, cl, x);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_axpy_dev(int dtype, int n, const double *coef, double sign, const void *x, void *y,
+                            const int *gate, cudaStream_t st)
+{
+    B200_DISPATCH(dtype, axpy_dev_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(n, coef, sign, (const T *)x,
+                                                                                       (T *)y, gate));
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scale_dev(int dtype, int n, const double *coef, bool reciprocal, const void *x, void *y,
+                             const int *gate, cudaStream_t st)
+{
+    B200_DISPATCH(dtype, scale_dev_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, st>>>(
+                             n, coef, reciprocal, (const T *)x, (T *)y, gate));
+    return cudaGetLastError();
+}
+
+}  // namespace b200

@@ -1,0 +1,164 @@
+// kernels.cuh -- launch interface of the B200 lmp platform kernels (sm_100a).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b200 {
+
+// Matrix tiles: a run of whole rows [r0, r1) whose nonzeros [row[r0], row[r1])
+// fit one shared-memory stage.  a0/a1 are that nonzero range widened to
+// multiples of 4 elements, the unit the bulk-copy engine moves (16 bytes of
+// column indices, 32 / 16 bytes of double / float values).
+struct Tile {
+    int r0, r1, a0, a1;
+};
+
+// Row segment [r0, r1) of a matrix schedule: tiles [t0, t1) and overlong rows
+// [l0, l1) (rows with more nonzeros than one stage holds, done warp-per-row).
+struct Seg {
+    int t0, t1, l0, l1, r0, r1;
+};
+
+constexpr int kCtasPerSm = 2;    // persistent CTAs per SM of the widest tile variant (grid caps)
+
+// IterateControl state kept in device memory by the fused solvers.
+struct DevState {
+    double rho, alpha, beta, res, res0, pap, rz, rr;
+    double abstol, reltol, divtol, pad0;
+    int iter, status, maxits, hist_len;
+    double *hist;     // optional residual history (hist_len entries)
+};
+
+enum Status : int { kIterate = 0, kSuccessAbs = 1, kSuccessRel = 2, kFailDiv = 3, kFailMaxits = 4 };
+
+#ifdef __CUDACC__
+// IterateControl::Check (src/common/iterate_control.cc:84-110), first step 0.
+__device__ __forceinline__ int check_state(DevState *st, int step, double value)
+{
+    if (step == 0) st->res0 = value;
+    if (value < st->abstol) return kSuccessAbs;
+    if (value < st->reltol * st->res0) return kSuccessRel;
+    if (value > st->divtol * st->res0) return kFailDiv;
+    if (step >= st->maxits) return kFailMaxits;
+    return kIterate;
+}
+#endif
+
+// SpMV kernel variants (chosen per matrix when it is created):
+//   kSpmvTileWide  -- bulk-copy tiles of <= 2048 nonzeros, 4 stages, 2 CTAs/SM
+//   kSpmvTileSmall -- bulk-copy tiles of <= 1024 nonzeros, 3 stages, 4 CTAs/SM
+//   kSpmvDirect    -- no staging: 2^lg lanes per row read values / indices
+//                     with streaming loads, high occupancy, x through L1
+enum SpmvCfg : int { kSpmvTileWide = 0, kSpmvTileSmall = 1, kSpmvDirect = 2 };
+int spmv_tile_cap(int cfg);
+
+// SpMV epilogues (per row i, s = sum_j a_ij x_j):
+enum Epi : int {
+    EPI_SET = 0,     // y_i = s
+    EPI_ADD = 1,     // y_i += s
+    EPI_DOT_X = 2,   // y_i = s; reduce x_i * y_i
+    EPI_RESID = 3,   // y_i = b_i - s; reduce y_i^2
+    EPI_SGS_F = 4,   // y_i = (-b_i + s) * d1_i            (MC-SGS forward, d1 = -1/d)
+    EPI_SGS_B = 5,   // y_i = (y_i * d2_i + s) * d1_i      (MC-SGS diagonal + backward, d2 = -d)
+    EPI_ILU_F = 6,   // y_i = -(-b_i + s)                  (ILU forward, unit L)
+    EPI_ILU_B = 7,   // y_i = (-y_i + s) * d1_i            (ILU backward, d1 = -1/u_ii)
+};
+
+// What the last CTA does with a reduced value v (EPI_DOT_X / EPI_RESID).
+enum Fin : int {
+    FIN_NONE = 0,
+    FIN_STORE = 1,       // *dot_out = v
+    FIN_CG_ALPHA = 2,    // st->pap = v; st->alpha = st->rho / v
+    FIN_RES_INIT = 3,    // st->rr = v; st->res = sqrt(v); st->status = Check(0, res)
+};
+
+struct CsrView {
+    const int *row;
+    const int *col;
+    const void *val;
+    const Tile *tiles;
+    const int *long_rows;
+    int lg;          // log2 of lanes per row
+    int dtype;       // 0 double, 1 float
+    int cfg;         // SpmvCfg
+    // row-pattern dictionary (used when use_pat): column j of row i is
+    // i + pat_delta[pat_off[pid[i]] + (j - row[i])]
+    const uint16_t *pid;
+    const int *pat_off;
+    const int *pat_delta;
+    int npat, ndelta, use_pat;
+};
+
+constexpr int kMaxPatterns = 1024;
+constexpr int kMaxPatternDeltas = 6144;
+
+struct SpmvOp {
+    int epi = EPI_SET;
+    int fin = FIN_NONE;
+    const void *x = nullptr;
+    void *y = nullptr;
+    const void *b = nullptr;
+    const void *d1 = nullptr;
+    const void *d2 = nullptr;
+    double *dot_out = nullptr;
+    DevState *st = nullptr;
+    const int *gate = nullptr;    // skip the launch body when *gate != 0
+};
+
+struct Scratch {
+    double *partials;    // [8][kMaxGrid]
+    unsigned *ticket;
+    int *err;
+    int num_sms;
+};
+
+cudaError_t spmv_configure();
+cudaError_t launch_spmv(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st);
+
+// ---- BLAS1 (dtype 0 double, 1 float; scalars in double) ----
+cudaError_t launch_dot(const Scratch &s, int dtype, int n, const void *x, const void *y, double *out,
+                       bool sqrt_out, cudaStream_t st);
+cudaError_t launch_axpy(int dtype, int n, double a, const void *x, void *y, cudaStream_t st);
+cudaError_t launch_scaleadd(int dtype, int n, double a, const void *x, void *y, cudaStream_t st);
+cudaError_t launch_scale(int dtype, int n, double a, void *y, cudaStream_t st);
+cudaError_t launch_ewmul(int dtype, int n, const void *x, void *y, cudaStream_t st);
+cudaError_t launch_cast(int src_dtype, const void *src, int dst_dtype, void *dst, int n, cudaStream_t st);
+cudaError_t launch_gather(int dtype, int n, const int *idx, const void *x, void *out, cudaStream_t st);
+cudaError_t launch_scatter(int dtype, int n, const int *idx, const void *vals, void *x, cudaStream_t st);
+cudaError_t launch_fill(int dtype, int n, double v, void *y, cudaStream_t st);
+
+// ---- fused Krylov steps (vectors of type dtype, scalars in DevState) ----
+// CG update: x += alpha p; r -= alpha Ap; with invd (Jacobi) reduce rr and
+// r.(invd r), without reduce rr only (rz = rr when precond == 0, nothing when
+// precond == 2: the caller reduces r.z after its own apply).  The last CTA
+// advances iter, stores res, runs Check and, when iterating, sets
+// beta = rz / rho and rho = rz (precond 0/1).
+cudaError_t launch_cg_update(const Scratch &s, int dtype, int n, int precond, void *x, void *r, const void *p,
+                             const void *Ap, const void *invd, DevState *st, cudaStream_t stm);
+// p = beta p + z with z = invd .* r (precond 1), z = r (precond 0), or z given.
+cudaError_t launch_cg_pupdate(int dtype, int n, int precond, void *p, const void *r, const void *invd,
+                              const void *z, DevState *st, cudaStream_t stm);
+// CG start after r = b - A x: z = M r for Jacobi/none, p = z, rho = r.z,
+// res = ||r||, status = Check(0, res).  precond 2: caller supplies z.
+cudaError_t launch_cg_start(const Scratch &s, int dtype, int n, int precond, const void *r, const void *invd,
+                            const void *z, void *p, DevState *st, cudaStream_t stm);
+// rz = r.z; beta = rz / rho; rho = rz (gated on status).
+cudaError_t launch_cg_rz(const Scratch &s, int dtype, int n, const void *r, const void *z, DevState *st,
+                         cudaStream_t stm);
+// Mixed precision helpers: rl = (float) r, xl = 0; x += (double) cl.
+cudaError_t launch_cast_residual(int n, const double *r, float *rl, float *xl, cudaStream_t st);
+cudaError_t launch_add_correction(int n, const float *cl, double *x, cudaStream_t st);
+
+// GMRES pieces (double or float basis; scalars double):
+// h[i] = w.v ; then w -= h v  (one modified Gram-Schmidt step), device scalars.
+cudaError_t launch_dot_to(const Scratch &s, int dtype, int n, const void *x, const void *y, double *out,
+                          const int *gate, cudaStream_t st);
+cudaError_t launch_dot_norm_to(const Scratch &s, int dtype, int n, const void *x, double *out, const int *gate,
+                               cudaStream_t st);
+cudaError_t launch_axpy_dev(int dtype, int n, const double *coef, double sign, const void *x, void *y,
+                            const int *gate, cudaStream_t st);
+cudaError_t launch_scale_dev(int dtype, int n, const double *coef, bool reciprocal, const void *x, void *y,
+                             const int *gate, cudaStream_t st);
+
+}  // namespace b200

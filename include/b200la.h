@@ -1,0 +1,253 @@
+/*
+ * b200la.h -- C ABI of the B200 lmp platform for HiFlow3.
+ *
+ * The B200 platform is one more lmp ("local multi-platform") backend of
+ * HiFlow3's linear algebra.  Its C++ subclasses of lVector<T> / lMatrix<T>
+ * and the LinearSolver<LAD> implementations call only the functions below.
+ * Plain C types only: every pointer argument is either a host pointer or a
+ * device pointer as stated, sizes are ints (the reference's index type,
+ * src/linear_algebra/lmp/lmatrix_formats.h:40-45), scalars are doubles.
+ *
+ * Every function returns a b200la_status (0 = success).  On failure the
+ * context keeps a message, b200la_last_error().  Values are computed in the
+ * matrix/vector dtype (B200LA_F64 or B200LA_F32); reductions accumulate
+ * globally in double.
+ *
+ * Citations name the reference interface each entry point stands in for
+ * (paths relative to the HiFlow3 2.0 source tree).
+ */
+#ifndef B200LA_H
+#define B200LA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200LA_F64 0
+#define B200LA_F32 1
+
+typedef enum {
+    B200LA_OK = 0,
+    B200LA_ERR_ARG = 1,        /* invalid argument (null, size, dtype) */
+    B200LA_ERR_CUDA = 2,       /* a CUDA call failed */
+    B200LA_ERR_ALLOC = 3,      /* device or host allocation failed */
+    B200LA_ERR_DEVICE = 4,     /* no usable sm_100 device */
+    B200LA_ERR_CSR = 5,        /* malformed CSR (non-monotone rows, column out of range) */
+    B200LA_ERR_BUDGET = 6,     /* request refused by the serving memory budget */
+    B200LA_ERR_TIMEOUT = 7,    /* a bounded device wait gave up */
+    B200LA_ERR_SETUP = 8,      /* preconditioner analysis failed (e.g. no colours / levels) */
+    B200LA_ERR_NOTFOUND = 9    /* unknown serving request id */
+} b200la_status;
+
+/* IterateControl (src/common/iterate_control.h) */
+typedef struct {
+    int maxits;
+    double abstol, reltol, divtol;
+} b200la_control;
+
+/* IterateControl::State of the stop test (src/common/iterate_control.cc:84-110) */
+#define B200LA_ITERATE 0
+#define B200LA_SUCCESS_ABS 1
+#define B200LA_SUCCESS_REL 2
+#define B200LA_FAIL_DIV 3
+#define B200LA_FAIL_MAXITS 4
+
+typedef struct {
+    int iters;          /* Krylov iterations (inner iterations for MPIR) */
+    int status;         /* B200LA_SUCCESS_* / B200LA_FAIL_* */
+    double res0, res;   /* initial and final residual norm */
+    int outer;          /* MPIR outer corrections (0 otherwise) */
+    int launches;       /* kernels launched by the solve */
+    double solve_ms;    /* device time of the solve */
+} b200la_result;
+
+typedef struct b200la_ctx b200la_ctx;
+typedef struct b200la_csr b200la_csr;
+typedef struct b200la_precond b200la_precond;
+
+/* ---------------------------------------------------------------- context */
+
+/* init_platform_gpu (src/linear_algebra/lmp/cuda/platform_management_gpu.cu:78-171):
+ * select `device`, create the platform's stream and reduction scratch. */
+int b200la_create(int device, b200la_ctx **out);
+int b200la_destroy(b200la_ctx *ctx);
+/* Run the context's work on a caller-owned cudaStream_t (NULL: the context's own). */
+int b200la_set_stream(b200la_ctx *ctx, void *cuda_stream);
+void *b200la_get_stream(b200la_ctx *ctx);
+/* lVector::Sync (src/linear_algebra/lmp/lvector.h:245) */
+int b200la_sync(b200la_ctx *ctx);
+const char *b200la_last_error(const b200la_ctx *ctx);
+const char *b200la_status_string(int status);
+int b200la_num_sms(const b200la_ctx *ctx);
+
+/* ----------------------------------------------------------------- memory */
+
+/* memallocdev / memfreedev / memcpy2dev / memcpy2host / memcpydev
+ * (src/linear_algebra/lmp/lmp_mem.h:28-88, cuda/mem_cuda.cu:42-107).
+ * Copies are ordered on the context's stream; host buffers of the async
+ * forms must stay valid until b200la_sync. */
+int b200la_malloc(b200la_ctx *ctx, size_t bytes, void **dptr);
+int b200la_free(b200la_ctx *ctx, void *dptr);
+int b200la_memcpy_h2d(b200la_ctx *ctx, void *dst, const void *src, size_t bytes);
+int b200la_memcpy_d2h(b200la_ctx *ctx, void *dst, const void *src, size_t bytes);
+int b200la_memcpy_d2d(b200la_ctx *ctx, void *dst, const void *src, size_t bytes);
+int b200la_memset_zero(b200la_ctx *ctx, void *dptr, size_t bytes);
+/* Page-locked host buffers for asynchronous transfers (memallochost, lmp_mem.h:28-40). */
+int b200la_host_alloc(b200la_ctx *ctx, size_t bytes, void **hptr);
+int b200la_host_free(b200la_ctx *ctx, void *hptr);
+/* Device-time measurement on the context's stream, the CUDA-event counterpart
+ * of the ScopedTimer harness (src/tools/ScopedTimer.h:31-163): timer_start
+ * records an event, timer_stop records a second one, waits for it and returns
+ * the milliseconds between them. */
+int b200la_timer_start(b200la_ctx *ctx);
+int b200la_timer_stop(b200la_ctx *ctx, double *ms);
+
+/* ----------------------------------------------------------------- matrix */
+
+/* CSR_lMatrix<T>::Init + CopyFrom of a host CPU_CSR_lMatrix
+ * (src/linear_algebra/lmp/lmatrix_csr_cpu.cc:106-139; cuda/lmatrix_csr_gpu.cc:85-95).
+ * row/col/val are HOST arrays (val of type dtype).  The CSR is validated,
+ * uploaded and given its tile schedule (lanes per row from the mean row length). */
+int b200la_csr_create(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row, const int *col,
+                      const void *val, int dtype, b200la_csr **out);
+/* Same with rows grouped into segments [seg_off[s], seg_off[s+1]) that the
+ * schedule never mixes (colours / levels), n_seg segments. */
+int b200la_csr_create_segmented(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row,
+                                const int *col, const void *val, int dtype, int n_seg, const int *seg_off,
+                                b200la_csr **out);
+int b200la_csr_destroy(b200la_csr *A);
+/* lMatrix::CastFrom (src/linear_algebra/lmp/lmatrix.h:297-301): device-side copy in dtype. */
+int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, b200la_csr **out);
+int b200la_csr_info(const b200la_csr *A, int *n_rows, int *n_cols, int *nnz, int *dtype, int *lanes_per_row,
+                    int *n_tiles, int *n_long_rows);
+/* Storage form the SpMV uses: *npat = number of distinct row patterns in the
+ * matrix's row-pattern dictionary (0: none), *uses_dict = 1 when SpMV reads
+ * the dictionary instead of the explicit column indices. */
+int b200la_csr_format(const b200la_csr *A, int *npat, int *uses_dict);
+/* lMatrix::CopyTo a host CSR (host arrays, val of the matrix dtype). */
+int b200la_csr_download(b200la_ctx *ctx, const b200la_csr *A, int *row, int *col, void *val);
+/* New values, same structure (host array of the matrix dtype). */
+int b200la_csr_set_values(b200la_ctx *ctx, b200la_csr *A, const void *val);
+/* extract_invdiagelements (src/linear_algebra/lmp/lmatrix_csr_cpu.cc:2414-2431): out[i] = 1/a_ii, device. */
+int b200la_csr_invdiag(b200la_ctx *ctx, const b200la_csr *A, void *out_dev);
+
+/* ------------------------------------------------------------------- SpMV */
+
+/* lMatrix::VectorMult y = A x (src/linear_algebra/lmp/lmatrix.h:331; GPU
+ * cuda/GPUscalar_csr_lmatrix.cu:89-111).  x, y device vectors of A's dtype. */
+int b200la_spmv(b200la_ctx *ctx, const b200la_csr *A, const void *x, void *y);
+/* lMatrix::VectorMultAdd y += A x (src/linear_algebra/lmp/lmatrix.h:336). */
+int b200la_spmv_add(b200la_ctx *ctx, const b200la_csr *A, const void *x, void *y);
+/* Fused y = A x and *dot_dev = x . y (device double), as CG's
+ * VectorMult + Dot (src/linear_solver/cg.cc:211-212). */
+int b200la_spmv_dot(b200la_ctx *ctx, const b200la_csr *A, const void *x, void *y, double *dot_dev);
+/* Fused r = b - A x and *nrm_dev = ||r||^2 (cg.cc:200-202: VectorMult, ScaleAdd, Dot). */
+int b200la_residual(b200la_ctx *ctx, const b200la_csr *A, const void *b, const void *x, void *r,
+                    double *nrm2sq_dev);
+
+/* ------------------------------------------------------------------- BLAS1 */
+
+/* lVector::Dot / Norm2 (src/linear_algebra/lmp/lvector.h:266,274; GPU
+ * cuda/GPUblas_lvector.cu:204-220).  Result to a HOST double (synchronises). */
+int b200la_dot(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, double *result);
+int b200la_nrm2(b200la_ctx *ctx, int dtype, int n, const void *x, double *result);
+/* Same, result to a DEVICE double, no synchronisation. */
+int b200la_dot_dev(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, double *result_dev);
+/* lVector::Axpy: y += alpha x (lvector.h:283) */
+int b200la_axpy(b200la_ctx *ctx, int dtype, int n, double alpha, const void *x, void *y);
+/* lVector::ScaleAdd: y = alpha y + x (lvector.h:289) */
+int b200la_scaleadd(b200la_ctx *ctx, int dtype, int n, double alpha, const void *x, void *y);
+/* lVector::Scale: y *= alpha (lvector.h:278) */
+int b200la_scale(b200la_ctx *ctx, int dtype, int n, double alpha, void *y);
+/* lVector::ElementWiseMult: y = y .* x (lvector.h:248) */
+int b200la_ewmul(b200la_ctx *ctx, int dtype, int n, const void *x, void *y);
+/* lVector::CastFrom / CastTo double <-> float (lvector.h:231-235) */
+int b200la_cast(b200la_ctx *ctx, int src_dtype, const void *src, int dst_dtype, void *dst, int n);
+/* GetIndexedValues / SetIndexedValues (lvector.h:152-160): out[i] = x[idx[i]] / x[idx[i]] = v[i];
+ * idx is a device array of n_idx entries, each in [0, size of x). */
+int b200la_gather(b200la_ctx *ctx, int dtype, int n_idx, const int *idx_dev, const void *x, void *out);
+int b200la_scatter(b200la_ctx *ctx, int dtype, int n_idx, const int *idx_dev, const void *vals, void *x);
+/* lVector::Reorder (src/linear_algebra/lmp/lvector_cpu.cc:75-94): out[i] = in[perm[i]], device perm. */
+int b200la_permute(b200la_ctx *ctx, int dtype, int n, const int *perm_dev, const void *in, void *out);
+
+/* ------------------------------------------------------- host-side setup */
+/* One-time host algorithms, results identical to the reference's. */
+
+/* TransformFromCOO / init_structure (lmatrix_csr_cpu.cc:951-1044, 1101-1121); coo_val may be NULL. */
+int b200la_coo_to_csr(int n_rows, int nnz, const int *coo_row, const int *coo_col, const double *coo_val,
+                      int *row, int *col, double *val);
+/* add_values (lmatrix_csr_cpu.cc:1148-1181) */
+int b200la_add_values(const int *row, const int *col, double *val, const int *rows, int num_rows,
+                      const int *cols, int num_cols, const double *values);
+/* ZeroRows (lmatrix_csr_cpu.cc:1047-1068; via CoupledMatrix::diagonalize_rows, coupled_matrix.cc:550-576) */
+int b200la_zero_rows(const int *row, const int *col, double *val, const int *index_set, int size, double alpha);
+/* Multicoloring (lmatrix_csr_cpu.cc:2175-2290); sizes holds n entries; perm[new] = old. */
+int b200la_multicoloring(int n, const int *row, const int *col, int *ncolors, int *sizes, int *perm);
+/* Levelscheduling (lmatrix_csr_cpu.cc:2295-2392); sizes holds n entries; perm[new] = old. */
+int b200la_levelscheduling(int n, const int *row, const int *col, int *nlevels, int *sizes, int *perm);
+/* Reorder (lmatrix_csr_cpu.cc:1847-1861): B = P A P^T, perm[new] = old. */
+int b200la_reorder_csr(int n, const int *row, const int *col, const double *val, const int *perm, int *row_out,
+                       int *col_out, double *val_out);
+/* ilu0 (lmatrix_csr_cpu.cc:1880-1930), in place on val. */
+int b200la_ilu0(int n, const int *row, const int *col, double *val);
+/* Structured Q1 workloads (lexicographic DoFs; weak forms of
+ * examples/poisson/poisson_tutorial.h:152-176 and examples/convection_diffusion/convdiff.cc:75-117):
+ * kind 0 Poisson (kcell per cell or NULL), kind 1 convection-diffusion (nu, beta). */
+int b200la_q1_sizes(int dim, int N, int *n, int64_t *nnz);
+int b200la_q1_assemble(int dim, int N, int kind, const double *kcell, double nu, const double *beta, int *row,
+                       int *col, double *val);
+int b200la_q1_rhs(uint64_t seed, int dim, int N, double *b);
+
+/* --------------------------------------------------------- preconditioners */
+
+#define B200LA_PRECOND_JACOBI 1
+#define B200LA_PRECOND_MCSGS 2
+#define B200LA_PRECOND_ILU0_LS 3
+#define B200LA_PRECOND_ILU0_MC 4
+
+/* lPreconditioner_Jacobi::Build (src/linear_algebra/lmp/lpreconditioner.cc:127-148). */
+int b200la_precond_jacobi(b200la_ctx *ctx, const b200la_csr *A, b200la_precond **out);
+/* lPreconditioner_MultiColoring_SymmetricGaussSeidel Build (lpreconditioner_mc.cc:157-195,
+ * lpreconditioner_mc_sgs.cc:46-59) from the natural-order HOST CSR: colouring, the
+ * permuted operator (returned in *A_perm, dtype), dropped L/U sweep matrices and D. */
+int b200la_precond_mcsgs(b200la_ctx *ctx, int n, const int *row, const int *col, const double *val,
+                         double omega, int dtype, b200la_precond **out, b200la_csr **A_perm);
+/* lPreconditioner_MultiColoring_ILUp with ILU(0) (lpreconditioner_mc_ilup.cc:84-262):
+ * mode B200LA_PRECOND_ILU0_LS factorises in natural order then level-schedules
+ * (mc = false, ls = true); B200LA_PRECOND_ILU0_MC colours first (mc = true). */
+int b200la_precond_ilu0(b200la_ctx *ctx, int n, const int *row, const int *col, const double *val, int mode,
+                        int dtype, b200la_precond **out, b200la_csr **A_perm);
+/* Permutation (perm[new] = old, host array of n) and block structure
+ * (colours or levels; sizes holds n entries). */
+int b200la_precond_info(const b200la_precond *P, int *kind, int *n, int *nblocks, int *block_sizes, int *perm);
+/* ApplylPreconditioner: z = M^-1 r (device vectors of the preconditioner's dtype). */
+int b200la_precond_apply(b200la_ctx *ctx, const b200la_precond *P, const void *r, void *z);
+int b200la_precond_destroy(b200la_precond *P);
+
+/* ---------------------------------------------------------------- solvers */
+
+/* CG<LAD>::Solve (src/linear_solver/cg.cc:68-248): P NULL = SolveNoPrecond.
+ * b, x device vectors of A's dtype; x holds the start vector and the result.
+ * Scalars stay on the device; the host polls the stop state in batches. */
+int b200la_cg(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P, const void *b, void *x,
+              const b200la_control *ctl, b200la_result *res);
+/* As b200la_cg, with the residual norm after every iteration written to the
+ * host array hist (max hist_len entries). */
+int b200la_cg_hist(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P, const void *b, void *x,
+                   const b200la_control *ctl, b200la_result *res, double *hist, int hist_len);
+/* GMRES<LAD>::SolveRight with restart m (src/linear_solver/gmres.cc:285-510). */
+int b200la_gmres(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P, int m, const void *b, void *x,
+                 const b200la_control *ctl, b200la_result *res);
+/* MPIR<LAD_high,LAD_low>::Solve (src/linear_solver/mpir.cc:69-326) with an FP32 Jacobi-CG
+ * error correction.  A64 is the FP64 operator; A32 (may be NULL: cast here) its FP32 copy.
+ * outer->reltol is relative to ||b - A x0||. */
+int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_csr *A32, const double *b, double *x,
+                const b200la_control *outer, const b200la_control *inner, int max_outer, b200la_result *res);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* B200LA_H */

@@ -497,3 +497,35 @@ class Ref:
 
     def max_threads(self):
         return self.lib.ref_max_threads()
+
+
+def _ref_timing_sigs(L):
+    L.ref_mpir.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int,
+                           C.c_double, C.c_double, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                           C.POINTER(C.c_double)]
+    L.ref_mpir.restype = C.c_double
+    L.ref_pcg_timed.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p,
+                                C.c_double, C.c_int, C.POINTER(C.c_int)]
+    L.ref_pcg_timed.restype = C.c_double
+
+
+def ref_mpir(ref, row, col, val, b, nthreads, max_outer=50, reltol=1e-10, inner_reltol=1e-4,
+             inner_maxits=100000, sample_inner=0, impl=1):
+    """The reference's lmp objects driving MPIR (FP64 outer, FP32 Jacobi-CG inner)."""
+    _ref_timing_sigs(ref.lib)
+    n = len(row) - 1
+    x = np.zeros(n)
+    o, i, r = C.c_int(), C.c_int(), C.c_double()
+    dt = ref.lib.ref_mpir(impl, nthreads, n, len(col), _i32(row), _i32(col), _f64(val), _f64(b), x, max_outer,
+                          reltol, inner_reltol, inner_maxits, sample_inner, C.byref(o), C.byref(i), C.byref(r))
+    return dict(seconds=dt, outer=o.value, inner_total=i.value, res=r.value, x=x)
+
+
+def ref_pcg_timed(ref, row, col, val, b, nthreads, reltol=1e-10, maxits=100000, impl=1):
+    _ref_timing_sigs(ref.lib)
+    n = len(row) - 1
+    x = np.zeros(n)
+    it = C.c_int()
+    dt = ref.lib.ref_pcg_timed(impl, nthreads, n, len(col), _i32(row), _i32(col), _f64(val), _f64(b), x, reltol,
+                               maxits, C.byref(it))
+    return dict(seconds=dt, iters=it.value, x=x)

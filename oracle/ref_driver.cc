@@ -516,3 +516,153 @@ double ref_time_spmv(int nthreads, int reps, int n, int nnz, const int *row, con
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
 }  // extern "C"
+
+namespace {
+
+template <typename T>
+lMatrix<T> *make_matrix_t(int impl, int n, int nnz, const int *row, const int *col, const double *val, int nthreads)
+{
+    CPUsimple_CSR_lMatrix<T> *s = new CPUsimple_CSR_lMatrix<T>(nnz, n, n, "A");
+    std::memcpy(s->matrix.row, row, sizeof(int) * (n + 1));
+    std::memcpy(s->matrix.col, col, sizeof(int) * nnz);
+    for (int j = 0; j < nnz; ++j) s->matrix.val[j] = (T)val[j];
+    if (impl == 0) return s;
+    CPUopenmp_CSR_lMatrix<T> *o = new CPUopenmp_CSR_lMatrix<T>();
+    o->CopyStructureFrom(*s);
+    o->CopyFrom(*s);
+    o->set_num_threads(nthreads > 0 ? nthreads : 1);
+    delete s;
+    return o;
+}
+
+template <typename T>
+lVector<T> *make_vector_t(int impl, int n, int nthreads)
+{
+    if (impl == 0) {
+        CPUsimple_lVector<T> *x = new CPUsimple_lVector<T>(n, "v");
+        x->Zeros();
+        return x;
+    }
+    CPUopenmp_lVector<T> *x = new CPUopenmp_lVector<T>(n, "v");
+    x->set_num_threads(nthreads > 0 ? nthreads : 1);
+    x->Zeros();
+    return x;
+}
+
+// CG<LAD>::SolvePrecond with lPreconditioner_Jacobi, restated over lVector<T>
+// (src/linear_solver/cg.cc:164-248); at most `cap` iterations when cap > 0.
+template <typename T>
+int pcg_t(lMatrix<T> &A, lPreconditioner<T> &P, lVector<T> &b, lVector<T> &x, Control &ctl, int cap, int *iters)
+{
+    lVector<T> *r = b.CloneWithoutContent(), *p = b.CloneWithoutContent();
+    lVector<T> *z = b.CloneWithoutContent(), *Ap = b.CloneWithoutContent();
+    int iter = 0;
+    A.VectorMult(x, r);
+    r->ScaleAdd((T)-1.0, b);
+    T beta;
+    double res = std::sqrt((double)r->Dot(*r));
+    int conv = ctl.check(iter, res);
+    z->Zeros();
+    P.ApplylPreconditioner(*r, z);
+    p->CopyFrom(*z);
+    beta = r->Dot(*z);
+    while (conv == 0 && (cap <= 0 || iter < cap)) {
+        ++iter;
+        A.VectorMult(*p, Ap);
+        const T alpha = beta / Ap->Dot(*p);
+        x.Axpy(*p, alpha);
+        r->Axpy(*Ap, -alpha);
+        res = std::sqrt((double)r->Dot(*r));
+        conv = ctl.check(iter, res);
+        if (conv) break;
+        z->Zeros();
+        P.ApplylPreconditioner(*r, z);
+        const T gamma = r->Dot(*z);
+        beta = gamma / beta;
+        p->ScaleAdd(beta, *z);
+        beta = gamma;
+    }
+    *iters = iter;
+    delete r; delete p; delete z; delete Ap;
+    return conv;
+}
+
+}  // namespace
+
+extern "C" {
+
+// MPIR<LAD_high, LAD_low>::Solve restated over the reference's lmp objects
+// (src/linear_solver/mpir.cc:69-326): FP64 residual, CastFrom to FP32, FP32
+// Jacobi-CG error correction, CastFrom back, FP64 update.  The relative stop
+// uses the initial residual.  With sample_inner > 0 the run stops after that
+// many inner iterations in total (a bounded timing sample).  Returns the wall
+// time in seconds of the solve (setup excluded).
+double ref_mpir(int impl, int nthreads, int n, int nnz, const int *row, const int *col, const double *val,
+                const double *b, double *x, int max_outer, double reltol, double inner_reltol,
+                int inner_maxits, int sample_inner, int *outer_done, int *inner_done, double *res_out)
+{
+    lMatrix<double> *Ah = make_matrix_t<double>(impl, n, nnz, row, col, val, nthreads);
+    lMatrix<float> *Al = make_matrix_t<float>(impl, n, nnz, row, col, val, nthreads);
+    lVector<double> *vb = make_vector_t<double>(impl, n, nthreads), *vx = make_vector_t<double>(impl, n, nthreads);
+    std::memcpy(dynamic_cast<CPU_lVector<double> *>(vb)->buffer, b, sizeof(double) * n);
+    std::memcpy(dynamic_cast<CPU_lVector<double> *>(vx)->buffer, x, sizeof(double) * n);
+    lVector<double> *resh = vb->CloneWithoutContent(), *corh = vb->CloneWithoutContent();
+    lVector<float> *resl = make_vector_t<float>(impl, n, nthreads), *corl = make_vector_t<float>(impl, n, nthreads);
+    lVector<float> *dl = resl->CloneWithoutContent();
+    lPreconditioner_Jacobi<float> J;
+    J.Init(*dl);
+    J.SetupOperator(*Al);
+    J.Build();
+    const auto t0 = std::chrono::steady_clock::now();
+    Ah->VectorMult(*vx, resh);
+    resh->ScaleAdd(-1.0, *vb);
+    double res = resh->Norm2();
+    const double res0 = res;
+    int outer = 0, inner_total = 0;
+    while (res > 0.0 && res > reltol * res0 && outer < max_outer &&
+           (sample_inner <= 0 || inner_total < sample_inner)) {
+        ++outer;
+        resl->CastFrom(*resh);
+        corl->Zeros();
+        Control ic{inner_maxits, 0.0, inner_reltol, 1e6, 0.0};
+        int it = 0;
+        pcg_t<float>(*Al, J, *resl, *corl, ic, sample_inner > 0 ? sample_inner - inner_total : 0, &it);
+        inner_total += it;
+        corh->CastFrom(*corl);
+        vx->Axpy(*corh, 1.0);
+        Ah->VectorMult(*vx, resh);
+        resh->ScaleAdd(-1.0, *vb);
+        res = resh->Norm2();
+    }
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::memcpy(x, dynamic_cast<CPU_lVector<double> *>(vx)->buffer, sizeof(double) * n);
+    *outer_done = outer;
+    *inner_done = inner_total;
+    *res_out = res;
+    delete Ah; delete Al; delete vb; delete vx; delete resh; delete corh; delete resl; delete corl; delete dl;
+    return dt;
+}
+
+// FP64 Jacobi-CG over the reference's objects with an iteration cap, timed
+// (seconds, setup excluded): the plain-precision comparison.
+double ref_pcg_timed(int impl, int nthreads, int n, int nnz, const int *row, const int *col, const double *val,
+                     const double *b, double *x, double reltol, int maxits, int *iters)
+{
+    lMatrix<double> *A = make_matrix_t<double>(impl, n, nnz, row, col, val, nthreads);
+    lVector<double> *vb = make_vector_t<double>(impl, n, nthreads), *vx = make_vector_t<double>(impl, n, nthreads);
+    std::memcpy(dynamic_cast<CPU_lVector<double> *>(vb)->buffer, b, sizeof(double) * n);
+    lVector<double> *d = vb->CloneWithoutContent();
+    lPreconditioner_Jacobi<double> J;
+    J.Init(*d);
+    J.SetupOperator(*A);
+    J.Build();
+    Control ctl{maxits, 0.0, reltol, 1e6, 0.0};
+    const auto t0 = std::chrono::steady_clock::now();
+    pcg_t<double>(*A, J, *vb, *vx, ctl, 0, iters);
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::memcpy(x, dynamic_cast<CPU_lVector<double> *>(vx)->buffer, sizeof(double) * n);
+    delete A; delete vb; delete vx; delete d;
+    return dt;
+}
+
+}  // extern "C"

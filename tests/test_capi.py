@@ -1,0 +1,46 @@
+"""The C-ABI library loads and exports every entry point include/b200la.h declares."""
+import ctypes
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_header_symbols_exported(b200):
+    L = b200.lib()
+    names = b200.exported_symbols()
+    assert len(names) > 50
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+
+
+def test_symbols_via_nm(b200):
+    out = subprocess.run(["nm", "-D", "--defined-only", b200.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (b200la_\w+)", out))
+    assert set(b200.exported_symbols()) <= exported
+
+
+def test_status_strings(b200):
+    L = b200.lib()
+    assert L.b200la_status_string(0) == b"ok"
+    assert L.b200la_status_string(5) == b"malformed CSR"
+
+
+def test_create_without_gpu_fails_cleanly(b200):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    h = ctypes.c_void_p()
+    assert b200.lib().b200la_create(0, ctypes.byref(h)) == 4   # no usable sm_100 device
+    with pytest.raises(b200.B200Error):
+        b200.Platform(0)
+
+
+def test_library_has_no_oracle_dependency(b200):
+    out = subprocess.run(["nm", "-D", b200.LIB_PATH], capture_output=True, text=True).stdout
+    assert "orc_" not in out and "ref_" not in out
+    ldd = subprocess.run(["ldd", b200.LIB_PATH], capture_output=True, text=True).stdout
+    assert "oracle" not in ldd

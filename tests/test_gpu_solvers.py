@@ -1,0 +1,248 @@
+"""GPU parity of the B200 preconditioners and solvers.
+
+Bars: colours, permutations and levels bit-exact with the reference (golden);
+preconditioner applies within 1e-12 relative of the oracle; Krylov solves
+reach the same relative residual within +-5% of the reference's iteration
+count (the counts usually coincide); solutions within 1e-8 relative of the
+reference's.
+"""
+import numpy as np
+import pytest
+
+from pyoracle import control
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def pf(b200):
+    return b200.Platform(0)
+
+
+def within5(got, want):
+    return abs(got - want) <= max(1, int(np.ceil(0.05 * want)))
+
+
+def test_cg_kat(pf, b200):
+    # test/LinearAlgebra/cg.cc:35-91
+    row = np.array([0, 3, 6, 9], np.int32)
+    col = np.array([0, 1, 2] * 3, np.int32)
+    val = np.array([2, -1, 0, -1, 2, -1, 0, -1, 2.0])
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    for P in (None, b200.Preconditioner.Jacobi(pf, A)):
+        x = pf.vector(3)
+        cg = b200.CG(pf)
+        cg.SetupOperator(A)
+        cg.SetupPreconditioner(P)
+        cg.InitControl(100, 1e-300, 0.0, 1e6)
+        cg.Solve(pf.vector([1.0, -2.0, 0.0]), x)
+        np.testing.assert_allclose(x.numpy(), [-0.25, -1.5, -0.75], atol=1e-12)
+    gm = b200.GMRES(pf, 30)
+    gm.SetupOperator(A)
+    # the Krylov space is exhausted after 3 steps; the device's summation
+    # order leaves a residual of rounding size there, so the absolute stop is
+    # set above it
+    gm.InitControl(100, 1e-13, 0.0, 1e6)
+    x = pf.vector(3)
+    gm.Solve(pf.vector([1.0, -2.0, 0.0]), x)
+    np.testing.assert_allclose(x.numpy(), [-0.25, -1.5, -0.75], atol=1e-12)
+
+
+@pytest.mark.parametrize("dim,N", [(2, 32), (3, 12)])
+@pytest.mark.parametrize("name", ["none", "jacobi"])
+def test_cg_vs_reference(pf, b200, golden, dim, N, name):
+    key = f"solve{dim}d{N}"
+    row, col, val = b200.q1_assemble(dim, N)
+    b = golden[key + "_b"]
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    cg = b200.CG(pf)
+    cg.SetupOperator(A)
+    if name == "jacobi":
+        cg.SetupPreconditioner(b200.Preconditioner.Jacobi(pf, A))
+    cg.InitControl(5000, 0.0, 1e-10, 1e6)
+    x = pf.vector(len(b))
+    st = cg.Solve(pf.vector(b), x, history=5001)
+    ref_it = int(golden[f"{key}_{name}_iters"][0])
+    assert st == b200.SUCCESS_REL
+    assert within5(cg.iter(), ref_it), (cg.iter(), ref_it)
+    xr = golden[f"{key}_{name}_x"]
+    assert np.linalg.norm(x.numpy() - xr) <= 1e-8 * np.linalg.norm(xr)
+    h = golden[f"{key}_{name}_hist"]
+    k = min(len(h), len(cg.history))
+    np.testing.assert_allclose(cg.history[:k][:10], h[:k][:10], rtol=1e-10)
+
+
+@pytest.mark.parametrize("dim,N", [(2, 8), (3, 7)])
+def test_mcsgs_setup_and_apply(pf, b200, oracle, golden, dim, N):
+    key = f"{dim}d{N}_p"
+    row, col, val = golden[key + "_row"], golden[key + "_col"], golden[key + "_val"]
+    P = b200.Preconditioner.MultiColoringSGS(pf, row, col, val)
+    assert np.array_equal(P.perm, golden[key + "_mcsgs_perm"])
+    assert np.array_equal(P.block_sizes, golden[key + "_mcsgs_sizes"])
+    Ar, Ac, Av = P.A_perm.download()
+    assert np.array_equal(Ar, golden[key + "_mcsgs_Arow"]) and np.array_equal(Ac, golden[key + "_mcsgs_Acol"])
+    assert np.array_equal(Av, golden[key + "_mcsgs_Aval"])
+    r = golden[key + "_x"]
+    z = pf.vector(len(r))
+    P.ApplyPreconditioner(pf.vector(r), z)
+    zr = golden[key + "_mcsgs_z"]
+    assert np.max(np.abs(z.numpy() - zr)) <= 1e-12 * np.max(np.abs(zr))
+
+
+@pytest.mark.parametrize("dim,N", [(2, 32), (3, 12)])
+def test_mcsgs_pcg_vs_reference(pf, b200, golden, dim, N):
+    key = f"solve{dim}d{N}"
+    row, col, val = b200.q1_assemble(dim, N)
+    P = b200.Preconditioner.MultiColoringSGS(pf, row, col, val)
+    b = golden[key + "_b"][P.perm]
+    cg = b200.CG(pf)
+    cg.SetupOperator(P.A_perm)
+    cg.SetupPreconditioner(P)
+    cg.InitControl(5000, 0.0, 1e-8, 1e6)
+    x = pf.vector(len(b))
+    assert cg.Solve(pf.vector(b), x) == b200.SUCCESS_REL
+    ref_it = int(golden[f"{key}_mcsgs_iters"][0])
+    assert within5(cg.iter(), ref_it), (cg.iter(), ref_it)
+    xr = golden[f"{key}_mcsgs_x"]
+    assert np.linalg.norm(x.numpy() - xr) <= 1e-7 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("syncfree", ["0", "1"])
+@pytest.mark.parametrize("dim,N,tag", [(2, 17, "cd"), (3, 7, "p"), (2, 8, "pk")])
+def test_ilu0_ls_apply(pf, b200, golden, dim, N, tag, syncfree, monkeypatch):
+    monkeypatch.setenv("B200LA_SYNCFREE", syncfree)
+    key = f"{dim}d{N}_{tag}"
+    row, col, val = golden[key + "_row"], golden[key + "_col"], golden[key + "_val"]
+    P = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS)
+    assert np.array_equal(P.perm, golden[key + "_iluls_perm"])
+    assert np.array_equal(P.block_sizes, golden[key + "_iluls_sizes"])
+    r = golden[key + "_x"]
+    z = pf.vector(len(r))
+    for _ in range(3):   # repeated applies (epochs of the sync-free sweep)
+        P.ApplyPreconditioner(pf.vector(r), z)
+        zr = golden[key + "_iluls_z"]
+        assert np.max(np.abs(z.numpy() - zr)) <= 1e-12 * np.max(np.abs(zr))
+
+
+def test_ilu0_mc_apply(pf, b200, golden):
+    key = "2d17_cd"
+    row, col, val = golden[key + "_row"], golden[key + "_col"], golden[key + "_val"]
+    P = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_MC)
+    assert np.array_equal(P.perm, golden[key + "_ilumc_perm"])
+    r = golden[key + "_x"]
+    z = pf.vector(len(r))
+    P.ApplyPreconditioner(pf.vector(r), z)
+    zr = golden[key + "_ilumc_z"]
+    assert np.max(np.abs(z.numpy() - zr)) <= 1e-12 * np.max(np.abs(zr))
+
+
+@pytest.mark.parametrize("syncfree", ["0", "1"])
+def test_gmres_ilu_ls_vs_reference(pf, b200, golden, syncfree, monkeypatch):
+    monkeypatch.setenv("B200LA_SYNCFREE", syncfree)
+    row, col, val = b200.q1_assemble(2, 32, 1, None, 1e-3, (1.0, 0.5))
+    P = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS)
+    b = golden["gmres2d32_b"][P.perm]
+    gm = b200.GMRES(pf, 30)
+    gm.SetupOperator(P.A_perm)
+    gm.SetupPreconditioner(P)
+    gm.InitControl(1000, 0.0, 1e-9, 1e6)
+    x = pf.vector(len(b))
+    assert gm.Solve(pf.vector(b), x) == b200.SUCCESS_REL
+    ref_it = int(golden["gmres2d32_iluls_iters"][0])
+    assert within5(gm.iter(), ref_it), (gm.iter(), ref_it)
+    xr = golden["gmres2d32_iluls_x"]
+    assert np.linalg.norm(x.numpy() - xr) <= 1e-7 * np.linalg.norm(xr)
+
+
+def test_gmres_unpreconditioned_vs_reference(pf, b200, golden):
+    row, col, val = b200.q1_assemble(2, 32, 1, None, 1e-3, (1.0, 0.5))
+    b = golden["gmres2d32_b"]
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    gm = b200.GMRES(pf, 30)
+    gm.SetupOperator(A)
+    gm.InitControl(3000, 0.0, 1e-9, 1e6)
+    x = pf.vector(len(b))
+    assert gm.Solve(pf.vector(b), x) == b200.SUCCESS_REL
+    ref_it = int(golden["gmres2d32_none_iters"][0])
+    assert within5(gm.iter(), ref_it), (gm.iter(), ref_it)
+
+
+def test_mpir_vs_oracle(pf, b200, oracle):
+    dim, N = 3, 12
+    rng = np.random.default_rng(5)
+    kc = np.exp(rng.standard_normal(N ** dim))
+    row, col, val = b200.q1_assemble(dim, N, 0, kc)
+    b = b200.q1_rhs(9, dim, N)
+    ref = oracle.mpir(row, col, val, b, outer=control(50, 0, 1e-10, 1e6), inner=control(10000, 0, 1e-4, 1e6))
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    m = b200.MPIR(pf, max_outer=50)
+    m.SetupOperator(A)
+    m.InitControl(50, 0.0, 1e-10, 1e6)
+    m.InitInnerControl(10000, 0.0, 1e-4, 1e6)
+    x = pf.vector(len(b))
+    assert m.Solve(pf.vector(b), x) == b200.SUCCESS_REL
+    assert m.result.res <= 1e-10 * m.result.res0
+    assert abs(m.result.outer - ref["outer"]) <= 1
+    assert within5(m.result.iters, ref["inner_total"]), (m.result.iters, ref["inner_total"])
+    # error against the FP64 oracle solve
+    xo = oracle.pcg(row, col, val, b, precond=oracle.invdiag(row, col, val), ctl=control(10000, 0, 1e-12, 1e6))["x"]
+    assert np.linalg.norm(x.numpy() - xo) <= 1e-8 * np.linalg.norm(xo)
+
+
+def test_stop_states(pf, b200):
+    row, col, val = b200.q1_assemble(2, 16)
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    b = b200.q1_rhs(1, 2, 16)
+    cg = b200.CG(pf)
+    cg.SetupOperator(A)
+    cg.InitControl(3, 0.0, 1e-12, 1e6)
+    x = pf.vector(len(b))
+    assert cg.Solve(pf.vector(b), x) == b200.FAIL_MAXITS
+    assert cg.iter() == 3
+    # zero right-hand side: the absolute test fires at step 0
+    cg.InitControl(100, 1e-30, 1e-12, 1e6)
+    x = pf.vector(len(b))
+    assert cg.Solve(pf.vector(len(b)), x) == b200.SUCCESS_ABS
+    assert cg.iter() == 0
+
+
+def test_precond_dtype_mismatch_rejected(pf, b200):
+    row, col, val = b200.q1_assemble(2, 8)
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    A32 = A.CastFrom(b200.F32)
+    P = b200.Preconditioner.Jacobi(pf, A)
+    cg = b200.CG(pf)
+    cg.SetupOperator(A32)
+    cg.SetupPreconditioner(P)
+    with pytest.raises(b200.B200Error) as e:
+        cg.Solve(pf.vector(len(row) - 1, b200.F32), pf.vector(len(row) - 1, b200.F32))
+    assert e.value.code == 1
+
+
+def test_full_size_spmv_128cubed(pf, b200, oracle):
+    """The 3-D 128^3 operator: GPU SpMV against the oracle's at full size."""
+    row, col, val = b200.q1_assemble(3, 128)
+    n = len(row) - 1
+    x = np.random.default_rng(7).uniform(-1, 1, n)
+    y_ref = oracle.spmv(row, col, val, x)
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    yv = pf.vector(n)
+    A.VectorMult(pf.vector(x), yv)
+    sc = np.add.reduceat(np.abs(val) * np.abs(x[col]), row[:-1])
+    assert np.all(np.abs(yv.numpy() - y_ref) <= 1e-13 * sc)
+
+
+def test_full_size_cg_property(pf, b200, oracle):
+    """3-D 64^3 Jacobi-CG to 1e-10: the true residual, recomputed by the
+    oracle's SpMV, meets the tolerance."""
+    row, col, val = b200.q1_assemble(3, 64)
+    b = b200.q1_rhs(42, 3, 64)
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    cg = b200.CG(pf)
+    cg.SetupOperator(A)
+    cg.SetupPreconditioner(b200.Preconditioner.Jacobi(pf, A))
+    cg.InitControl(20000, 0.0, 1e-10, 1e6)
+    x = pf.vector(len(b))
+    assert cg.Solve(pf.vector(b), x) == b200.SUCCESS_REL
+    r = b - oracle.spmv(row, col, val, x.numpy())
+    assert np.linalg.norm(r) <= 2e-10 * np.linalg.norm(b)
