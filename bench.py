@@ -115,9 +115,17 @@ class Clocks:
 
 
 def spmv_bytes(n, nnz, vbytes):
-    """Algorithmic bytes of one SpMV: values + column indices + row pointer,
-    x read once, y written once."""
+    """Algorithmic bytes of one CSR SpMV: values + column indices + row
+    pointer, x read once, y written once."""
     return vbytes * nnz + 4 * nnz + 4 * (n + 1) + 2 * vbytes * n
+
+
+def dict_spmv_bytes(n, nnz, vbytes):
+    """Algorithmic bytes of one SpMV on the row-pattern dictionary in the
+    sliced layout: values, a 2-byte pattern id per row, one offset per
+    32-row chunk, x read once, y written once (padding of short rows and the
+    few-KB pattern table excluded)."""
+    return vbytes * nnz + 2 * n + 4 * ((n + 31) // 32 + 1) + 2 * vbytes * n
 
 
 # --------------------------------------------------------------- CPU baseline
@@ -281,7 +289,8 @@ def run_b200(args, rank, world, local_rank, dist):
         for _ in range(reps):
             L.b200la_spmv_dot(pf.h, A.h, xx.ptr, yy.ptr, ctypes.c_void_p(d.data_ptr()))
         t_ms = pf.timer_stop() / reps
-        by = spmv_bytes(n, nnz, vbytes)
+        uses_dict = A.info()["uses_pattern_dictionary"]
+        by = dict_spmv_bytes(n, nnz, vbytes) if uses_dict else spmv_bytes(n, nnz, vbytes)
         return by, t_ms, by / (t_ms * 1e-3) / 1e9
 
     by64, t64, gbs64 = spmv_rate(A64, 8)
@@ -339,12 +348,13 @@ def run_b200(args, rank, world, local_rank, dist):
                   "relres_true": relres, "err_vs_fp64_solution": err},
         "fp64_cg": {"ms": fp64_ms, "iters": fp64_iters, "err_vs_fp64_solution": err64},
         "mixed_speedup_vs_fp64": fp64_ms / ms_step,
-        "spmv": {"fp64_gbs": gbs64, "fp64_us": t64 * 1e3, "fp64_bytes": by64,
-                 "fp32_gbs": gbs32, "fp32_us": t32 * 1e3, "fp32_bytes": by32,
-                 "fp64_frac_of_peak": gbs64 / peak},
-        "roofline": {"bound": "hbm", "kernel": "spmv_tile_kernel<float, EPI_DOT_X> (FP32 SpMV + p.Ap of the inner CG)",
+        "spmv": {"fp64_csr_gbs": gbs64, "fp64_csr_us": t64 * 1e3, "fp64_csr_bytes": by64,
+                 "fp64_csr_frac_of_peak": gbs64 / peak,
+                 "fp32_dict_gbs": gbs32, "fp32_dict_us": t32 * 1e3, "fp32_dict_bytes": by32},
+        "roofline": {"bound": "hbm",
+                     "kernel": "spmv_sell_kernel<float, EPI_DOT_X>: FP32 dictionary SpMV + p.Ap of the inner CG",
                      "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,
-                     "peak_source": peak_kind, "traffic": None},
+                     "peak_source": peak_kind, "bytes_per_launch": by32, "traffic": None},
         "gpu_launches": launches,
         "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n, "matches_device_run": e2e_ok},

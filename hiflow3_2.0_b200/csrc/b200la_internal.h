@@ -54,6 +54,15 @@ struct b200la_csr {
     int *pat_off = nullptr, *pat_delta = nullptr;
     int npat = 0, ndelta = 0;
     bool use_pat = false;             // SpMV runs on the dictionary
+    // gather lines of the dictionary (null when there are too many)
+    int *line_start = nullptr, *line_span = nullptr, *entry_line = nullptr, *entry_lo = nullptr;
+    int nlines = 0, span_sum = 0;
+    int stage_x = 0;                  // x staged per row tile (B200LA_STAGE_X=1 at creation)
+    int l2hint = 0;                   // L2 priorities on SpMV loads (B200LA_L2HINT bits: 1 stream first, 2 x last)
+    // sliced (SELL-32) copy of the values for the dictionary SpMV
+    int *sell_off = nullptr;
+    void *sell_val = nullptr;
+    size_t sell_len = 0;
 };
 
 struct b200la_precond {

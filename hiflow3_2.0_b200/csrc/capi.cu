@@ -80,6 +80,17 @@ CsrView csr_view(const b200la_csr *A)
     v.npat = A->npat;
     v.ndelta = A->ndelta;
     v.use_pat = A->pid != nullptr && A->use_pat;
+    v.line_start = A->line_start;
+    v.line_span = A->line_span;
+    v.entry_line = A->entry_line;
+    v.entry_lo = A->entry_lo;
+    v.nlines = A->nlines;
+    v.span_sum = A->span_sum;
+    v.stage_x = A->stage_x;
+    v.l2hint = A->l2hint;
+    v.sell_off = A->sell_off;
+    v.sell_val = A->sell_val;
+    v.n_cols = A->m;
     return v;
 }
 
@@ -131,11 +142,11 @@ extern "C" int b200la_create(int device, b200la_ctx **out)
     cudaError_t e;
     if ((e = cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking)) ||
         (e = cudaMalloc(&ctx->partials, sizeof(double) * 8 * kMaxGrid)) ||
-        (e = cudaMalloc(&ctx->ticket, sizeof(unsigned) * 4)) || (e = cudaMalloc(&ctx->dev_err, sizeof(int))) ||
+        (e = cudaMalloc(&ctx->ticket, sizeof(unsigned) * kTicketWords)) || (e = cudaMalloc(&ctx->dev_err, sizeof(int))) ||
         (e = cudaMalloc(&ctx->st, sizeof(DevState))) || (e = cudaMalloc(&ctx->dscal, sizeof(double) * 256)) ||
         (e = cudaMallocHost(&ctx->st_host, sizeof(DevState))) ||
         (e = cudaMallocHost(&ctx->hscal, sizeof(double) * 256)) || (e = cudaEventCreate(&ctx->ev0)) ||
-        (e = cudaEventCreate(&ctx->ev1)) || (e = cudaMemset(ctx->ticket, 0, sizeof(unsigned) * 4)) ||
+        (e = cudaEventCreate(&ctx->ev1)) || (e = cudaMemset(ctx->ticket, 0, sizeof(unsigned) * kTicketWords)) ||
         (e = cudaMemset(ctx->dev_err, 0, sizeof(int))) || (e = spmv_configure()) || (e = sweeps_configure())) {
         ctx->stream = ctx->own_stream;
         b200la_destroy(ctx);
@@ -355,6 +366,69 @@ static void build_segment(const int *row, int s0, int s1, int lg, int cap, std::
     segs.push_back(sg);
 }
 
+// (Re)build the sliced copy of A's values from A->val (device); needs the
+// dictionary.  Chunk c holds 32 * (longest row of the chunk) values.
+static int build_sell(b200la_ctx *ctx, b200la_csr *A)
+{
+    if (!A->pid || !A->use_pat || A->n == 0) return B200LA_OK;
+    const size_t es = dsize(A->dtype);
+    cudaError_t e;
+    if (!A->sell_off) {
+        const int nch = (A->n + 31) / 32;
+        std::vector<int> off(nch + 1, 0);
+        for (int c = 0; c < nch; ++c) {
+            int L = 0;
+            for (int r = 32 * c; r < std::min(A->n, 32 * c + 32); ++r) L = std::max(L, A->h_row[r + 1] - A->h_row[r]);
+            off[c + 1] = off[c] + 32 * L;
+        }
+        A->sell_len = (size_t)off[nch];
+        if ((e = cudaMalloc(&A->sell_off, sizeof(int) * (nch + 1))) ||
+            (e = cudaMalloc(&A->sell_val, es * std::max<size_t>(A->sell_len, 32))) ||
+            (e = cudaMemcpy(A->sell_off, off.data(), sizeof(int) * (nch + 1), cudaMemcpyHostToDevice)))
+            return ctx_fail(ctx, B200LA_ERR_ALLOC, "sliced layout", e);
+        A->bytes += sizeof(int) * (nch + 1) + es * A->sell_len;
+    }
+    if ((e = cudaMemsetAsync(A->sell_val, 0, es * std::max<size_t>(A->sell_len, 32), ctx->stream)) ||
+        (e = launch_csr_to_sell(A->dtype, A->n, A->row, A->val, A->sell_off, A->sell_val, ctx->stream)) ||
+        (e = cudaStreamSynchronize(ctx->stream)))
+        return ctx_fail(ctx, B200LA_ERR_CUDA, "sliced layout", e);
+    return B200LA_OK;
+}
+
+static int upload_lines(b200la_ctx *ctx, b200la_csr *A, const std::vector<int> &ls, const std::vector<int> &lsp,
+                        const std::vector<int> &el, const std::vector<int> &elo)
+{
+    cudaError_t e;
+    const size_t L = ls.size(), E = std::max<size_t>(el.size(), 1);
+    if ((e = cudaMalloc(&A->line_start, sizeof(int) * L)) || (e = cudaMalloc(&A->line_span, sizeof(int) * L)) ||
+        (e = cudaMalloc(&A->entry_line, sizeof(int) * E)) || (e = cudaMalloc(&A->entry_lo, sizeof(int) * E)) ||
+        (e = cudaMemcpy(A->line_start, ls.data(), sizeof(int) * L, cudaMemcpyHostToDevice)) ||
+        (e = cudaMemcpy(A->line_span, lsp.data(), sizeof(int) * L, cudaMemcpyHostToDevice)) ||
+        (!el.empty() && (e = cudaMemcpy(A->entry_line, el.data(), sizeof(int) * el.size(), cudaMemcpyHostToDevice))) ||
+        (!el.empty() && (e = cudaMemcpy(A->entry_lo, elo.data(), sizeof(int) * el.size(), cudaMemcpyHostToDevice))))
+        return ctx_fail(ctx, B200LA_ERR_ALLOC, "csr_create: gather lines", e);
+    A->nlines = (int)L;
+    A->span_sum = 0;
+    for (int s : lsp) A->span_sum += s;
+    return B200LA_OK;
+}
+
+static int copy_lines(b200la_ctx *ctx, const b200la_csr *A, b200la_csr *B)
+{
+    B->line_start = B->line_span = B->entry_line = B->entry_lo = nullptr;
+    if (!A->line_start) return B200LA_OK;
+    cudaError_t e;
+    const size_t L = A->nlines, E = std::max(A->ndelta, 1);
+    if ((e = cudaMalloc(&B->line_start, sizeof(int) * L)) || (e = cudaMalloc(&B->line_span, sizeof(int) * L)) ||
+        (e = cudaMalloc(&B->entry_line, sizeof(int) * E)) || (e = cudaMalloc(&B->entry_lo, sizeof(int) * E)) ||
+        (e = cudaMemcpy(B->line_start, A->line_start, sizeof(int) * L, cudaMemcpyDeviceToDevice)) ||
+        (e = cudaMemcpy(B->line_span, A->line_span, sizeof(int) * L, cudaMemcpyDeviceToDevice)) ||
+        (e = cudaMemcpy(B->entry_line, A->entry_line, sizeof(int) * E, cudaMemcpyDeviceToDevice)) ||
+        (e = cudaMemcpy(B->entry_lo, A->entry_lo, sizeof(int) * E, cudaMemcpyDeviceToDevice)))
+        return ctx_fail(ctx, B200LA_ERR_ALLOC, "csr_cast: gather lines", e);
+    return B200LA_OK;
+}
+
 int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row, const int *col,
                const void *val, int dtype, int n_seg, const int *seg_off, b200la_csr **out)
 {
@@ -378,6 +452,7 @@ int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row,
     A->dtype = dtype;
     A->lg = lanes_log2(n_rows, nnz);
     A->cfg = spmv_cfg_choice();
+    if (const char *h = std::getenv("B200LA_L2HINT")) A->l2hint = std::atoi(h);
     const int cap = spmv_tile_cap(A->cfg);
     A->h_row.assign(row, row + n_rows + 1);
     std::vector<Tile> tiles;
@@ -441,6 +516,21 @@ int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row,
         }
         A->bytes += sizeof(uint16_t) * n_rows + sizeof(int) * (poff.size() + pdel.size());
         A->use_pat = pattern_policy(dtype);
+        if (const char *sx = std::getenv("B200LA_STAGE_X")) A->stage_x = std::atoi(sx);
+        std::vector<int> ls, lsp, el, elo;
+        host::pattern_lines(pdel, ls, lsp, el, elo);
+        if (!ls.empty() && (int)ls.size() <= kMaxGatherLines) {
+            int rc = upload_lines(ctx, A, ls, lsp, el, elo);
+            if (rc) {
+                b200la_csr_destroy(A);
+                return rc;
+            }
+        }
+        const int rc = build_sell(ctx, A);
+        if (rc) {
+            b200la_csr_destroy(A);
+            return rc;
+        }
     }
     *out = A;
     return B200LA_OK;
@@ -472,6 +562,12 @@ extern "C" int b200la_csr_destroy(b200la_csr *A)
     if (A->pid) cudaFree(A->pid);
     if (A->pat_off) cudaFree(A->pat_off);
     if (A->pat_delta) cudaFree(A->pat_delta);
+    if (A->line_start) cudaFree(A->line_start);
+    if (A->line_span) cudaFree(A->line_span);
+    if (A->entry_line) cudaFree(A->entry_line);
+    if (A->entry_lo) cudaFree(A->entry_lo);
+    if (A->sell_off) cudaFree(A->sell_off);
+    if (A->sell_val) cudaFree(A->sell_val);
     delete A;
     return B200LA_OK;
 }
@@ -489,6 +585,10 @@ extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, 
     B->pid = nullptr;
     B->pat_off = nullptr;
     B->pat_delta = nullptr;
+    B->line_start = B->line_span = B->entry_line = B->entry_lo = nullptr;
+    B->sell_off = nullptr;
+    B->sell_val = nullptr;
+    B->sell_len = 0;
     const size_t pad = 8, es = dsize(dtype);
     cudaError_t e;
     if (A->pid) {
@@ -503,6 +603,11 @@ extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, 
             return ctx_fail(ctx, B200LA_ERR_ALLOC, "csr_cast: pattern dictionary", e);
         }
         B->use_pat = pattern_policy(dtype);
+        const int rc = copy_lines(ctx, A, B);
+        if (rc) {
+            b200la_csr_destroy(B);
+            return rc;
+        }
     }
     if ((e = cudaMalloc(&B->row, sizeof(int) * (A->n + 1 + pad))) ||
         (e = cudaMalloc(&B->col, sizeof(int) * (A->nnz + pad))) ||
@@ -524,6 +629,11 @@ extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, 
         (e = cudaStreamSynchronize(s))) {
         b200la_csr_destroy(B);
         return ctx_fail(ctx, B200LA_ERR_CUDA, "csr_cast", e);
+    }
+    const int rc = build_sell(ctx, B);
+    if (rc) {
+        b200la_csr_destroy(B);
+        return rc;
     }
     *out = B;
     return B200LA_OK;
@@ -567,7 +677,7 @@ extern "C" int b200la_csr_set_values(b200la_ctx *ctx, b200la_csr *A, const void 
     if (!ctx || !A || (A->nnz && !val)) return B200LA_ERR_ARG;
     if (A->nnz) CK(cudaMemcpyAsync(A->val, val, dsize(A->dtype) * A->nnz, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    return B200LA_OK;
+    return build_sell(ctx, A);
 }
 
 extern "C" int b200la_csr_invdiag(b200la_ctx *ctx, const b200la_csr *A, void *out)

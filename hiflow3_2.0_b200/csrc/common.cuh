@@ -76,6 +76,51 @@ __device__ __forceinline__ uint64_t l2_evict_first_policy()
     return pol;
 }
 
+// L2 eviction policies for individual loads.  A sparse operator streams its
+// values and indices once per product while the gathered vector is re-read
+// by every row: the stream is marked evict-first (and skips L1) and the
+// vector evict-last, so that vector traffic of the kernels between two
+// products cannot push the vector out of L2.  kind: 0 normal, 1 first, 2 last.
+__device__ __forceinline__ uint64_t l2_policy(int kind)
+{
+    uint64_t p;
+    if (kind == 1) asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    else if (kind == 2) asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    else asm("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ double ld_stream(const double *a, uint64_t pol)
+{
+    double v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_stream(const float *a, uint64_t pol)
+{
+    float v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ int ld_stream(const int *a, uint64_t pol)
+{
+    int v;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ double ld_keep(const double *a, uint64_t pol)
+{
+    double v;
+    asm("ld.global.nc.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ float ld_keep(const float *a, uint64_t pol)
+{
+    float v;
+    asm("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol));
+    return v;
+}
+
 // Global -> shared bulk copy completing on an mbarrier.  dst, src 16-byte
 // aligned; bytes a multiple of 16.  The L2 policy marks the streamed matrix
 // as evict-first so the gathered vector stays resident in L2.
@@ -87,6 +132,29 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
         " [%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
         "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(policy)
         : "memory");
+}
+
+// True when the stop-state word *gate is set (a solver's IterateControl
+// state has left "iterate").  One thread per CTA reads it (through L2) and
+// broadcasts it: a load by every thread of the grid on one address would
+// serialise in L2.  Must be called by all threads of the CTA.
+__device__ __forceinline__ bool gate_closed(const int *gate)
+{
+    if (!gate) return false;
+    __shared__ int s_gate;
+    if (threadIdx.x == 0) s_gate = __ldcg(gate);
+    __syncthreads();
+    return s_gate != 0;
+}
+
+// One double read once per CTA and broadcast (scalars of the recurrences).
+__device__ __forceinline__ double cta_scalar(const double *p)
+{
+    __shared__ double s_val;
+    __syncthreads();
+    if (threadIdx.x == 0) s_val = __ldcg(p);
+    __syncthreads();
+    return s_val;
 }
 
 template <typename T>
@@ -121,10 +189,19 @@ __device__ __forceinline__ void block_sum(double (&v)[NQ], double *sm)
     __syncthreads();
 }
 
+// Ticket words: kTicketGroups group counters and one final counter, each on
+// its own 128-byte line (a single counter hit by ~1000 CTAs serialises for
+// tens of microseconds).
+constexpr int kTicketGroups = 32;
+constexpr int kTicketStride = 32;   // unsigned words between counters
+constexpr int kTicketWords = (kTicketGroups + 1) * kTicketStride;
+
 // Grid-wide deterministic reduction tail.  Each CTA passes its per-thread
-// values; partials is [NQ][kMaxGrid]; ticket is reset to 0 by the last CTA.
-// Returns true on thread 0 of the last CTA, with out[] holding the totals
-// summed in CTA order.
+// values; partials is [NQ][kMaxGrid].  CTAs report to one of kTicketGroups
+// group counters; the last CTA of a group reports to the final counter; the
+// CTA that completes the final counter sums all partials.  Counters are reset
+// by the CTAs that complete them.  Returns true on thread 0 of the last CTA,
+// with out[] holding the totals in a fixed order.
 template <int NQ>
 __device__ __forceinline__ bool grid_reduce(double (&v)[NQ], double *partials, unsigned *ticket,
                                             double (&out)[NQ])
@@ -136,8 +213,20 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NQ], double *partials, u
 #pragma unroll
         for (int q = 0; q < NQ; ++q) partials[q * kMaxGrid + blockIdx.x] = v[q];
         __threadfence();
-        const unsigned t = atomicAdd(ticket, 1u);
-        last = (t == gridDim.x - 1);
+        const unsigned ngroups = gridDim.x < kTicketGroups ? gridDim.x : kTicketGroups;
+        const unsigned g = blockIdx.x % ngroups;
+        const unsigned gsize = (gridDim.x - g + ngroups - 1) / ngroups;
+        unsigned *gc = ticket + kTicketStride * (1 + g);
+        bool l = false;
+        if (atomicAdd(gc, 1u) == gsize - 1) {
+            *gc = 0u;
+            __threadfence();
+            if (atomicAdd(ticket, 1u) == ngroups - 1) {
+                *ticket = 0u;
+                l = true;
+            }
+        }
+        last = l;
     }
     __syncthreads();
     if (!last) return false;
@@ -156,7 +245,6 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NQ], double *partials, u
     if (threadIdx.x == 0) {
 #pragma unroll
         for (int q = 0; q < NQ; ++q) out[q] = w[q];
-        *ticket = 0u;
     }
     return threadIdx.x == 0;
 }

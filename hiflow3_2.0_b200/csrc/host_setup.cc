@@ -451,6 +451,31 @@ bool row_patterns(int n, const int *row, const int *col, int max_pat, int max_de
     return true;
 }
 
+void pattern_lines(const std::vector<int> &pat_delta, std::vector<int> &line_start, std::vector<int> &line_span,
+                   std::vector<int> &entry_line, std::vector<int> &entry_lo)
+{
+    std::vector<int> d(pat_delta);
+    std::sort(d.begin(), d.end());
+    d.erase(std::unique(d.begin(), d.end()), d.end());
+    line_start.clear();
+    line_span.clear();
+    for (size_t i = 0; i < d.size(); ++i) {
+        if (i == 0 || d[i] != d[i - 1] + 1) {
+            line_start.push_back(d[i]);
+            line_span.push_back(0);
+        } else {
+            line_span.back() = d[i] - line_start.back();
+        }
+    }
+    entry_line.resize(pat_delta.size());
+    entry_lo.resize(pat_delta.size());
+    for (size_t k = 0; k < pat_delta.size(); ++k) {
+        const int l = (int)(std::upper_bound(line_start.begin(), line_start.end(), pat_delta[k]) - line_start.begin()) - 1;
+        entry_line[k] = l;
+        entry_lo[k] = pat_delta[k] - line_start[l];
+    }
+}
+
 int validate_csr(int n_rows, int n_cols, int nnz, const int *row, const int *col, long long *bad_at)
 {
     if (n_rows < 0 || n_cols < 0 || nnz < 0) return -1;

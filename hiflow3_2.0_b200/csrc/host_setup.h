@@ -60,6 +60,14 @@ void dropoffs(Csr &A, const std::vector<int> &block_off);
 bool row_patterns(int n, const int *row, const int *col, int max_pat, int max_delta, std::vector<uint16_t> &pid,
                   std::vector<int> &pat_off, std::vector<int> &pat_delta);
 
+// Gather lines of a pattern table: the union of all pattern offsets, split
+// into runs of consecutive integers [line_start[l], line_start[l] + line_span[l]].
+// For every stored offset, its run (entry_line) and its position in the run
+// (entry_lo).  A tile of R consecutive rows then reads x only on the lines
+// shifted by the tile's first row, each R + span long.
+void pattern_lines(const std::vector<int> &pat_delta, std::vector<int> &line_start, std::vector<int> &line_span,
+                   std::vector<int> &entry_line, std::vector<int> &entry_lo);
+
 // Validation of a CSR before upload: row monotone, row[0] == 0, columns in
 // [0, n_cols).  Returns 0 or a negative code naming the first violation.
 int validate_csr(int n_rows, int n_cols, int nnz, const int *row, const int *col, long long *bad_at);

@@ -11,6 +11,21 @@ namespace {
 
 // ------------------------------------------------------------------ BLAS1
 
+// 16-byte vectors: 2 doubles or 4 floats per load / store.
+template <typename T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+    using type = double2;
+    static constexpr int W = 2;
+};
+template <>
+struct Vec16<float> {
+    using type = float4;
+    static constexpr int W = 4;
+};
+
+
 inline int stream_grid(const Scratch *s, int n, int per_thread = 4)
 {
     int g = (n + kBlock * per_thread - 1) / (kBlock * per_thread);
@@ -24,10 +39,23 @@ template <typename T>
 __global__ void __launch_bounds__(kBlock) dot_kernel(int n, const T *__restrict__ x, const T *__restrict__ y,
                                                      double *out, bool sqrt_out, const int *gate, Scratch sc)
 {
-    if (gate && *reinterpret_cast<const volatile int *>(gate) != 0) return;
-    T a = T(0);
-    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) a += x[i] * y[i];
-    double v[1] = {(double)a}, o[1];
+    if (gate_closed(gate)) return;
+    using V = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::W;
+    const int tid = blockIdx.x * kBlock + threadIdx.x, stride = gridDim.x * kBlock;
+    double a = 0.0;
+    const bool vec = ((reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(y)) & 15) == 0;
+    const int nv = vec ? n / W : 0;
+    for (int iv = tid; iv < nv; iv += stride) {
+        const V xv = __ldg(reinterpret_cast<const V *>(x) + iv), yv = __ldg(reinterpret_cast<const V *>(y) + iv);
+        const T *xe = reinterpret_cast<const T *>(&xv), *ye = reinterpret_cast<const T *>(&yv);
+        T s = T(0);
+#pragma unroll
+        for (int k = 0; k < W; ++k) s += xe[k] * ye[k];
+        a += (double)s;
+    }
+    for (int i = nv * W + tid; i < n; i += stride) a += (double)(x[i] * y[i]);
+    double v[1] = {a}, o[1];
     if (grid_reduce<1>(v, sc.partials, sc.ticket, o)) *out = sqrt_out ? sqrt(o[0]) : o[0];
 }
 
@@ -81,31 +109,57 @@ __global__ void scatter_kernel(int n, const int *__restrict__ idx, const T *__re
 
 // ------------------------------------------------------------------ Krylov
 
+// x += alpha p; r -= alpha Ap; rr += r^2 and (Jacobi) rz += r (invd r) for
+// element i, partial sums of one 16-byte vector kept in T, then folded to double.
+template <typename T>
+__device__ __forceinline__ void cg_update_elem(T alpha, T &x, T &r, T p, T ap, T d, bool jac, T &rr, T &rz)
+{
+    x += alpha * p;
+    r -= alpha * ap;
+    rr += r * r;
+    if (jac) rz += r * (r * d);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(kBlock) cg_update_kernel(int n, int precond, T *__restrict__ x, T *__restrict__ r,
                                                            const T *__restrict__ p, const T *__restrict__ Ap,
                                                            const T *__restrict__ invd, DevState *st, Scratch sc)
 {
-    if (*reinterpret_cast<volatile int *>(&st->status) != kIterate) return;
-    const T alpha = (T)st->alpha;
+    if (gate_closed(&st->status)) return;
+    using V = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::W;
+    const T alpha = (T)cta_scalar(&st->alpha);
+    const bool jac = precond == 1;
     double rr = 0.0, rz = 0.0;
-    T prr = T(0), prz = T(0);
-    int cnt = 0;
-    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
-        x[i] += alpha * p[i];
-        const T ri = r[i] - alpha * Ap[i];
-        r[i] = ri;
-        prr += ri * ri;
-        if (precond == 1) prz += ri * (ri * invd[i]);
-        // FP32 partial sums are folded into double every 8 elements
-        if (sizeof(T) == 4 && ++cnt == 8) {
-            rr += (double)prr; rz += (double)prz;
-            prr = prz = T(0);
-            cnt = 0;
-        }
+    const uintptr_t al = reinterpret_cast<uintptr_t>(x) | reinterpret_cast<uintptr_t>(r) |
+                         reinterpret_cast<uintptr_t>(p) | reinterpret_cast<uintptr_t>(Ap) |
+                         (jac ? reinterpret_cast<uintptr_t>(invd) : 0);
+    const int nv = (al & 15) ? 0 : n / W;
+    const int tid = blockIdx.x * kBlock + threadIdx.x, stride = gridDim.x * kBlock;
+    for (int iv = tid; iv < nv; iv += stride) {
+        V xv = reinterpret_cast<const V *>(x)[iv], rv = reinterpret_cast<const V *>(r)[iv];
+        const V pv = reinterpret_cast<const V *>(p)[iv], av = __ldcs(reinterpret_cast<const V *>(Ap) + iv);
+        V dv = pv;
+        if (jac) dv = __ldg(reinterpret_cast<const V *>(invd) + iv);
+        T *xe = reinterpret_cast<T *>(&xv), *re = reinterpret_cast<T *>(&rv);
+        const T *pe = reinterpret_cast<const T *>(&pv), *ae = reinterpret_cast<const T *>(&av),
+                *de = reinterpret_cast<const T *>(&dv);
+        T prr = T(0), prz = T(0);
+#pragma unroll
+        for (int k = 0; k < W; ++k) cg_update_elem(alpha, xe[k], re[k], pe[k], ae[k], de[k], jac, prr, prz);
+        reinterpret_cast<V *>(x)[iv] = xv;
+        reinterpret_cast<V *>(r)[iv] = rv;
+        rr += (double)prr;
+        rz += (double)prz;
     }
-    rr += (double)prr;
-    rz += (double)prz;
+    for (int i = nv * W + tid; i < n; i += stride) {
+        T xi = x[i], ri = r[i], prr = T(0), prz = T(0);
+        cg_update_elem(alpha, xi, ri, p[i], Ap[i], jac ? invd[i] : T(0), jac, prr, prz);
+        x[i] = xi;
+        r[i] = ri;
+        rr += (double)prr;
+        rz += (double)prz;
+    }
     double v[2] = {rr, rz}, o[2];
     if (grid_reduce<2>(v, sc.partials, sc.ticket, o)) {
         const int it = st->iter + 1;
@@ -128,9 +182,26 @@ template <typename T>
 __global__ void cg_pupdate_kernel(int n, int precond, T *__restrict__ p, const T *__restrict__ r,
                                   const T *__restrict__ invd, const T *__restrict__ z, DevState *st)
 {
-    if (*reinterpret_cast<volatile int *>(&st->status) != kIterate) return;
-    const T beta = (T)st->beta;
-    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+    if (gate_closed(&st->status)) return;
+    using V = typename Vec16<T>::type;
+    constexpr int W = Vec16<T>::W;
+    const T beta = (T)cta_scalar(&st->beta);
+    const uintptr_t al = reinterpret_cast<uintptr_t>(p) | reinterpret_cast<uintptr_t>(precond == 2 ? z : r) |
+                         (precond == 1 ? reinterpret_cast<uintptr_t>(invd) : 0);
+    const int nv = (al & 15) ? 0 : n / W;
+    const int tid = blockIdx.x * kBlock + threadIdx.x, stride = gridDim.x * kBlock;
+    for (int iv = tid; iv < nv; iv += stride) {
+        V pv = reinterpret_cast<const V *>(p)[iv];
+        const V rv = reinterpret_cast<const V *>(precond == 2 ? z : r)[iv];
+        V dv = rv;
+        if (precond == 1) dv = __ldg(reinterpret_cast<const V *>(invd) + iv);
+        T *pe = reinterpret_cast<T *>(&pv);
+        const T *re = reinterpret_cast<const T *>(&rv), *de = reinterpret_cast<const T *>(&dv);
+#pragma unroll
+        for (int k = 0; k < W; ++k) pe[k] = beta * pe[k] + (precond == 1 ? re[k] * de[k] : re[k]);
+        reinterpret_cast<V *>(p)[iv] = pv;
+    }
+    for (int i = nv * W + tid; i < n; i += stride) {
         const T zi = (precond == 1) ? r[i] * invd[i] : (precond == 0 ? r[i] : z[i]);
         p[i] = beta * p[i] + zi;
     }
@@ -156,7 +227,7 @@ template <typename T>
 __global__ void __launch_bounds__(kBlock) cg_rz_kernel(int n, const T *__restrict__ r, const T *__restrict__ z,
                                                        DevState *st, Scratch sc)
 {
-    if (*reinterpret_cast<volatile int *>(&st->status) != kIterate) return;
+    if (gate_closed(&st->status)) return;
     double a = 0.0;
     for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) a += (double)(r[i] * z[i]);
     double v[1] = {a}, o[1];
@@ -185,8 +256,8 @@ template <typename T>
 __global__ void axpy_dev_kernel(int n, const double *coef, double sign, const T *__restrict__ x, T *__restrict__ y,
                                 const int *gate)
 {
-    if (gate && *reinterpret_cast<const volatile int *>(gate) != 0) return;
-    const T a = (T)(sign * *coef);
+    if (gate_closed(gate)) return;
+    const T a = (T)(sign * cta_scalar(coef));
     for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] += a * x[i];
 }
 
@@ -194,8 +265,9 @@ template <typename T>
 __global__ void scale_dev_kernel(int n, const double *coef, bool reciprocal, const T *__restrict__ x,
                                  T *__restrict__ y, const int *gate)
 {
-    if (gate && *reinterpret_cast<const volatile int *>(gate) != 0) return;
-    const T a = (T)(reciprocal ? 1.0 / *coef : *coef);
+    if (gate_closed(gate)) return;
+    const double cv = cta_scalar(coef);
+    const T a = (T)(reciprocal ? 1.0 / cv : cv);
     for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) y[i] = a * x[i];
 }
 

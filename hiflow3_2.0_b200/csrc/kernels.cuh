@@ -88,10 +88,23 @@ struct CsrView {
     const int *pat_off;
     const int *pat_delta;
     int npat, ndelta, use_pat;
+    // gather lines of the dictionary (x staged in shared memory per row tile
+    // when nlines > 0): see host::pattern_lines
+    const int *line_start, *line_span, *entry_line, *entry_lo;
+    int nlines, span_sum;
+    int stage_x;     // stage x through shared memory (B200LA_STAGE_X=1)
+    int l2hint;      // bit 0: evict-first matrix stream, bit 1: evict-last gathers (B200LA_L2HINT)
+    // sliced layout of the dictionary operator (null when absent): chunk c of
+    // 32 rows holds its values k-major at sell_val[sell_off[c] + 32 k + lane]
+    const int *sell_off;
+    const void *sell_val;
+    int n_cols;      // length of x
 };
 
 constexpr int kMaxPatterns = 1024;
 constexpr int kMaxPatternDeltas = 6144;
+constexpr int kMaxGatherLines = 64;
+constexpr int kMaxStagedX = 6144;     // staged x values per row tile
 
 struct SpmvOp {
     int epi = EPI_SET;
@@ -114,6 +127,9 @@ struct Scratch {
 };
 
 cudaError_t spmv_configure();
+// Scatter CSR values (row order) into the sliced layout (zero-filled before).
+cudaError_t launch_csr_to_sell(int dtype, int n, const int *row, const void *val, const int *sell_off, void *sv,
+                               cudaStream_t st);
 cudaError_t launch_spmv(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st);
 
 // ---- BLAS1 (dtype 0 double, 1 float; scalars in double) ----

@@ -163,9 +163,24 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
     };
 
     const int K = batch_size();
-    cudaGraphExec_t exec;
+    cudaGraphExec_t exec = nullptr;
     int nodes = 0;
-    rc = get_graph(
+    const bool no_graph = std::getenv("B200LA_NOGRAPH") != nullptr;
+    if (no_graph) {
+        // batches launched kernel by kernel on the stream (same work, no graph)
+        SK(cudaMemcpyAsync(hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+        SK(cudaStreamSynchronize(ctx->stream));
+        const long long max_b = (long long)ctl->maxits / K + 2;
+        for (long long bt = 0; hs->status == kIterate && bt < max_b; ++bt) {
+            for (int k = 0; k < K; ++k) {
+                rc = iteration();
+                if (rc) return rc;
+            }
+            SK(cudaMemcpyAsync(hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+            SK(cudaStreamSynchronize(ctx->stream));
+        }
+    }
+    if (!no_graph) rc = get_graph(
         ctx, {A, P, b, x, w.r, w.p, w.Ap, w.z, (const void *)(intptr_t)K, (const void *)(intptr_t)pc, ctx->stream},
         [&]() -> int {
             for (int k = 0; k < K; ++k) {
@@ -180,7 +195,7 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
     SK(cudaStreamSynchronize(ctx->stream));
     long long graph_launches = 0;
     const long long max_batches = (long long)ctl->maxits / K + 2;
-    for (long long bt = 0; hs->status == kIterate && bt < max_batches; ++bt) {
+    for (long long bt = 0; !no_graph && hs->status == kIterate && bt < max_batches; ++bt) {
         SK(cudaGraphLaunch(exec, ctx->stream));
         graph_launches += nodes;
         SK(cudaMemcpyAsync(hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));

@@ -113,7 +113,7 @@ __device__ __forceinline__ void long_rows(const CsrView &A, const Seg &seg, cons
 template <typename T, int EPI, int CAP, int ST, int MINB>
 __global__ void __launch_bounds__(kBlock, MINB) spmv_tile_kernel(CsrView A, Seg seg, SpmvOp op, Scratch sc)
 {
-    if (op.gate && *reinterpret_cast<const volatile int *>(op.gate) != 0) return;
+    if (gate_closed(op.gate)) return;
     extern __shared__ __align__(128) unsigned char smem[];
     using L = TileSmem<CAP>;
     constexpr int kVB = L::template val_bytes<T>();
@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(kBlock, MINB) spmv_tile_kernel(CsrView A, Seg 
 template <typename T, int EPI>
 __global__ void __launch_bounds__(kBlock) spmv_direct_kernel(CsrView A, Seg seg, SpmvOp op, Scratch sc)
 {
-    if (op.gate && *reinterpret_cast<const volatile int *>(op.gate) != 0) return;
+    if (gate_closed(op.gate)) return;
     const int *__restrict__ row = A.row;
     const int *__restrict__ col = A.col;
     const T *__restrict__ val = static_cast<const T *>(A.val);
@@ -201,15 +201,20 @@ __global__ void __launch_bounds__(kBlock) spmv_direct_kernel(CsrView A, Seg seg,
     const int rpb = kBlock >> A.lg;
     const int grp = threadIdx.x >> A.lg;
     const int lane_g = threadIdx.x & (G - 1);
+    const uint64_t pol_s = l2_policy(A.l2hint & 1 ? 1 : 0), pol_x = l2_policy(A.l2hint & 2 ? 2 : 0);
     double acc = 0.0;
     for (int base = seg.r0 + blockIdx.x * rpb; base < seg.r1; base += gridDim.x * rpb) {
         const int r = base + grp;
         const bool active = r < seg.r1;
         T s = T(0);
         if (active) {
-            const int j1 = __ldg(row + r + 1);
+            const int j0 = __ldg(row + r), j1 = __ldg(row + r + 1);
+            // the group's G-element windows start on a multiple of G, so each
+            // window is one aligned segment (a 32-byte sector for 4 doubles);
+            // elements outside the row are masked
 #pragma unroll 4
-            for (int j = __ldg(row + r) + lane_g; j < j1; j += G) s += __ldcs(val + j) * __ldg(x + __ldcs(col + j));
+            for (int j = (j0 & ~(G - 1)) + lane_g; j < j1; j += G)
+                if (j >= j0) s += ld_stream(val + j, pol_s) * ld_keep(x + ld_stream(col + j, pol_s), pol_x);
         }
         for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (active && lane_g == 0) epilogue<T, EPI>(r, s, op, acc);
@@ -227,7 +232,7 @@ __global__ void __launch_bounds__(kBlock) spmv_direct_kernel(CsrView A, Seg seg,
 template <typename T, int EPI>
 __global__ void __launch_bounds__(kBlock) spmv_pattern_kernel(CsrView A, Seg seg, SpmvOp op, Scratch sc)
 {
-    if (op.gate && *reinterpret_cast<const volatile int *>(op.gate) != 0) return;
+    if (gate_closed(op.gate)) return;
     extern __shared__ int s_pat[];   // pattern offsets, then the offsets' table
     int *s_off = s_pat;
     int *s_delta = s_pat + A.npat + 1;
@@ -241,6 +246,7 @@ __global__ void __launch_bounds__(kBlock) spmv_pattern_kernel(CsrView A, Seg seg
     const int rpb = kBlock >> A.lg;
     const int grp = threadIdx.x >> A.lg;
     const int lane_g = threadIdx.x & (G - 1);
+    const uint64_t pol_s = l2_policy(A.l2hint & 1 ? 1 : 0), pol_x = l2_policy(A.l2hint & 2 ? 2 : 0);
     double acc = 0.0;
     for (int base = seg.r0 + blockIdx.x * rpb; base < seg.r1; base += gridDim.x * rpb) {
         const int r = base + grp;
@@ -250,11 +256,129 @@ __global__ void __launch_bounds__(kBlock) spmv_pattern_kernel(CsrView A, Seg seg
             const int j0 = __ldg(row + r), len = __ldg(row + r + 1) - j0;
             const int *d = s_delta + s_off[__ldg(A.pid + r)];
 #pragma unroll 4
-            for (int k = lane_g; k < len; k += G) s += __ldcs(val + j0 + k) * __ldg(x + r + d[k]);
+            for (int k = lane_g; k < len; k += G) s += ld_stream(val + j0 + k, pol_s) * ld_keep(x + r + d[k], pol_x);
         }
         for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (active && lane_g == 0) epilogue<T, EPI>(r, s, op, acc);
     }
+    if constexpr (reduces<EPI>()) {
+        double v[1] = {acc}, out[1];
+        if (grid_reduce<1>(v, sc.partials, sc.ticket, out)) finalize(op, out[0]);
+    }
+}
+
+// Pattern-dictionary SpMV on the sliced layout (SELL-32): warp w takes chunk
+// c of 32 consecutive rows, lane l row 32c + l; the chunk's values are stored
+// k-major (value k of all 32 rows together), so each load instruction reads
+// one 128-byte line of values, and in a chunk whose rows share a pattern the
+// gathers x[r + d_k] of one k are 32 consecutive entries as well.  Rows
+// shorter than the chunk's longest row are padded with zeros.
+template <typename T, int EPI>
+__global__ void __launch_bounds__(kBlock) spmv_sell_kernel(CsrView A, Seg seg, SpmvOp op, Scratch sc)
+{
+    if (gate_closed(op.gate)) return;
+    extern __shared__ int s_pat[];
+    int *s_off = s_pat;
+    int *s_delta = s_pat + A.npat + 1;
+    for (int i = threadIdx.x; i <= A.npat; i += kBlock) s_off[i] = A.pat_off[i];
+    for (int i = threadIdx.x; i < A.ndelta; i += kBlock) s_delta[i] = A.pat_delta[i];
+    __syncthreads();
+    const T *__restrict__ sv = static_cast<const T *>(A.sell_val);
+    const T *__restrict__ x = static_cast<const T *>(op.x);
+    const uint64_t pol_s = l2_policy(A.l2hint & 1 ? 1 : 0), pol_x = l2_policy(A.l2hint & 2 ? 2 : 0);
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    const int nw = gridDim.x * (kBlock / 32);
+    const int c0 = seg.r0 >> 5, c1 = (seg.r1 - 1) >> 5;
+    double acc = 0.0;
+    for (int c = c0 + gw; c <= c1; c += nw) {
+        const int r = (c << 5) + lane;
+        const bool active = r >= seg.r0 && r < seg.r1;
+        const int base = __ldg(A.sell_off + c), L = (__ldg(A.sell_off + c + 1) - base) >> 5;
+        const int p = active ? (int)__ldg(A.pid + r) : 0;
+        const int len = active ? s_off[p + 1] - s_off[p] : 0;
+        const int *d = s_delta + s_off[p];
+        const T *v = sv + base + lane;
+        T s = T(0);
+#pragma unroll 9
+        for (int k = 0; k < L; ++k) {
+            const T a = ld_stream(v + (k << 5), pol_s);
+            if (k < len) s += a * ld_keep(x + r + d[k], pol_x);
+        }
+        if (active) epilogue<T, EPI>(r, s, op, acc);
+    }
+    if constexpr (reduces<EPI>()) {
+        double vv[1] = {acc}, out[1];
+        if (grid_reduce<1>(vv, sc.partials, sc.ticket, out)) finalize(op, out[0]);
+    }
+}
+
+// Pattern-dictionary SpMV with x staged in shared memory.  Rows are taken in
+// tiles of R = kBlock / 2^lg consecutive rows; the x values a tile needs lie
+// on the dictionary's gather lines shifted by the tile's first row, so the
+// CTA loads those lines with coalesced loads (R + span values each, zero
+// outside [0, n)) and every row gathers from shared memory through a
+// precomputed per-entry offset.  The unified L1 then carries only the
+// streamed values.
+template <typename T, int EPI>
+__global__ void __launch_bounds__(kBlock) spmv_pattern_staged_kernel(CsrView A, Seg seg, SpmvOp op, Scratch sc,
+                                                                     int n_x)
+{
+    if (gate_closed(op.gate)) return;
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    const int R = kBlock >> A.lg;
+    int *s_off = reinterpret_cast<int *>(s_raw);              // npat + 1
+    int *s_soff = s_off + A.npat + 1;                          // ndelta: staged offset of each entry
+    int *s_lbase = s_soff + A.ndelta;                          // nlines + 1
+    int *s_lstart = s_lbase + A.nlines + 1;                    // nlines
+    const int head = (A.npat + 1 + A.ndelta + 2 * A.nlines + 1 + 3) & ~3;   // ints, 16-byte multiple
+    T *s_x = reinterpret_cast<T *>(reinterpret_cast<int *>(s_raw) + head);
+    for (int i = threadIdx.x; i <= A.npat; i += kBlock) s_off[i] = A.pat_off[i];
+    for (int i = threadIdx.x; i < A.nlines; i += kBlock) s_lstart[i] = A.line_start[i];
+    if (threadIdx.x == 0) {
+        int b = 0;
+        for (int l = 0; l < A.nlines; ++l) {
+            s_lbase[l] = b;
+            b += R + A.line_span[l];
+        }
+        s_lbase[A.nlines] = b;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < A.ndelta; i += kBlock) s_soff[i] = s_lbase[A.entry_line[i]] + A.entry_lo[i];
+    const int *__restrict__ row = A.row;
+    const T *__restrict__ val = static_cast<const T *>(A.val);
+    const T *__restrict__ x = static_cast<const T *>(op.x);
+    const int G = 1 << A.lg;
+    const int grp = threadIdx.x >> A.lg;
+    const int lane_g = threadIdx.x & (G - 1);
+    const int staged = s_lbase[A.nlines];
+    double acc = 0.0;
+    for (int r0 = seg.r0 + blockIdx.x * R; r0 < seg.r1; r0 += gridDim.x * R) {
+        __syncthreads();
+        // stage the tile's gather lines (coalesced, line by line)
+        for (int l = 0; l < A.nlines; ++l) {
+            const int len = s_lbase[l + 1] - s_lbase[l];
+            const int g0 = r0 + s_lstart[l];
+            T *dst = s_x + s_lbase[l];
+            for (int i = threadIdx.x; i < len; i += kBlock) {
+                const int gi = g0 + i;
+                dst[i] = (gi >= 0 && gi < n_x) ? __ldg(x + gi) : T(0);
+            }
+        }
+        __syncthreads();
+        const int r = r0 + grp;
+        const bool active = r < seg.r1;
+        T s = T(0);
+        if (active) {
+            const int j0 = __ldg(row + r), len = __ldg(row + r + 1) - j0;
+            const int *so = s_soff + s_off[__ldg(A.pid + r)];
+#pragma unroll 4
+            for (int k = lane_g; k < len; k += G) s += __ldcs(val + j0 + k) * s_x[so[k] + grp];
+        }
+        for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (active && lane_g == 0) epilogue<T, EPI>(r, s, op, acc);
+    }
+    (void)staged;
     if constexpr (reduces<EPI>()) {
         double v[1] = {acc}, out[1];
         if (grid_reduce<1>(v, sc.partials, sc.ticket, out)) finalize(op, out[0]);
@@ -293,12 +417,32 @@ template <typename T, int EPI>
 void launch_epi(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st)
 {
     const int ntiles = seg.t1 - seg.t0, nlong = seg.l1 - seg.l0;
+    if (A.use_pat && A.sell_val) {
+        const int chunks = ((seg.r1 - 1) >> 5) - (seg.r0 >> 5) + 1;
+        int grid = (chunks + kBlock / 32 - 1) / (kBlock / 32);
+        const int cap = s.num_sms * 8;
+        if (grid > cap) grid = cap;
+        if (grid < 1) grid = 1;
+        const size_t sm = sizeof(int) * (A.npat + 1 + A.ndelta);
+        spmv_sell_kernel<T, EPI><<<grid, kBlock, sm, st>>>(A, seg, op, s);
+        return;
+    }
     if (A.use_pat) {
         const int rpb = kBlock >> A.lg;
         int grid = (seg.r1 - seg.r0 + rpb - 1) / rpb;
         const int cap = s.num_sms * 8;
         if (grid > cap) grid = cap;
         if (grid < 1) grid = 1;
+        const int staged = A.nlines * rpb + A.span_sum;
+        // measured on B200 (128^3 Q1): staging x per 64-row tile costs more
+        // (two barriers and nine short line copies per tile) than the L1 hits
+        // of the direct gathers save, so it is opt-in
+        if (A.stage_x && A.nlines > 0 && staged <= kMaxStagedX) {
+            const int head = (A.npat + 1 + A.ndelta + 2 * A.nlines + 1 + 3) & ~3;
+            const size_t sm = sizeof(int) * (head + 2) + sizeof(T) * staged;
+            spmv_pattern_staged_kernel<T, EPI><<<grid, kBlock, sm, st>>>(A, seg, op, s, A.n_cols);
+            return;
+        }
         const size_t sm = sizeof(int) * (A.npat + 1 + A.ndelta);
         spmv_pattern_kernel<T, EPI><<<grid, kBlock, sm, st>>>(A, seg, op, s);
         return;
@@ -343,6 +487,31 @@ cudaError_t launch_t(const Scratch &s, const CsrView &A, const Seg &seg, const S
 }  // namespace
 
 int spmv_tile_cap(int cfg) { return cfg == kSpmvTileSmall ? 1024 : 2048; }
+
+namespace {
+template <typename T>
+__global__ void csr_to_sell_kernel(int n, const int *__restrict__ row, const T *__restrict__ val,
+                                   const int *__restrict__ sell_off, T *__restrict__ sv)
+{
+    for (int r = blockIdx.x * kBlock + threadIdx.x; r < n; r += gridDim.x * kBlock) {
+        const int base = sell_off[r >> 5] + (r & 31);
+        const int j0 = row[r], len = row[r + 1] - j0;
+        for (int k = 0; k < len; ++k) sv[base + (k << 5)] = val[j0 + k];
+    }
+}
+}  // namespace
+
+cudaError_t launch_csr_to_sell(int dtype, int n, const int *row, const void *val, const int *sell_off, void *sv,
+                               cudaStream_t st)
+{
+    const int g = (n + kBlock - 1) / kBlock < 148 * 8 ? (n + kBlock - 1) / kBlock : 148 * 8;
+    if (g < 1) return cudaSuccess;
+    if (dtype == 0)
+        csr_to_sell_kernel<double><<<g, kBlock, 0, st>>>(n, row, (const double *)val, sell_off, (double *)sv);
+    else
+        csr_to_sell_kernel<float><<<g, kBlock, 0, st>>>(n, row, (const float *)val, sell_off, (float *)sv);
+    return cudaGetLastError();
+}
 
 cudaError_t spmv_configure()
 {

@@ -55,7 +55,7 @@ template <typename T>
 __global__ void jacobi_kernel(int n, const T *__restrict__ invd, const T *__restrict__ r, T *__restrict__ z,
                               const int *gate)
 {
-    if (gate && *reinterpret_cast<const volatile int *>(gate) != 0) return;
+    if (gate_closed(gate)) return;
     for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) z[i] = r[i] * invd[i];
 }
 
@@ -79,8 +79,11 @@ struct SyncFreeArgs {
 template <typename T>
 __global__ void __launch_bounds__(kBlock) syncfree_sweep_kernel(SyncFreeArgs a)
 {
-    if (a.gate && *reinterpret_cast<const volatile int *>(a.gate) != 0) return;
-    const unsigned epoch = *reinterpret_cast<volatile unsigned *>(a.sync) + (a.backward ? 2u : 1u);
+    if (gate_closed(a.gate)) return;
+    __shared__ unsigned s_epoch;
+    if (threadIdx.x == 0) s_epoch = __ldcg(a.sync) + (a.backward ? 2u : 1u);
+    __syncthreads();
+    const unsigned epoch = s_epoch;
     unsigned *ticket = a.sync + 1 + a.backward;
     const int lane = threadIdx.x & 31;
     const int G = 1 << a.lg;
