@@ -22,6 +22,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libb200la.so")
 
 F64, F32 = 0, 1
+NOALLOC_MAX_N = 67108864      # B200LA_NOALLOC_MAX_N of include/b200la.h
 PRECOND_JACOBI, PRECOND_MCSGS, PRECOND_ILU0_LS, PRECOND_ILU0_MC = 1, 2, 3, 4
 ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS = range(5)
 
@@ -103,6 +104,7 @@ def lib():
         "b200la_dot": ([_P, _I, _I, _P, _P, C.POINTER(_D)], _I),
         "b200la_nrm2": ([_P, _I, _I, _P, C.POINTER(_D)], _I),
         "b200la_dot_dev": ([_P, _I, _I, _P, _P, _P], _I),
+        "b200la_dot_noalloc": ([_I, _I, _P, _P, _P, _P], _I),
         "b200la_axpy": ([_P, _I, _I, _D, _P, _P], _I),
         "b200la_scaleadd": ([_P, _I, _I, _D, _P, _P], _I),
         "b200la_scale": ([_P, _I, _I, _D, _P], _I),

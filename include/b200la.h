@@ -156,6 +156,19 @@ int b200la_dot(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, 
 int b200la_nrm2(b200la_ctx *ctx, int dtype, int n, const void *x, double *result);
 /* Same, result to a DEVICE double, no synchronisation. */
 int b200la_dot_dev(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, double *result_dev);
+/* Dot product x . y written to *result_dev (a DEVICE double) without a
+ * context and without allocating any device memory.  No counterpart in the
+ * reference: it serves callers that cannot allocate -- an application that
+ * owns all device memory through its own pool, or a stream-ordered pipeline
+ * in which cudaMalloc (which may synchronise the device) is not allowed after
+ * set-up.  Its scratch is a fixed array inside the library (about 135 KB per
+ * GPU, held until exit), so n is limited to B200LA_NOALLOC_MAX_N; larger n
+ * returns B200LA_ERR_ARG before anything is launched.  stream is a
+ * cudaStream_t (NULL: the default stream).  The first call on a device sets up
+ * the array's device address and should come before any stream capture; calls
+ * whose kernels overlap on the GPU share the array and race. */
+#define B200LA_NOALLOC_MAX_N 67108864
+int b200la_dot_noalloc(int dtype, int n, const void *x, const void *y, double *result_dev, void *stream);
 /* lVector::Axpy: y += alpha x (lvector.h:283) */
 int b200la_axpy(b200la_ctx *ctx, int dtype, int n, double alpha, const void *x, void *y);
 /* lVector::ScaleAdd: y = alpha y + x (lvector.h:289) */
