@@ -53,6 +53,18 @@ def load_workloads():
     return importlib.import_module("hiflow3_b200.workloads")
 
 
+def profiled_traffic(name="spmv_sell_f32_128cubed.md"):
+    """DRAM bytes per launch of the dominant kernel from the committed ncu
+    summary (dram__bytes_read.sum + dram__bytes_write.sum of one capture)."""
+    import re
+    p = os.path.join(ROOT, "profiles", name)
+    if os.path.exists(p):
+        m = re.search(r"^traffic_bytes_per_launch:\s*(\d+)", open(p).read(), flags=re.M)
+        if m:
+            return int(m.group(1))
+    return None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -354,7 +366,9 @@ def run_b200(args, rank, world, local_rank, dist):
         "roofline": {"bound": "hbm",
                      "kernel": "spmv_sell_kernel<float, EPI_DOT_X>: FP32 dictionary SpMV + p.Ap of the inner CG",
                      "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,
-                     "peak_source": peak_kind, "bytes_per_launch": by32, "traffic": None},
+                     "peak_source": peak_kind, "bytes_per_launch": by32,
+                     "traffic": profiled_traffic() if args.N == 128 else None,
+                     "traffic_source": "profiles/spmv_sell_f32_128cubed.md (ncu, one launch)"},
         "gpu_launches": launches,
         "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n, "matches_device_run": e2e_ok},
