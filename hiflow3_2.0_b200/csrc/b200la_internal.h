@@ -63,6 +63,8 @@ struct b200la_csr {
     int *sell_off = nullptr;
     void *sell_val = nullptr;
     size_t sell_len = 0;
+    int sell_lmax = 0;                // longest chunk row length
+    int sell_tma = 0;                 // bulk-copy tiles (B200LA_SELL_TMA at creation)
 };
 
 struct b200la_precond {

@@ -90,6 +90,8 @@ CsrView csr_view(const b200la_csr *A)
     v.l2hint = A->l2hint;
     v.sell_off = A->sell_off;
     v.sell_val = A->sell_val;
+    v.sell_lmax = A->sell_lmax;
+    v.sell_tma = A->sell_tma;
     v.n_cols = A->m;
     return v;
 }
@@ -376,11 +378,14 @@ static int build_sell(b200la_ctx *ctx, b200la_csr *A)
     if (!A->sell_off) {
         const int nch = (A->n + 31) / 32;
         std::vector<int> off(nch + 1, 0);
+        A->sell_lmax = 0;
         for (int c = 0; c < nch; ++c) {
             int L = 0;
             for (int r = 32 * c; r < std::min(A->n, 32 * c + 32); ++r) L = std::max(L, A->h_row[r + 1] - A->h_row[r]);
             off[c + 1] = off[c] + 32 * L;
+            A->sell_lmax = std::max(A->sell_lmax, L);
         }
+        if (const char *e = std::getenv("B200LA_SELL_TMA")) A->sell_tma = std::atoi(e);
         A->sell_len = (size_t)off[nch];
         if ((e = cudaMalloc(&A->sell_off, sizeof(int) * (nch + 1))) ||
             (e = cudaMalloc(&A->sell_val, es * std::max<size_t>(A->sell_len, 32))) ||

@@ -98,6 +98,8 @@ struct CsrView {
     // 32 rows holds its values k-major at sell_val[sell_off[c] + 32 k + lane]
     const int *sell_off;
     const void *sell_val;
+    int sell_lmax;   // longest chunk (values per row) of the sliced layout
+    int sell_tma;    // bulk-copy tiles for the sliced layout
     int n_cols;      // length of x
 };
 

@@ -313,6 +313,87 @@ __global__ void __launch_bounds__(kBlock) spmv_sell_kernel(CsrView A, Seg seg, S
     }
 }
 
+// The sliced dictionary SpMV with the values brought in by the bulk-copy
+// engine: a tile is 8 consecutive 32-row chunks -- one contiguous, 128-byte
+// aligned range of the sliced values -- and a persistent grid keeps kSellStages
+// tiles per CTA in flight (one cp.async.bulk each, evict-first in L2).  Warp w
+// of the CTA reduces chunk w of the tile from shared memory, one row per lane.
+constexpr int kSellStages = 3;
+constexpr size_t kSellTmaMaxSmem = 200 * 1024;
+
+template <typename T, int EPI>
+__global__ void __launch_bounds__(kBlock, 2)
+    spmv_sell_tma_kernel(CsrView A, Seg seg, SpmvOp op, Scratch sc, int stage_elems)
+{
+    if (gate_closed(op.gate)) return;
+    extern __shared__ __align__(128) unsigned char smem[];
+    int *s_off = reinterpret_cast<int *>(smem);
+    int *s_delta = s_off + A.npat + 1;
+    const int head = ((A.npat + 1 + A.ndelta) * 4 + 127) & ~127;
+    T *stages = reinterpret_cast<T *>(smem + head);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + head + kSellStages * stage_elems * (int)sizeof(T));
+    for (int i = threadIdx.x; i <= A.npat; i += kBlock) s_off[i] = A.pat_off[i];
+    for (int i = threadIdx.x; i < A.ndelta; i += kBlock) s_delta[i] = A.pat_delta[i];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kSellStages; ++s) mbar_init(&bars[s], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    const T *__restrict__ sv = static_cast<const T *>(A.sell_val);
+    const T *__restrict__ x = static_cast<const T *>(op.x);
+    const uint64_t pol_x = l2_policy(A.l2hint & 2 ? 2 : 0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int c0 = seg.r0 >> 5, c1 = (seg.r1 - 1) >> 5;
+    const int ntile = (c1 - c0 + 1 + kBlock / 32 - 1) / (kBlock / 32);
+    const int my_n = ((int)blockIdx.x < ntile) ? (ntile - 1 - (int)blockIdx.x) / (int)gridDim.x + 1 : 0;
+    uint64_t pol = 0;
+    auto issue = [&](int k, int stg) {
+        const int t = blockIdx.x + k * gridDim.x;
+        const int cb = c0 + t * (kBlock / 32);
+        const int ce = min(cb + kBlock / 32, c1 + 1);
+        const int e0 = __ldg(A.sell_off + cb), e1 = __ldg(A.sell_off + ce);
+        const unsigned bytes = (unsigned)(e1 - e0) * (unsigned)sizeof(T);
+        mbar_arrive_expect_tx(&bars[stg], bytes);
+        if (bytes) bulk_g2s(stages + stg * stage_elems, sv + e0, bytes, &bars[stg], pol);
+    };
+    if (threadIdx.x == 0) {
+        pol = l2_evict_first_policy();
+        for (int k = 0; k < kSellStages && k < my_n; ++k) issue(k, k);
+    }
+    double acc = 0.0;
+    for (int k = 0; k < my_n; ++k) {
+        const int stg = k % kSellStages;
+        const bool ok = mbar_wait_bounded(&bars[stg], (unsigned)(k / kSellStages) & 1u, sc.err);
+        if (__syncthreads_or(!ok)) break;
+        const int t = blockIdx.x + k * gridDim.x;
+        const int cb = c0 + t * (kBlock / 32);
+        const int c = cb + warp;
+        if (c <= c1) {
+            const int ebase = __ldg(A.sell_off + cb);
+            const int e0 = __ldg(A.sell_off + c), L = (__ldg(A.sell_off + c + 1) - e0) >> 5;
+            const T *v = stages + stg * stage_elems + (e0 - ebase) + lane;
+            const int r = (c << 5) + lane;
+            const bool active = r >= seg.r0 && r < seg.r1;
+            const int p = active ? (int)__ldg(A.pid + r) : 0;
+            const int len = active ? s_off[p + 1] - s_off[p] : 0;
+            const int *d = s_delta + s_off[p];
+            T s = T(0);
+#pragma unroll 9
+            for (int q = 0; q < L; ++q) {
+                const T a = v[q << 5];
+                if (q < len) s += a * ld_keep(x + r + d[q], pol_x);
+            }
+            if (active) epilogue<T, EPI>(r, s, op, acc);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && k + kSellStages < my_n) issue(k + kSellStages, stg);
+    }
+    if constexpr (reduces<EPI>()) {
+        double vv[1] = {acc}, out[1];
+        if (grid_reduce<1>(vv, sc.partials, sc.ticket, out)) finalize(op, out[0]);
+    }
+}
+
 // Pattern-dictionary SpMV with x staged in shared memory.  Rows are taken in
 // tiles of R = kBlock / 2^lg consecutive rows; the x values a tile needs lie
 // on the dictionary's gather lines shifted by the tile's first row, so the
@@ -392,6 +473,27 @@ cudaError_t set_tile_attr()
                                 ST * TileSmem<CAP>::template stage_bytes<T>() + ST * 8);
 }
 
+template <typename T, int EPI>
+cudaError_t set_sell_attr()
+{
+    return cudaFuncSetAttribute(spmv_sell_tma_kernel<T, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)kSellTmaMaxSmem);
+}
+
+template <typename T>
+cudaError_t configure_sell()
+{
+    cudaError_t e;
+    if ((e = set_sell_attr<T, EPI_SET>())) return e;
+    if ((e = set_sell_attr<T, EPI_ADD>())) return e;
+    if ((e = set_sell_attr<T, EPI_DOT_X>())) return e;
+    if ((e = set_sell_attr<T, EPI_RESID>())) return e;
+    if ((e = set_sell_attr<T, EPI_SGS_F>())) return e;
+    if ((e = set_sell_attr<T, EPI_SGS_B>())) return e;
+    if ((e = set_sell_attr<T, EPI_ILU_F>())) return e;
+    return set_sell_attr<T, EPI_ILU_B>();
+}
+
 template <typename T, int CAP, int ST, int MINB>
 cudaError_t configure_tile()
 {
@@ -417,6 +519,19 @@ template <typename T, int EPI>
 void launch_epi(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st)
 {
     const int ntiles = seg.t1 - seg.t0, nlong = seg.l1 - seg.l0;
+    const int stage_elems = (kBlock / 32) * 32 * A.sell_lmax;
+    const size_t sell_sm = (((A.npat + 1 + A.ndelta) * 4 + 127) & ~127) +
+                           (size_t)kSellStages * stage_elems * sizeof(T) + kSellStages * 8;
+    if (A.use_pat && A.sell_val && A.sell_tma && sell_sm <= kSellTmaMaxSmem) {
+        const size_t sm = sell_sm;
+        const int chunks = ((seg.r1 - 1) >> 5) - (seg.r0 >> 5) + 1;
+        int grid = (chunks + kBlock / 32 - 1) / (kBlock / 32);
+        const int cap = s.num_sms * 2;
+        if (grid > cap) grid = cap;
+        if (grid < 1) grid = 1;
+        spmv_sell_tma_kernel<T, EPI><<<grid, kBlock, sm, st>>>(A, seg, op, s, stage_elems);
+        return;
+    }
     if (A.use_pat && A.sell_val) {
         const int chunks = ((seg.r1 - 1) >> 5) - (seg.r0 >> 5) + 1;
         int grid = (chunks + kBlock / 32 - 1) / (kBlock / 32);
@@ -519,7 +634,9 @@ cudaError_t spmv_configure()
     if ((e = configure_tile<double, 2048, 4, 2>())) return e;
     if ((e = configure_tile<float, 2048, 4, 2>())) return e;
     if ((e = configure_tile<double, 1024, 3, 4>())) return e;
-    return configure_tile<float, 1024, 3, 4>();
+    if ((e = configure_tile<float, 1024, 3, 4>())) return e;
+    if ((e = configure_sell<double>())) return e;
+    return configure_sell<float>();
 }
 
 cudaError_t launch_spmv(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st)

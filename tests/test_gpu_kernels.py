@@ -128,14 +128,15 @@ def test_spmv_lane_layouts(pf, b200, oracle, lanes, monkeypatch):
     assert spmv_ok(yv.numpy(), oracle.spmv(row, col, val, x), row_scale(row, col, val, x), 1e-13)
 
 
-@pytest.mark.parametrize("mode,stage", [("0", "0"), ("2", "0"), ("2", "1")])
-@pytest.mark.parametrize("dim,N,kind", [(3, 10, 0), (2, 33, 1)])
-def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, dim, N, kind, monkeypatch):
-    """SpMV through the row-pattern dictionary (mode 2, both precisions, x read
-    directly or staged in shared memory) equals SpMV through explicit column
-    indices (mode 0)."""
+@pytest.mark.parametrize("mode,stage,tma", [("0", "0", "0"), ("2", "0", "0"), ("2", "1", "0"), ("2", "0", "1")])
+@pytest.mark.parametrize("dim,N,kind", [(3, 10, 0), (2, 33, 1), (3, 21, 0)])
+def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, tma, dim, N, kind, monkeypatch):
+    """SpMV through the row-pattern dictionary (mode 2, both precisions; sliced
+    layout read directly or by bulk-copy tiles, or CSR value order with x
+    staged in shared memory) equals SpMV through explicit column indices."""
     monkeypatch.setenv("B200LA_PATTERN", mode)
     monkeypatch.setenv("B200LA_STAGE_X", stage)
+    monkeypatch.setenv("B200LA_SELL_TMA", tma)
     row, col, val = oracle.q1_assemble(dim, N, kind, None, nu=1e-3, beta=(1.0, 0.5))
     n = len(row) - 1
     x = np.random.default_rng(4).uniform(-1, 1, n)
