@@ -28,7 +28,11 @@ ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS = range(5)
 
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "allocation failed",
           4: "no usable sm_100 device", 5: "malformed CSR", 6: "refused by memory budget",
-          7: "bounded device wait gave up", 8: "preconditioner setup failed", 9: "unknown request"}
+          7: "bounded device wait gave up", 8: "preconditioner setup failed", 9: "unknown request",
+          10: "request pending"}
+PENDING = 10
+SERVE_CG, SERVE_GMRES = 0, 1
+SERVE_F64, SERVE_MIXED = 0, 1
 
 
 class B200Error(RuntimeError):
@@ -45,6 +49,39 @@ class Control(C.Structure):
 class Result(C.Structure):
     _fields_ = [("iters", C.c_int), ("status", C.c_int), ("res0", C.c_double), ("res", C.c_double),
                 ("outer", C.c_int), ("launches", C.c_int), ("solve_ms", C.c_double)]
+
+
+class ServeConfig(C.Structure):
+    """b200la_serve_config."""
+    _fields_ = [("device", C.c_int), ("budget_bytes", C.c_double), ("max_slots", C.c_int),
+                ("active_bytes", C.c_double), ("max_active", C.c_int), ("iters_per_round", C.c_int),
+                ("autotune", C.c_int), ("warps", C.c_int), ("ctas_per_sm", C.c_int), ("chunks_per_warp", C.c_int)]
+
+
+class Request(C.Structure):
+    """b200la_request."""
+    _fields_ = [("method", C.c_int), ("precision", C.c_int), ("n", C.c_int), ("nnz", C.c_int),
+                ("row", C.c_void_p), ("col", C.c_void_p), ("val", C.c_void_p),
+                ("q1_dim", C.c_int), ("q1_N", C.c_int), ("q1_kind", C.c_int), ("q1_kcell", C.c_void_p),
+                ("q1_nu", C.c_double), ("q1_beta", C.c_double * 3), ("b", C.c_void_p), ("rhs_seed", C.c_uint64),
+                ("x", C.c_void_p), ("ctl", Control), ("inner", Control), ("max_outer", C.c_int),
+                ("gmres_m", C.c_int), ("gmres_precond", C.c_int)]
+
+
+class ServeResult(C.Structure):
+    """b200la_serve_result."""
+    _fields_ = [("status", C.c_int), ("iters", C.c_int), ("outer", C.c_int), ("res0", C.c_double),
+                ("res", C.c_double), ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_ready", C.c_double),
+                ("t_done", C.c_double), ("bytes", C.c_double)]
+
+
+class ServeInfo(C.Structure):
+    """b200la_serve_info."""
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("failed", C.c_longlong),
+                ("rounds", C.c_longlong), ("batch_iters", C.c_longlong), ("busy_ms", C.c_double),
+                ("resident_bytes", C.c_double), ("peak_resident_bytes", C.c_double), ("peak_active", C.c_int),
+                ("warps", C.c_int), ("ctas_per_sm", C.c_int), ("chunks_per_warp", C.c_int),
+                ("iters_per_round", C.c_int), ("active_bytes", C.c_double)]
 
 
 def build(force=False):
@@ -133,6 +170,14 @@ def lib():
         "b200la_cg_hist": ([_P, _P, _P, _P, _P, C.POINTER(Control), C.POINTER(Result), _P, _I], _I),
         "b200la_gmres": ([_P, _P, _P, _I, _P, _P, C.POINTER(Control), C.POINTER(Result)], _I),
         "b200la_mpir": ([_P, _P, _P, _P, _P, C.POINTER(Control), C.POINTER(Control), _I, C.POINTER(Result)], _I),
+        "b200la_q1_assemble_device": ([_P, _I, _I, _I, _P, _D, _P, _P, _P, _P], _I),
+        "b200la_q1_rhs_device": ([_P, C.c_uint64, _I, _I, _P], _I),
+        "b200la_serve_start": ([C.POINTER(ServeConfig), C.POINTER(_P)], _I),
+        "b200la_serve_submit": ([_P, C.POINTER(Request), C.POINTER(C.c_longlong)], _I),
+        "b200la_serve_poll": ([_P, C.c_longlong, C.POINTER(ServeResult)], _I),
+        "b200la_serve_wait": ([_P, C.c_longlong, _D, C.POINTER(ServeResult)], _I),
+        "b200la_serve_stats": ([_P, C.POINTER(ServeInfo)], _I),
+        "b200la_serve_stop": ([_P], _I),
     }
     for name, (args, res) in sig.items():
         f = getattr(L, name)

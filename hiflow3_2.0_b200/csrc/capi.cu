@@ -215,6 +215,7 @@ extern "C" const char *b200la_status_string(int s)
     case B200LA_ERR_TIMEOUT: return "bounded device wait gave up";
     case B200LA_ERR_SETUP: return "preconditioner setup failed";
     case B200LA_ERR_NOTFOUND: return "unknown request";
+    case B200LA_PENDING: return "request pending";
     default: return "unknown status";
     }
 }

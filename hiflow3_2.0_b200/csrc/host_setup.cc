@@ -87,17 +87,6 @@ int q1_sizes(int dim, int N, int *n, int64_t *nnz)
     return 0;
 }
 
-namespace {
-
-struct Q1Tables {
-    int dim, nv, nq;
-    double phi[8][8];       // [q][a]
-    double grad[8][8][3];   // [q][a][d]
-    double w[8];
-    double gg[8][8][8];     // [q][i][j] = grad_j . grad_i
-    double dJ;
-};
-
 void q1_tables(int dim, double h, Q1Tables &t)
 {
     t.dim = dim;
@@ -133,6 +122,8 @@ void q1_tables(int dim, double h, Q1Tables &t)
     t.dJ = 1.0;
     for (int d = 0; d < dim; ++d) t.dJ *= h;
 }
+
+namespace {
 
 void q1_element(const Q1Tables &t, int kind, double coef, const double *beta, double *Ke)
 {

@@ -33,6 +33,19 @@ void zero_rows(const int *row, const int *col, double *val, const int *idx, int 
 // Structured Q1 systems: lexicographic DoFs (x fastest), element matrices of
 // examples/poisson/poisson_tutorial.h:152-176 (kind 0) and
 // examples/convection_diffusion/convdiff.cc:75-117 (kind 1) with 2-point Gauss.
+// Quadrature tables of the Q1 element on a cell of side h: shape values,
+// gradients, weights, gradient products and the Jacobian determinant.  The
+// device assembler uploads these very numbers so that both assemblers round
+// identically.
+struct Q1Tables {
+    int dim, nv, nq;
+    double phi[8][8];       // [q][a]
+    double grad[8][8][3];   // [q][a][d]
+    double w[8];
+    double gg[8][8][8];     // [q][i][j] = grad_j . grad_i
+    double dJ;
+};
+void q1_tables(int dim, double h, Q1Tables &t);
 int q1_sizes(int dim, int N, int *n, int64_t *nnz);
 int q1_assemble(int dim, int N, int kind, const double *kcell, double nu, const double *beta, int *row, int *col,
                 double *val);

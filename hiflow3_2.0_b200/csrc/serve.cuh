@@ -1,0 +1,101 @@
+// serve.cuh -- device layout of the continuous-batching solve server.
+//
+// Every resident request (a "slot") owns one SysDesc in a device table and
+// one SysState.  Its operator is stored in 32-row chunks: the SELL layout
+// (chunk c holds its rows' entries k-major, sell[off[c] + 32 k + lane], rows
+// zero-padded to the chunk's longest row) or, for rows too long for that, the
+// CSR with one warp per row.  Two batched kernels advance every active
+// system by one iteration of its Krylov recurrence; a tile table lists which
+// chunks of which systems a launch covers.
+//
+// Determinism: a system's arithmetic never depends on the batch it is in.
+// Row sums run in a fixed order (one thread per row in column order, or a
+// fixed shuffle tree per row), reductions go through one partial per 32-row
+// chunk, and the CTA that completes a system's tiles sums those partials in a
+// fixed order over 256 virtual lanes.  Tile size, block size, grid size and
+// the other systems of the batch change only the schedule.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace b200 {
+namespace srv {
+
+// Per-system phase of the state machine run by the two kernels.
+//   FP64 Jacobi-PCG (CG<LAD>::SolvePrecond, src/linear_solver/cg.cc:164-248):
+//     CG_START (update kernel: r = b, rho = r.z, res0) -> CG ... -> DONE
+//   Mixed (MPIR<LAD_high, LAD_low>::Solve, src/linear_solver/mpir.cc:69-326,
+//   with an FP32 Jacobi-CG error correction):
+//     OUTER (update kernel: r = b - A x in FP64, r_low = (float) r, x_low = 0)
+//       -> INNER (FP32 CG on A x_low = r_low) -> CORRECT (SpMV kernel:
+//       x += (double) x_low; update kernel: the next outer residual) -> ... -> DONE
+enum Phase : int { PH_CG_START = 0, PH_CG = 1, PH_OUTER = 2, PH_INNER = 3, PH_CORRECT = 4, PH_DONE = 5 };
+// FMT_STENCIL: a structured Q1 operator stored by stencil position: entry k
+// of row i is the coupling to column i + delta_k (the 9 / 27 offsets
+// (dk P + dj) P + di in column order, P = N + 1 nodes per line), chunk c at
+// val[32 L c + 32 k + lane], zero where the row has no such neighbour.  No
+// column indices or offsets are stored or loaded.
+enum Fmt : int { FMT_SELL = 0, FMT_CSRW = 1, FMT_STENCIL = 2 };
+
+constexpr int kChunk = 32;          // rows per chunk
+constexpr int kFinLanes = 256;      // virtual lanes of the per-system final sums
+constexpr int kTicketWords = 64;    // two ticket counters per slot, 128 bytes apart
+constexpr int kMaxRowSell = 64;     // longest row kept in the SELL layout
+
+struct SysState {
+    double rho, alpha, beta, res, res0, res_in0;
+    double abstol, reltol, divtol, in_abstol, in_reltol, in_divtol;
+    int iter;        // FP64: CG iterations; mixed: inner iterations in total
+    int inner_iter;  // mixed: iterations of the running inner solve
+    int outer;       // mixed: corrections applied
+    int status;      // B200LA_ITERATE / SUCCESS_* / FAIL_*
+    int phase, maxits, in_maxits, max_outer;
+    int pbuf;        // which of the two search-direction buffers holds p
+    int pad[3];
+};
+
+struct SysDesc {
+    int n, nchunks, mixed, fmt;
+    int pstride;           // chunk partials per quantity (nchunks rounded up to even)
+    int sdim, sP, sL;      // FMT_STENCIL: dimension, nodes per line, stencil width
+    const int *off;        // SELL: chunk offsets [nchunks + 1]; CSRW: row pointer [n + 1]
+    const int *col;
+    const double *val64;
+    const float *val32;    // mixed only
+    const double *b;
+    double *x;
+    void *r, *z, *p0, *p1, *ap, *xl;  // FP64 system: double r, z = D^-1 r, p, Ap; mixed: float ... and x_low
+    const void *invd;      // 1 / a_ii: double, or float for mixed
+    double *part;          // [3][pstride] chunk partials
+    unsigned *ticket;      // kTicketWords words
+    int *done;             // final status word polled by the host (0 while running)
+};
+
+// Column offset of stencil position k (column order).
+__host__ __device__ __forceinline__ int stencil_delta(int dim, int P, int k)
+{
+    return dim == 3 ? ((k / 9 - 1) * P + (k / 3 % 3 - 1)) * P + (k % 3 - 1) : (k / 3 - 1) * P + (k % 3 - 1);
+}
+
+struct Tile {
+    int sys, c0, c1, ntiles;   // chunks [c0, c1) of slot sys, which has ntiles tiles
+};
+
+// Tile table in device memory: word 0 the tile count, tiles from word 4.
+constexpr int kTileHdrWords = 4;
+
+// One batch iteration (SpMV kernel, update kernel) over the tile table.
+// SysDesc and SysState tables are indexed by slot.
+cudaError_t launch_round(int nw, int grid, const SysDesc *sys, SysState *state, const int *tiles, cudaStream_t st);
+// CSR (device, FP64) -> the slot's chunk layout, 1 / a_ii, and FP32 values when mixed.
+cudaError_t launch_build_slot(const SysDesc &d, const int *row, const int *col, const double *val,
+                              cudaStream_t st);
+
+}  // namespace srv
+
+cudaError_t launch_q1_assemble(int dim, int N, int kind, const double *kcell, double nu, const double *beta, int *row,
+                               int *col, double *val, cudaStream_t st);
+cudaError_t launch_q1_rhs(unsigned long long seed, int dim, int N, double *b, cudaStream_t st);
+
+}  // namespace b200

@@ -32,7 +32,7 @@ def grf_cells(N, dim=3, sigma=1.0, ell=0.1, seed=2024):
     lam = np.maximum(lam, 0.0)
     rng = np.random.default_rng(seed)
     white = rng.standard_normal((M,) * dim)
-    g = np.fft.irfftn(np.sqrt(lam) * np.fft.rfftn(white), s=(M,) * dim)
+    g = np.fft.irfftn(np.sqrt(lam) * np.fft.rfftn(white), s=(M,) * dim, axes=tuple(range(dim)))
     g = g[(slice(0, N),) * dim]
     # array axes are (z, y, x) so that flattening gives x fastest
     return np.ascontiguousarray(g).reshape(-1)

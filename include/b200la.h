@@ -39,7 +39,8 @@ typedef enum {
     B200LA_ERR_BUDGET = 6,     /* request refused by the serving memory budget */
     B200LA_ERR_TIMEOUT = 7,    /* a bounded device wait gave up */
     B200LA_ERR_SETUP = 8,      /* preconditioner analysis failed (e.g. no colours / levels) */
-    B200LA_ERR_NOTFOUND = 9    /* unknown serving request id */
+    B200LA_ERR_NOTFOUND = 9,   /* unknown serving request id */
+    B200LA_PENDING = 10        /* serving request still queued or running */
 } b200la_status;
 
 /* IterateControl (src/common/iterate_control.h) */
@@ -213,6 +214,14 @@ int b200la_q1_sizes(int dim, int N, int *n, int64_t *nnz);
 int b200la_q1_assemble(int dim, int N, int kind, const double *kcell, double nu, const double *beta, int *row,
                        int *col, double *val);
 int b200la_q1_rhs(uint64_t seed, int dim, int N, double *b);
+/* The same CSR (bit-identical values) and right-hand side built on the device
+ * on the context's stream: row (n+1), col, val (nnz) and b (n) device arrays,
+ * kcell a device array of N^dim cell coefficients or NULL, beta 3 host doubles
+ * or NULL.  No counterpart in the reference, which assembles on the host
+ * (src/assembly/standard_assembly.cc, coupled_matrix.cc:579-607). */
+int b200la_q1_assemble_device(b200la_ctx *ctx, int dim, int N, int kind, const double *kcell, double nu,
+                              const double *beta, int *row, int *col, double *val);
+int b200la_q1_rhs_device(b200la_ctx *ctx, uint64_t seed, int dim, int N, double *b);
 
 /* --------------------------------------------------------- preconditioners */
 
@@ -259,6 +268,95 @@ int b200la_gmres(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P, 
  * outer->reltol is relative to ||b - A x0||. */
 int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_csr *A32, const double *b, double *x,
                 const b200la_control *outer, const b200la_control *inner, int max_outer, b200la_result *res);
+
+/* ---------------------------------------------------------------- serving */
+
+/* A continuous-batching solve server; the reference has no counterpart (its
+ * solvers run one system at a time, src/linear_solver/cg.cc:68-248).
+ * Requests are admitted against a device-memory budget as they arrive, kept
+ * resident in HBM (operator, Jacobi diagonal, Krylov state), and every
+ * admitted SPD request joins the batch that one CUDA-graph replay advances by
+ * iters_per_round iterations; finished requests leave between replays and
+ * their memory admits the next.  A system's arithmetic does not depend on the
+ * batch it runs in: its result is bit-identical alone and in any mix.
+ * Nonsymmetric requests run on a second stream, one at a time (GMRES).
+ * Requests start from x0 = 0.  Host arrays named by a request must stay valid
+ * until the request has finished. */
+typedef struct b200la_server b200la_server;
+
+typedef struct {
+    int device;
+    double budget_bytes;     /* device bytes resident requests may hold (0: 60e9) */
+    int max_slots;           /* resident requests at most (0: 4096) */
+    double active_bytes;     /* bytes one batch iteration may stream (0: 256 MiB) */
+    int max_active;          /* requests iterated together at most (0: 1024) */
+    int iters_per_round;     /* batch iterations per graph replay (0: 16) */
+    int autotune;            /* 1: time the kernel shapes on a calibration batch at start */
+    int warps;               /* kernel shape when not tuned (0: defaults) */
+    int ctas_per_sm;
+    int chunks_per_warp;
+} b200la_serve_config;
+
+#define B200LA_SERVE_CG 0       /* SPD: Jacobi-PCG (FP64) or FP32 Jacobi-CG inside FP64 defect correction */
+#define B200LA_SERVE_GMRES 1    /* nonsymmetric: GMRES(m), FP64, Jacobi or ILU(0) level-scheduled */
+#define B200LA_SERVE_F64 0
+#define B200LA_SERVE_MIXED 1
+
+typedef struct {
+    int method;              /* B200LA_SERVE_CG / B200LA_SERVE_GMRES */
+    int precision;           /* B200LA_SERVE_F64 / B200LA_SERVE_MIXED (CG only) */
+    /* operator: a host CSR (FP64) ... */
+    int n, nnz;
+    const int *row, *col;
+    const double *val;
+    /* ... or, when row is NULL, the structured Q1 system of b200la_q1_assemble
+     * assembled on the device (kcell: host array of N^dim coefficients or NULL) */
+    int q1_dim, q1_N, q1_kind;
+    const double *q1_kcell;
+    double q1_nu;
+    double q1_beta[3];
+    /* right-hand side: host array, or when NULL the Q1 stream of rhs_seed */
+    const double *b;
+    uint64_t rhs_seed;
+    double *x;               /* host result, n doubles */
+    b200la_control ctl;      /* CG / GMRES stop test; mixed: the outer defect-correction test */
+    b200la_control inner;    /* mixed: the FP32 CG's stop test */
+    int max_outer;           /* mixed: corrections at most */
+    int gmres_m;             /* GMRES restart length */
+    int gmres_precond;       /* B200LA_PRECOND_JACOBI or B200LA_PRECOND_ILU0_LS */
+} b200la_request;
+
+typedef struct {
+    int status;              /* B200LA_SUCCESS_* / B200LA_FAIL_*, or -B200LA_ERR_* when it failed to run */
+    int iters;               /* Krylov iterations (inner iterations in total for mixed) */
+    int outer;               /* mixed: corrections */
+    double res0, res;        /* first and last residual norm of the stop test */
+    double t_submit, t_admit, t_ready, t_done;   /* seconds since the server started */
+    double bytes;            /* device bytes the request held */
+} b200la_serve_result;
+
+typedef struct {
+    long long submitted, completed, failed;
+    long long rounds, batch_iters;
+    double busy_ms;          /* device time of the graph replays */
+    double resident_bytes, peak_resident_bytes;
+    int peak_active;
+    int warps, ctas_per_sm, chunks_per_warp, iters_per_round;   /* kernel shape in use */
+    double active_bytes;
+} b200la_serve_info;
+
+int b200la_serve_start(const b200la_serve_config *cfg, b200la_server **out);
+/* Queue a request; returns its id.  B200LA_ERR_BUDGET when it could never fit
+ * the budget, B200LA_ERR_CSR / B200LA_ERR_ARG for malformed input. */
+int b200la_serve_submit(b200la_server *s, const b200la_request *req, long long *id);
+/* B200LA_OK with the result once finished, B200LA_PENDING before,
+ * B200LA_ERR_NOTFOUND for an unknown id. */
+int b200la_serve_poll(b200la_server *s, long long id, b200la_serve_result *res);
+/* As poll, waiting up to timeout_s seconds (B200LA_PENDING if still running). */
+int b200la_serve_wait(b200la_server *s, long long id, double timeout_s, b200la_serve_result *res);
+int b200la_serve_stats(b200la_server *s, b200la_serve_info *out);
+/* Finish every queued request, then release the server. */
+int b200la_serve_stop(b200la_server *s);
 
 #ifdef __cplusplus
 }
