@@ -375,12 +375,114 @@ def run_b200(args, rank, world, local_rank, dist):
         "setup_s": {"assembly": t_asm, "upload_and_cast": t_up},
         "clocks": clk.summary(),
     }
+    if args.serve_requests > 0:
+        line["serving"] = serving_bench(b200, pf, args.serve_requests)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(row, col, val, b, res_mixed["outer"], res_mixed["inner_total"], fp64_iters)
         line["cpu_baseline"] = cb if cb else {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                               "sample": "oracle/_ref missing"}
     pf.close()
     return line
+
+
+def serving_bench(b200, pf, nreq, sample=64, seed=2025):
+    """The serving loop on the seeded request stream: saturation throughput
+    (every request offered at t = 0), p50/p99 latency at Poisson arrival rates
+    below saturation, and the drop-in FP64 Jacobi-CG solving a sample of the
+    same requests one at a time."""
+    import importlib
+    srv = importlib.import_module("hiflow3_b200.serving")
+    fb = srv.FieldBank()
+    stream = srv.c5_stream(nreq, seed=seed)
+    kcache = {}
+
+    def kcell(r):
+        key = (r["N"], r["field"])
+        if key not in kcache:
+            kcache[key] = fb.kcell(r["N"], r["field"])
+        return kcache[key]
+
+    def req(r):
+        kc = kcell(r) if r["dim"] == 2 else None
+        return dict(q1=dict(dim=r["dim"], N=r["N"], kcell=kc), rhs_seed=r["rhs_seed"], precision=r["precision"],
+                    ctl=(100000, 0.0, 1e-10, 1e6), inner=(100000, 0.0, 1e-4, 1e6), max_outer=50)
+
+    reqs = [req(r) for r in stream]
+
+    def ok(r):
+        return r["status"] in (b200.SUCCESS_ABS, b200.SUCCESS_REL) and r["res"] <= 1e-10 * r["res0"]
+
+    s = srv.Server(autotune=True)
+    t0 = time.perf_counter()
+    ids = [s.submit(**a) for a in reqs]
+    res = [s.wait(i) for i in ids]
+    t_sat = time.perf_counter() - t0
+    st = s.stats()
+    s.stop()
+    sat = len(res) / t_sat
+    shape = dict(warps=st["warps"], ctas_per_sm=st["ctas_per_sm"], chunks_per_warp=st["chunks_per_warp"])
+    lat = [r["latency"] for r in res]
+    out = {"requests": len(res), "solves_per_s": sat, "wall_s": t_sat, "met_1e-10": sum(map(ok, res)),
+           "latency_ms": {k: v * 1e3 for k, v in srv.percentiles(lat).items()},
+           "iterations": int(sum(r["iters"] for r in res)), "rounds": st["rounds"],
+           "batch_iterations": st["batch_iters"], "gpu_busy_s": st["busy_ms"] / 1e3,
+           "peak_active": st["peak_active"], "peak_resident_gb": st["peak_resident_bytes"] / 1e9,
+           "kernel_shape": shape, "active_bytes": st["active_bytes"],
+           "mix": {"2d": sum(r["dim"] == 2 for r in stream), "3d": sum(r["dim"] == 3 for r in stream),
+                   "mixed_precision": sum(r["precision"] == b200.SERVE_MIXED for r in stream)}}
+    sweeps = []
+    m = min(nreq, 1024)
+    for frac in (0.5, 0.8):
+        rate = frac * sat
+        arr = srv.poisson_arrivals(m, rate, seed=int(frac * 100))
+        s = srv.Server(**shape)
+        t0 = time.perf_counter()
+        ids = []
+        for k in range(m):
+            dt = t0 + arr[k] - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            ids.append(s.submit(**reqs[k]))
+        rs = [s.wait(i) for i in ids]
+        t_all = time.perf_counter() - t0
+        s.stop()
+        pc = srv.percentiles([r["latency"] for r in rs])
+        sweeps.append({"offered_per_s": rate, "served_per_s": m / t_all, "requests": m,
+                       "p50_ms": pc["p50"] * 1e3, "p99_ms": pc["p99"] * 1e3, "met_1e-10": sum(map(ok, rs))})
+    out["rate_sweep"] = sweeps
+    # one at a time: the drop-in FP64 Jacobi-CG (lMatrix upload, solve, download)
+    solve_s = full_s = 0.0
+    err = 0.0
+    for k in range(min(sample, nreq)):
+        r = stream[k]
+        kc = kcell(r) if r["dim"] == 2 else None
+        row, col, val = b200.q1_assemble(r["dim"], r["N"], 0, kc)
+        bh = b200.q1_rhs(r["rhs_seed"], r["dim"], r["N"])
+        pf.sync()
+        ta = time.perf_counter()
+        A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+        P = b200.Preconditioner.Jacobi(pf, A)
+        cg = b200.CG(pf)
+        cg.SetupOperator(A)
+        cg.SetupPreconditioner(P)
+        cg.InitControl(100000, 0.0, 1e-10, 1e6)
+        xv, bv = pf.vector(len(bh)), pf.vector(bh)
+        pf.sync()
+        tb = time.perf_counter()
+        cg.Solve(bv, xv)
+        pf.sync()
+        tc = time.perf_counter()
+        xh = xv.numpy()
+        td = time.perf_counter()
+        solve_s += tc - tb
+        full_s += td - ta
+        err = max(err, float(np.linalg.norm(res[k]["x"] - xh) / np.linalg.norm(xh)))
+    ns = min(sample, nreq)
+    out["one_at_a_time_fp64"] = {"sample": ns, "solves_per_s": ns / solve_s,
+                                 "solves_per_s_with_upload": ns / full_s}
+    out["speedup_vs_one_at_a_time"] = sat / (ns / solve_s)
+    out["max_rel_diff_vs_fp64_one_at_a_time"] = err
+    return out
 
 
 def main():
@@ -391,6 +493,8 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--N", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=4096,
+                    help="requests of the serving stream (0: skip the serving measurement)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -90,8 +90,8 @@ struct b200la_server {
     int *d_tiles = nullptr, *h_tiles = nullptr;
     cudaGraphExec_t graph = nullptr;
     // kernel shape
-    int nw = 8, ctas_per_sm = 4, cpw = 2, iters = 16;
-    double active_cap = 256.0 * 1024 * 1024;
+    int nw = 8, ctas_per_sm = 2, cpw = 4, iters = 16;
+    double active_cap = 512.0 * 1024 * 1024;
     int max_active = 1024;
 
     std::mutex mu;
@@ -678,8 +678,8 @@ int autotune(b200la_server *S)
     struct Shape {
         int nw, cps, cpw;
     };
-    const Shape shapes[] = {{4, 8, 1}, {4, 8, 2},  {4, 16, 1}, {4, 16, 2}, {8, 4, 1}, {8, 4, 2},
-                            {8, 8, 1}, {8, 8, 2}, {8, 4, 4},  {4, 16, 4}, {8, 8, 4}};
+    const Shape shapes[] = {{8, 2, 2}, {8, 2, 4}, {8, 2, 8}, {4, 4, 2}, {4, 4, 4},
+                            {4, 4, 8}, {8, 4, 4}, {4, 8, 4}, {8, 3, 4}, {4, 6, 4}};
     float best = 1e30f;
     Shape pick{S->nw, S->ctas_per_sm, S->cpw};
     for (const Shape &sh : shapes) {
@@ -764,7 +764,7 @@ extern "C" int b200la_serve_start(const b200la_serve_config *cfg, b200la_server 
     if (c.max_slots <= 0) c.max_slots = 4096;
     if (c.max_active <= 0) c.max_active = 1024;
     if (c.iters_per_round <= 0) c.iters_per_round = 16;
-    if (c.active_bytes <= 0) c.active_bytes = 256.0 * 1024 * 1024;
+    if (c.active_bytes <= 0) c.active_bytes = 512.0 * 1024 * 1024;
     S->device = c.device;
     S->iters = c.iters_per_round;
     S->active_cap = c.active_bytes;
