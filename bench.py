@@ -140,6 +140,23 @@ def dict_spmv_bytes(n, nnz, vbytes):
     return vbytes * nnz + 2 * n + 4 * ((n + 31) // 32 + 1) + 2 * vbytes * n
 
 
+# --------------------------------------------------------------- ranks
+
+def reduce_max(x, dist, device):
+    """Max of a float over all ranks (x itself on a single process)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard(items, rank, world):
+    """Rank's share of a request stream: every world-th item from rank."""
+    return items[rank::world]
+
+
 # --------------------------------------------------------------- CPU baseline
 
 def cpu_counts(N):
@@ -248,10 +265,7 @@ def run_b200(args, rank, world, local_rank, dist):
             launches += r.launches
         ms = pf.timer_stop()
     res_mixed = dict(outer=r.outer, inner_total=r.iters, res0=r.res0, res=r.res, status=r.status)
-    if world > 1:
-        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = reduce_max(ms, dist if world > 1 else None, "cuda")
     ms_step = ms / args.steps
     value = world * args.steps / (ms / 1e3)
     x_mixed = x.numpy()
@@ -338,10 +352,7 @@ def run_b200(args, rank, world, local_rank, dist):
     for _ in range(args.steps):
         e2e_step()
     e2e_ms = pf.timer_stop()
-    if world > 1:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = reduce_max(e2e_ms, dist if world > 1 else None, "cuda")
     xh = np.ctypeslib.as_array(ctypes.cast(hx, ctypes.POINTER(ctypes.c_double)), (n,)).copy()
     e2e_ok = bool(np.array_equal(xh, x_mixed))
     L.b200la_free(pf.h, db)
@@ -376,7 +387,8 @@ def run_b200(args, rank, world, local_rank, dist):
         "clocks": clk.summary(),
     }
     if args.serve_requests > 0:
-        line["serving"] = serving_bench(b200, pf, args.serve_requests)
+        line["serving"] = serving_bench(b200, pf, args.serve_requests, rank=rank, world=world,
+                                        dist=dist if world > 1 else None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(row, col, val, b, res_mixed["outer"], res_mixed["inner_total"], fp64_iters)
         line["cpu_baseline"] = cb if cb else {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
@@ -385,15 +397,18 @@ def run_b200(args, rank, world, local_rank, dist):
     return line
 
 
-def serving_bench(b200, pf, nreq, sample=64, seed=2025):
+def serving_bench(b200, pf, nreq, sample=64, seed=2025, rank=0, world=1, dist=None):
     """The serving loop on the seeded request stream: saturation throughput
     (every request offered at t = 0), p50/p99 latency at Poisson arrival rates
     below saturation, and the drop-in FP64 Jacobi-CG solving a sample of the
-    same requests one at a time."""
+    same requests one at a time.  With several ranks every rank serves its
+    shard of the stream on its own GPU (replicas); the job's rate is all
+    requests over the slowest rank's time."""
     import importlib
     srv = importlib.import_module("hiflow3_b200.serving")
     fb = srv.FieldBank()
-    stream = srv.c5_stream(nreq, seed=seed)
+    stream = shard(srv.c5_stream(nreq, seed=seed), rank, world)
+    nreq = len(stream)
     kcache = {}
 
     def kcell(r):
@@ -420,9 +435,11 @@ def serving_bench(b200, pf, nreq, sample=64, seed=2025):
     st = s.stats()
     s.stop()
     sat = len(res) / t_sat
+    t_job = reduce_max(t_sat, dist if world > 1 else None, "cuda")
     shape = dict(warps=st["warps"], ctas_per_sm=st["ctas_per_sm"], chunks_per_warp=st["chunks_per_warp"])
     lat = [r["latency"] for r in res]
-    out = {"requests": len(res), "solves_per_s": sat, "wall_s": t_sat, "met_1e-10": sum(map(ok, res)),
+    out = {"requests": len(res) * world, "solves_per_s": len(res) * world / t_job, "wall_s": t_job,
+           "met_1e-10": sum(map(ok, res)),
            "latency_ms": {k: v * 1e3 for k, v in srv.percentiles(lat).items()},
            "iterations": int(sum(r["iters"] for r in res)), "rounds": st["rounds"],
            "batch_iterations": st["batch_iters"], "gpu_busy_s": st["busy_ms"] / 1e3,
