@@ -53,7 +53,7 @@ def load_workloads():
     return importlib.import_module("hiflow3_b200.workloads")
 
 
-def profiled_traffic(name="spmv_sell_f32_128cubed.md"):
+def profiled_traffic(name="spmv_stencil_f32_128cubed.md"):
     """DRAM bytes per launch of the dominant kernel from the committed ncu
     summary (dram__bytes_read.sum + dram__bytes_write.sum of one capture)."""
     import re
@@ -138,6 +138,15 @@ def dict_spmv_bytes(n, nnz, vbytes):
     32-row chunk, x read once, y written once (padding of short rows and the
     few-KB pattern table excluded)."""
     return vbytes * nnz + 2 * n + 4 * ((n + 31) // 32 + 1) + 2 * vbytes * n
+
+
+def stencil_spmv_bytes(n, nb, vbytes):
+    """Algorithmic bytes of one SpMV on the stencil layout: the values of
+    3 nb positions per row (zero-padded chunks of 32 rows; FP32 positions in
+    groups of four), x read once, y written once; no indices."""
+    w = 4 if vbytes == 4 else 1
+    slots = (3 * nb + w - 1) // w * w
+    return vbytes * slots * 32 * ((n + 31) // 32) + 2 * vbytes * n
 
 
 # --------------------------------------------------------------- ranks
@@ -315,13 +324,36 @@ def run_b200(args, rank, world, local_rank, dist):
         for _ in range(reps):
             L.b200la_spmv_dot(pf.h, A.h, xx.ptr, yy.ptr, ctypes.c_void_p(d.data_ptr()))
         t_ms = pf.timer_stop() / reps
-        uses_dict = A.info()["uses_pattern_dictionary"]
-        by = dict_spmv_bytes(n, nnz, vbytes) if uses_dict else spmv_bytes(n, nnz, vbytes)
-        return by, t_ms, by / (t_ms * 1e-3) / 1e9
+        storage = A.info()["storage"]
+        by = {"csr": spmv_bytes(n, nnz, vbytes), "dictionary": dict_spmv_bytes(n, nnz, vbytes),
+              "stencil": stencil_spmv_bytes(n, 9, vbytes)}[storage]
+        return by, t_ms, by / (t_ms * 1e-3) / 1e9, storage
 
-    by64, t64, gbs64 = spmv_rate(A64, 8)
-    by32, t32, gbs32 = spmv_rate(A32, 4)
+    by64, t64, gbs64, st64 = spmv_rate(A64, 8)
+    by32, t32, gbs32, st32 = spmv_rate(A32, 4)
+    # the FP64 operator with explicit column indices (CSR) as well: the
+    # reference's storage; FP64 CG on it for comparison
+    os.environ["B200LA_STENCIL"] = "0"
+    A64c = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    del os.environ["B200LA_STENCIL"]
+    by64c, t64c, gbs64c, st64c = spmv_rate(A64c, 8)
+    cgc = b200.CG(pf)
+    cgc.SetupOperator(A64c)
+    cgc.SetupPreconditioner(b200.Preconditioner.Jacobi(pf, A64c))
+    cgc.InitControl(200000, 0.0, 1e-10, 1e6)
+    xc = pf.vector(n)
+    cgc.Solve(bv, xc)
+    pf.sync()
+    pf.timer_start()
+    for _ in range(k64):
+        xc.Zeros()
+        cgc.Solve(bv, xc)
+    fp64c_ms = pf.timer_stop() / k64
+    fp64c_iters = cgc.iter()
+    del A64c, cgc, xc
     peak, peak_kind = measured_peaks()
+    # SURVEY units: one FP64 / FP32 SpMV of this operator (CSR algorithmic bytes)
+    unit64, unit32 = spmv_bytes(n, nnz, 8), spmv_bytes(n, nnz, 4)
 
     # end to end through the C ABI: host b in, host x out, per step
     import ctypes
@@ -371,21 +403,31 @@ def run_b200(args, rank, world, local_rank, dist):
                   "relres_true": relres, "err_vs_fp64_solution": err},
         "fp64_cg": {"ms": fp64_ms, "iters": fp64_iters, "err_vs_fp64_solution": err64},
         "mixed_speedup_vs_fp64": fp64_ms / ms_step,
-        "spmv": {"fp64_csr_gbs": gbs64, "fp64_csr_us": t64 * 1e3, "fp64_csr_bytes": by64,
-                 "fp64_csr_frac_of_peak": gbs64 / peak,
-                 "fp32_dict_gbs": gbs32, "fp32_dict_us": t32 * 1e3, "fp32_dict_bytes": by32},
+        "fp64_cg_csr": {"ms": fp64c_ms, "iters": fp64c_iters,
+                        "note": "FP64 Jacobi-CG with the operator in CSR (explicit column indices)"},
+        "mixed_speedup_vs_fp64_csr": fp64c_ms / ms_step,
+        "spmv": {"fp64": {"storage": st64, "us": t64 * 1e3, "gbs": gbs64, "bytes": by64, "frac_of_peak": gbs64 / peak,
+                          "csr_unit_gbs": unit64 / (t64 * 1e-3) / 1e9},
+                 "fp64_csr": {"us": t64c * 1e3, "gbs": gbs64c, "bytes": by64c, "frac_of_peak": gbs64c / peak},
+                 "fp32_inner": {"storage": st32, "us": t32 * 1e3, "gbs": gbs32, "bytes": by32,
+                                "frac_of_peak": gbs32 / peak, "csr_unit_gbs": unit32 / (t32 * 1e-3) / 1e9},
+                 "csr_unit_bytes": {"fp64": unit64, "fp32": unit32}},
         "roofline": {"bound": "hbm",
-                     "kernel": "spmv_sell_kernel<float, EPI_DOT_X>: FP32 dictionary SpMV + p.Ap of the inner CG",
+                     "kernel": f"FP32 SpMV + p.Ap of the inner CG ({st32} layout)",
                      "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,
                      "peak_source": peak_kind, "bytes_per_launch": by32,
+                     "bytes_basis": "the layout's own bytes: values, x once, y once (no indices)",
+                     "csr_unit_bytes_per_launch": unit32, "achieved_csr_unit": unit32 / (t32 * 1e-3) / 1e9,
                      "traffic": profiled_traffic() if args.N == 128 else None,
-                     "traffic_source": "profiles/spmv_sell_f32_128cubed.md (ncu, one launch)"},
+                     "traffic_source": "profiles/spmv_stencil_f32_128cubed.md (ncu, one launch)"},
         "gpu_launches": launches,
         "e2e": {"value": world * args.steps / (e2e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": 8 * n,
                 "d2h_bytes_per_step": 8 * n, "matches_device_run": e2e_ok},
         "setup_s": {"assembly": t_asm, "upload_and_cast": t_up},
         "clocks": clk.summary(),
     }
+    if not args.no_configs:
+        line["configs"] = other_configs(b200, pf, wl)
     if args.serve_requests > 0:
         line["serving"] = serving_bench(b200, pf, args.serve_requests, rank=rank, world=world,
                                         dist=dist if world > 1 else None)
@@ -395,6 +437,78 @@ def run_b200(args, rank, world, local_rank, dist):
                                               "sample": "oracle/_ref missing"}
     pf.close()
     return line
+
+
+def other_configs(b200, pf, wl):
+    """Time to solution of the two other device configurations: C2 (3-D
+    Poisson 128^3, 8-colour MC-SGS PCG to 1e-8, FP64) and C4 (2-D
+    convection-diffusion 512^2, GMRES(30) + level-scheduled ILU(0) to 1e-9,
+    FP64 and mixed: FP32 factors and Arnoldi inside FP64 defect correction)."""
+    out = {}
+    # C2
+    row, col, val, b, _ = wl.system(b200, "c2")
+    t0 = time.perf_counter()
+    P = b200.Preconditioner.MultiColoringSGS(pf, row, col, val)
+    pf.sync()
+    t_setup = time.perf_counter() - t0
+    bp = b[P.perm]
+    cg = b200.CG(pf)
+    cg.SetupOperator(P.A_perm)
+    cg.SetupPreconditioner(P)
+    cg.InitControl(100000, 0.0, 1e-8, 1e6)
+    bv, x = pf.vector(bp), pf.vector(len(bp))
+    cg.Solve(bv, x)
+    x.Zeros()
+    pf.sync()
+    pf.timer_start()
+    cg.Solve(bv, x)
+    ms = pf.timer_stop()
+    out["c2_mcsgs_cg_fp64"] = {"ms": ms, "iters": cg.iter(), "status": cg.result.status,
+                               "colours": P.nblocks, "setup_s": t_setup}
+    del P, cg, bv, x
+    # C4
+    row, col, val, b, _ = wl.system(b200, "c4")
+    t0 = time.perf_counter()
+    P64 = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS)
+    P32 = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS, dtype=b200.F32)
+    pf.sync()
+    t_setup = time.perf_counter() - t0
+    bp = b[P64.perm]
+    bv = pf.vector(bp)
+    gm = b200.GMRES(pf, 30)
+    gm.SetupOperator(P64.A_perm)
+    gm.SetupPreconditioner(P64)
+    gm.InitControl(100000, 0.0, 1e-9, 1e6)
+    x = pf.vector(len(bp))
+    gm.Solve(bv, x)
+    x.Zeros()
+    pf.sync()
+    pf.timer_start()
+    gm.Solve(bv, x)
+    ms64 = pf.timer_stop()
+    x64 = x.numpy()
+    it64 = gm.iter()
+    m = b200.MPIR(pf, max_outer=50)
+    m.SetupOperator(P64.A_perm)
+    m.SetupLowPrecisionOperator(P32.A_perm)
+    m.SetupInnerGMRES(30, P32)
+    m.InitControl(50, 0.0, 1e-9, 1e6)
+    m.InitInnerControl(100000, 0.0, 1e-4, 1e6)
+    xm = pf.vector(len(bp))
+    m.Solve(bv, xm)
+    xm.Zeros()
+    pf.sync()
+    pf.timer_start()
+    m.Solve(bv, xm)
+    msm = pf.timer_stop()
+    rv = pf.vector(len(bp))
+    true = float(np.sqrt(P64.A_perm.Residual(bv, xm, rv)) / np.linalg.norm(bp))
+    out["c4_gmres_ilu_fp64"] = {"ms": ms64, "iters": it64, "levels": P64.nblocks, "setup_s": t_setup}
+    out["c4_gmres_ilu_mixed"] = {"ms": msm, "outer": m.result.outer, "inner_iters": m.result.iters,
+                                 "relres_true": true,
+                                 "rel_diff_vs_fp64": float(np.linalg.norm(xm.numpy() - x64) / np.linalg.norm(x64)),
+                                 "speedup_vs_fp64": ms64 / msm}
+    return out
 
 
 def serving_bench(b200, pf, nreq, sample=64, seed=2025, rank=0, world=1, dist=None):
@@ -510,6 +624,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--N", type=int, default=128)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-configs", action="store_true", help="skip the C2 / C4 time-to-solution runs")
     ap.add_argument("--serve-requests", type=int, default=4096,
                     help="requests of the serving stream (0: skip the serving measurement)")
     args = ap.parse_args()

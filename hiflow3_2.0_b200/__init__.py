@@ -170,6 +170,8 @@ def lib():
         "b200la_cg_hist": ([_P, _P, _P, _P, _P, C.POINTER(Control), C.POINTER(Result), _P, _I], _I),
         "b200la_gmres": ([_P, _P, _P, _I, _P, _P, C.POINTER(Control), C.POINTER(Result)], _I),
         "b200la_mpir": ([_P, _P, _P, _P, _P, C.POINTER(Control), C.POINTER(Control), _I, C.POINTER(Result)], _I),
+        "b200la_mpir_gmres": ([_P, _P, _P, _P, _I, _P, _P, C.POINTER(Control), C.POINTER(Control), _I,
+                               C.POINTER(Result)], _I),
         "b200la_q1_assemble_device": ([_P, _I, _I, _I, _P, _D, _P, _P, _P, _P], _I),
         "b200la_q1_rhs_device": ([_P, C.c_uint64, _I, _I, _P], _I),
         "b200la_serve_start": ([C.POINTER(ServeConfig), C.POINTER(_P)], _I),
@@ -494,6 +496,7 @@ class CSR_lMatrix:
         npat, uses = C.c_int(), C.c_int()
         self.pf.check(lib().b200la_csr_format(self.h, C.byref(npat), C.byref(uses)))
         out["row_patterns"], out["uses_pattern_dictionary"] = npat.value, bool(uses.value)
+        out["storage"] = {0: "csr", 1: "dictionary", 2: "stencil"}[uses.value]
         return out
 
     def CastFrom(self, dtype):
@@ -658,23 +661,36 @@ class GMRES(_Solver):
 
 class MPIR(_Solver):
     """MPIR<LAD_high, LAD_low> (src/linear_solver/mpir.cc): FP64 defect correction
-    around an FP32 Jacobi-CG."""
+    around an FP32 Jacobi-CG, or around an FP32 GMRES(m) with an FP32
+    preconditioner (SetupInnerGMRES)."""
 
     def __init__(self, platform, max_outer=50):
         super().__init__(platform)
         self.inner = Control(10000, 0.0, 1e-4, 1e6)
         self.max_outer = max_outer
         self.op32 = None
+        self.gmres_m = 0
+        self.prec32 = None
 
     def SetupLowPrecisionOperator(self, A32):
         self.op32 = A32
+
+    def SetupInnerGMRES(self, m, precond32=None):
+        self.gmres_m = m
+        self.prec32 = precond32
 
     def InitInnerControl(self, maxits, abstol, reltol, divtol):
         self.inner = Control(maxits, abstol, reltol, divtol)
 
     def Solve(self, b, x):
         A32 = self.op32.h if self.op32 is not None else None
-        rc = lib().b200la_mpir(self.pf.h, self.op.h, A32, b.ptr, x.ptr, C.byref(self.ctl), C.byref(self.inner),
-                               self.max_outer, C.byref(self.result))
+        if self.gmres_m > 0:
+            P32 = self.prec32.h if self.prec32 is not None else None
+            rc = lib().b200la_mpir_gmres(self.pf.h, self.op.h, A32, P32, self.gmres_m, b.ptr, x.ptr,
+                                         C.byref(self.ctl), C.byref(self.inner), self.max_outer,
+                                         C.byref(self.result))
+        else:
+            rc = lib().b200la_mpir(self.pf.h, self.op.h, A32, b.ptr, x.ptr, C.byref(self.ctl), C.byref(self.inner),
+                                   self.max_outer, C.byref(self.result))
         self.pf.check(rc, "MPIR::Solve")
         return self.result.status

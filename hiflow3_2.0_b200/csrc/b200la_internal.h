@@ -32,6 +32,8 @@ struct b200la_ctx {
     cudaEvent_t tev0 = nullptr, tev1 = nullptr;   // b200la_timer_start / stop
     void *work = nullptr;           // solver workspace
     size_t work_bytes = 0;
+    void *work_outer = nullptr;     // outer-loop workspace of the GMRES defect correction
+    size_t work_outer_bytes = 0;
     long long launches = 0;         // kernels launched through this context
     std::vector<GraphEntry> graphs; // captured solver iteration batches
     std::string msg;
@@ -65,6 +67,12 @@ struct b200la_csr {
     size_t sell_len = 0;
     int sell_lmax = 0;                // longest chunk row length
     int sell_tma = 0;                 // bulk-copy tiles (B200LA_SELL_TMA at creation)
+    // stencil layout (square operators whose row patterns all lie in one set
+    // of 3 or 9 bands of three consecutive column offsets): see kernels.cuh
+    std::vector<int> st_union;        // the union of the row patterns' offsets (host)
+    void *st_val = nullptr;
+    int st_nb = 0;                    // bands (0: no stencil layout)
+    int st_use = 0;                   // SpMV of the whole operator runs on it
 };
 
 struct b200la_precond {
@@ -90,6 +98,7 @@ int ctx_fail(const b200la_ctx *ctx, int code, const char *what, cudaError_t e);
 b200::Scratch ctx_scratch(const b200la_ctx *ctx);
 b200::CsrView csr_view(const b200la_csr *A);
 int ctx_work(b200la_ctx *ctx, size_t bytes, void **out);
+int ctx_work_outer(b200la_ctx *ctx, size_t bytes, void **out);
 int ctx_check_device_error(b200la_ctx *ctx);
 int spmv_run(b200la_ctx *ctx, const b200la_csr *A, const b200::Seg &seg, b200::SpmvOp op);
 int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row, const int *col, const void *val,

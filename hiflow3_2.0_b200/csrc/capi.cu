@@ -63,6 +63,15 @@ static bool pattern_policy(int dtype)
     return mode == 2 || (mode == 1 && dtype == B200LA_F32);
 }
 
+// Whether SpMV of the whole operator runs on the stencil layout (when the
+// matrix has one).  B200LA_STENCIL = 0: never, 1: FP32 only, 2: always (default).
+static bool stencil_policy(int dtype)
+{
+    const char *e = std::getenv("B200LA_STENCIL");
+    const int mode = e ? std::atoi(e) : 2;
+    return mode == 2 || (mode == 1 && dtype == B200LA_F32);
+}
+
 CsrView csr_view(const b200la_csr *A)
 {
     CsrView v;
@@ -93,6 +102,11 @@ CsrView csr_view(const b200la_csr *A)
     v.sell_lmax = A->sell_lmax;
     v.sell_tma = A->sell_tma;
     v.n_cols = A->m;
+    v.n_rows = A->n;
+    v.st_val = A->st_val;
+    v.st_nb = A->st_nb;
+    v.st_use = A->st_use && A->st_val != nullptr;
+    for (int b = 0; b < kMaxBands; ++b) v.st_center[b] = b < A->st_nb ? A->st_union[3 * b + 1] : 0;
     return v;
 }
 
@@ -110,6 +124,24 @@ int ctx_work(b200la_ctx *ctx, size_t bytes, void **out)
         ctx->work_bytes = bytes;
     }
     *out = ctx->work;
+    return B200LA_OK;
+}
+
+// A second workspace for loops that call a solver which itself uses ctx_work.
+int ctx_work_outer(b200la_ctx *ctx, size_t bytes, void **out)
+{
+    if (bytes > ctx->work_outer_bytes) {
+        if (ctx->work_outer) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(ctx->work_outer);
+            ctx->work_outer = nullptr;
+            ctx->work_outer_bytes = 0;
+        }
+        cudaError_t e = cudaMalloc(&ctx->work_outer, bytes);
+        if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_ALLOC, "outer workspace", e);
+        ctx->work_outer_bytes = bytes;
+    }
+    *out = ctx->work_outer;
     return B200LA_OK;
 }
 
@@ -166,6 +198,7 @@ extern "C" int b200la_destroy(b200la_ctx *ctx)
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     graph_cache_clear(ctx);
     if (ctx->work) cudaFree(ctx->work);
+    if (ctx->work_outer) cudaFree(ctx->work_outer);
     if (ctx->partials) cudaFree(ctx->partials);
     if (ctx->ticket) cudaFree(ctx->ticket);
     if (ctx->dev_err) cudaFree(ctx->dev_err);
@@ -401,6 +434,40 @@ static int build_sell(b200la_ctx *ctx, b200la_csr *A)
     return B200LA_OK;
 }
 
+// The stencil layout of a square operator whose row patterns' offsets (their
+// union `uni`, ascending) form 3 or 9 bands of three consecutive offsets, with
+// at most 30 % zero padding.  Values are (re)scattered from the CSR.
+static void stencil_plan(b200la_csr *A, const std::vector<int> &uni)
+{
+    A->st_nb = 0;
+    A->st_union.clear();
+    const int L = (int)uni.size();
+    if (A->n != A->m || A->n == 0 || (L != 9 && L != 27)) return;
+    for (int b = 0; b < L / 3; ++b)
+        if (uni[3 * b + 1] != uni[3 * b] + 1 || uni[3 * b + 2] != uni[3 * b] + 2) return;
+    const double padded = (double)((A->n + 31) / 32) * 32 * L;
+    if (padded > 1.30 * (double)A->nnz) return;
+    A->st_union = uni;
+    A->st_nb = L / 3;
+}
+
+static int build_stencil(b200la_ctx *ctx, b200la_csr *A)
+{
+    if (!A->st_nb) return B200LA_OK;
+    const size_t es = dsize(A->dtype), len = stencil_len(A->n, A->st_nb, A->dtype);
+    cudaError_t e;
+    if (!A->st_val) {
+        if ((e = cudaMalloc(&A->st_val, es * len))) return ctx_fail(ctx, B200LA_ERR_ALLOC, "stencil layout", e);
+        A->bytes += es * len;
+    }
+    if ((e = cudaMemsetAsync(A->st_val, 0, es * len, ctx->stream)) ||
+        (e = launch_csr_to_stencil(A->dtype, A->n, A->row, A->col, A->val, A->st_union.data(), A->st_nb, A->st_val,
+                                   ctx->stream)) ||
+        (e = cudaStreamSynchronize(ctx->stream)))
+        return ctx_fail(ctx, B200LA_ERR_CUDA, "stencil layout", e);
+    return B200LA_OK;
+}
+
 static int upload_lines(b200la_ctx *ctx, b200la_csr *A, const std::vector<int> &ls, const std::vector<int> &lsp,
                         const std::vector<int> &el, const std::vector<int> &elo)
 {
@@ -532,7 +599,15 @@ int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row,
                 return rc;
             }
         }
-        const int rc = build_sell(ctx, A);
+        int rc = build_sell(ctx, A);
+        if (!rc && n_seg == 0) {
+            std::vector<int> uni(pdel);
+            std::sort(uni.begin(), uni.end());
+            uni.erase(std::unique(uni.begin(), uni.end()), uni.end());
+            stencil_plan(A, uni);
+            A->st_use = stencil_policy(dtype);
+            rc = build_stencil(ctx, A);
+        }
         if (rc) {
             b200la_csr_destroy(A);
             return rc;
@@ -574,6 +649,7 @@ extern "C" int b200la_csr_destroy(b200la_csr *A)
     if (A->entry_lo) cudaFree(A->entry_lo);
     if (A->sell_off) cudaFree(A->sell_off);
     if (A->sell_val) cudaFree(A->sell_val);
+    if (A->st_val) cudaFree(A->st_val);
     delete A;
     return B200LA_OK;
 }
@@ -595,6 +671,8 @@ extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, 
     B->sell_off = nullptr;
     B->sell_val = nullptr;
     B->sell_len = 0;
+    B->st_val = nullptr;
+    B->st_use = stencil_policy(dtype);
     const size_t pad = 8, es = dsize(dtype);
     cudaError_t e;
     if (A->pid) {
@@ -636,7 +714,8 @@ extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, 
         b200la_csr_destroy(B);
         return ctx_fail(ctx, B200LA_ERR_CUDA, "csr_cast", e);
     }
-    const int rc = build_sell(ctx, B);
+    int rc = build_sell(ctx, B);
+    if (!rc) rc = build_stencil(ctx, B);
     if (rc) {
         b200la_csr_destroy(B);
         return rc;
@@ -663,7 +742,7 @@ extern "C" int b200la_csr_format(const b200la_csr *A, int *npat, int *uses_dict)
 {
     if (!A) return B200LA_ERR_ARG;
     if (npat) *npat = A->pid ? A->npat : 0;
-    if (uses_dict) *uses_dict = (A->pid && A->use_pat) ? 1 : 0;
+    if (uses_dict) *uses_dict = (A->st_use && A->st_val) ? 2 : (A->pid && A->use_pat) ? 1 : 0;
     return B200LA_OK;
 }
 
@@ -683,7 +762,8 @@ extern "C" int b200la_csr_set_values(b200la_ctx *ctx, b200la_csr *A, const void 
     if (!ctx || !A || (A->nnz && !val)) return B200LA_ERR_ARG;
     if (A->nnz) CK(cudaMemcpyAsync(A->val, val, dsize(A->dtype) * A->nnz, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    return build_sell(ctx, A);
+    const int rc = build_sell(ctx, A);
+    return rc ? rc : build_stencil(ctx, A);
 }
 
 extern "C" int b200la_csr_invdiag(b200la_ctx *ctx, const b200la_csr *A, void *out)

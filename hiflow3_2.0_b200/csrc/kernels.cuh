@@ -73,6 +73,21 @@ enum Fin : int {
     FIN_RES_INIT = 3,    // st->rr = v; st->res = sqrt(v); st->status = Check(0, res)
 };
 
+constexpr int kMaxBands = 9;
+// Positions per lane and load in the stencil layout: FP32 values are grouped
+// by four (position k of row 32 c + lane at
+// 32 G W c + 32 W (k / W) + W lane + k % W, G = ceil(3 nb / W)), FP64 by one.
+template <typename T>
+__host__ __device__ constexpr int stencil_group()
+{
+    return sizeof(T) == 4 ? 4 : 1;
+}
+inline size_t stencil_len(int n, int nb, int dtype)
+{
+    const int W = dtype == 1 ? 4 : 1, G = (3 * nb + W - 1) / W;
+    return (size_t)((n + 31) / 32) * 32 * G * W;
+}
+
 struct CsrView {
     const int *row;
     const int *col;
@@ -101,6 +116,15 @@ struct CsrView {
     int sell_lmax;   // longest chunk (values per row) of the sliced layout
     int sell_tma;    // bulk-copy tiles for the sliced layout
     int n_cols;      // length of x
+    int n_rows;
+    // stencil layout (null when absent): the row patterns' offsets all lie in
+    // st_nb bands {c - 1, c, c + 1} (centres st_center[], ascending); the
+    // value of row i = 32 c + lane at offset st_center[b] + m - 1 is position
+    // k = 3 b + m of the row (see stencil_group for the address), zero where
+    // the row has no such column
+    const void *st_val;
+    int st_nb, st_use;
+    int st_center[kMaxBands];
 };
 
 constexpr int kMaxPatterns = 1024;
@@ -132,6 +156,10 @@ cudaError_t spmv_configure();
 // Scatter CSR values (row order) into the sliced layout (zero-filled before).
 cudaError_t launch_csr_to_sell(int dtype, int n, const int *row, const void *val, const int *sell_off, void *sv,
                                cudaStream_t st);
+// Scatter CSR values into the stencil layout (zero-filled before); uni holds
+// the 3 nb offsets of the bands in ascending order.
+cudaError_t launch_csr_to_stencil(int dtype, int n, const int *row, const int *col, const void *val, const int *uni,
+                                  int nb, void *out, cudaStream_t st);
 cudaError_t launch_spmv(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st);
 
 // ---- BLAS1 (dtype 0 double, 1 float; scalars in double) ----

@@ -213,40 +213,53 @@ __device__ __forceinline__ T sell_row(const int *__restrict__ cp, const T *__res
 // are added in column order, each gathered value formed by gather(j) exactly
 // as a direct gather would.  Columns outside [0, n) belong to zero entries
 // and are clamped into range.
-template <typename T, int DIM, typename G>
-__device__ __forceinline__ T stencil_row(const T *__restrict__ vp, int r0, int lane, int n, int P, uint64_t pol,
-                                         G gather)
+template <typename T, int DIM, int U, typename G>
+__device__ __forceinline__ void stencil_rows(const T *__restrict__ val, int L, const int (&cc)[U], int lane, int n,
+                                             int P, uint64_t pol, G gather, T (&s)[U])
 {
     constexpr int NB = DIM == 3 ? 9 : 3;
-    const int i = r0 + lane;
     const bool edge = lane == 0 || lane == 31;
-    const int he = lane == 0 ? r0 - 1 : r0 + 32;     // halo column before the band offset
-    T s = T(0);
+#pragma unroll
+    for (int u = 0; u < U; ++u) s[u] = T(0);
 #pragma unroll
     for (int b0 = 0; b0 < NB; b0 += 3) {
-        T a[9], w[3], h[3];
+        T a[U][9], w[U][3], h[U][3];
 #pragma unroll
-        for (int bb = 0; bb < 3; ++bb) {
-            const int band = b0 + bb;
-            const int d = DIM == 3 ? ((band / 3 - 1) * P + (band % 3 - 1)) * P : (band - 1) * P;
+        for (int u = 0; u < U; ++u) {
+            const int r0 = cc[u] * kChunk, i = r0 + lane;
+            const int he = lane == 0 ? r0 - 1 : r0 + 32;     // halo column before the band offset
+            const T *vp = val + (size_t)cc[u] * kChunk * L + lane;
 #pragma unroll
-            for (int m = 0; m < 3; ++m) a[3 * bb + m] = ld_stream(vp + 32 * (3 * band + m), pol);
-            w[bb] = gather(min(max(i + d, 0), n - 1));
-            h[bb] = edge ? gather(min(max(he + d, 0), n - 1)) : T(0);
+            for (int bb = 0; bb < 3; ++bb) {
+                const int band = b0 + bb;
+                const int d = DIM == 3 ? ((band / 3 - 1) * P + (band % 3 - 1)) * P : (band - 1) * P;
+#pragma unroll
+                for (int m = 0; m < 3; ++m) a[u][3 * bb + m] = ld_stream(vp + 32 * (3 * band + m), pol);
+                w[u][bb] = gather(min(max(i + d, 0), n - 1));
+                h[u][bb] = edge ? gather(min(max(he + d, 0), n - 1)) : T(0);
+            }
         }
 #pragma unroll
-        for (int bb = 0; bb < 3; ++bb) {
-            T left = __shfl_up_sync(0xffffffffu, w[bb], 1);
-            T right = __shfl_down_sync(0xffffffffu, w[bb], 1);
-            if (lane == 0) left = h[bb];
-            if (lane == 31) right = h[bb];
-            s += a[3 * bb] * left;
-            s += a[3 * bb + 1] * w[bb];
-            s += a[3 * bb + 2] * right;
+        for (int u = 0; u < U; ++u) {
+#pragma unroll
+            for (int bb = 0; bb < 3; ++bb) {
+                T left = __shfl_up_sync(0xffffffffu, w[u][bb], 1);
+                T right = __shfl_down_sync(0xffffffffu, w[u][bb], 1);
+                if (lane == 0) left = h[u][bb];
+                if (lane == 31) right = h[u][bb];
+                s[u] += a[u][3 * bb] * left;
+                s[u] += a[u][3 * bb + 1] * w[u][bb];
+                s[u] += a[u][3 * bb + 2] * right;
+            }
         }
+        // keep one group of three bands in flight at a time (register budget)
+        if (b0 + 3 < NB) asm volatile("" ::: "memory");
     }
-    return s;
 }
+
+template <typename T, typename G>
+__device__ __noinline__ T row_spmv_indexed(const SysDesc &d, const T *__restrict__ val, int c, int lane,
+                                           uint64_t pol, G gather);
 
 // Row 32 c + lane of A v, v given by gather(j).  SELL / STENCIL: one thread
 // per row, entries in column order.  CSRW: one warp per row, lanes strided
@@ -257,11 +270,22 @@ __device__ __forceinline__ T row_spmv(const SysDesc &d, const T *__restrict__ va
 {
     const int fmt = d.fmt, n = d.n;
     if (fmt == FMT_STENCIL) {
-        const int r0 = c * kChunk, P = d.sP;
-        const T *vp = val + (size_t)c * kChunk * d.sL + lane;
-        if (d.sdim == 3) return stencil_row<T, 3>(vp, r0, lane, n, P, pol, gather);
-        return stencil_row<T, 2>(vp, r0, lane, n, P, pol, gather);
+        const int cc[1] = {c};
+        T s[1];
+        if (d.sdim == 3) stencil_rows<T, 3, 1>(val, d.sL, cc, lane, n, d.sP, pol, gather, s);
+        else stencil_rows<T, 2, 1>(val, d.sL, cc, lane, n, d.sP, pol, gather, s);
+        return s[0];
     }
+    return row_spmv_indexed<T>(d, val, c, lane, pol, gather);
+}
+
+// SELL and CSRW rows (uploaded CSR requests), out of line so that their
+// registers do not constrain the stencil path.
+template <typename T, typename G>
+__device__ __noinline__ T row_spmv_indexed(const SysDesc &d, const T *__restrict__ val, int c, int lane,
+                                           uint64_t pol, G gather)
+{
+    const int fmt = d.fmt, n = d.n;
     const int *off = d.off, *col = d.col;
     if (fmt == FMT_SELL) {
         const int b = __ldg(off + c), L = (__ldg(off + c + 1) - b) >> 5;
@@ -296,7 +320,29 @@ __device__ __forceinline__ void k1_chunks(const TileCtx &c, const T *val, uint64
     T *ap = static_cast<T *>(c.d.ap);
     double *part = c.d.part;
     auto gather = [=](int j) { return pnew_at(beta, po, z, j); };
-    for (int ch = c.t.c0 + warp; ch < c.t.c1; ch += NW) {
+    int ch = c.t.c0 + warp;
+    if (c.d.fmt == FMT_STENCIL && c.d.sdim == 2) {
+        // 2-D stencil: two chunks per warp with their loads in flight together
+        for (; ch + NW < c.t.c1; ch += 2 * NW) {
+            const int cc[2] = {ch, ch + NW};
+            T s2[2];
+            stencil_rows<T, 2, 2>(val, c.d.sL, cc, lane, n, c.d.sP, pol, gather, s2);
+#pragma unroll
+            for (int u = 0; u < 2; ++u) {
+                const int i = cc[u] * kChunk + lane;
+                double dp = 0.0;
+                if (i < n) {
+                    const T pi = pnew_at(beta, po, z, i);
+                    pn[i] = pi;
+                    ap[i] = s2[u];
+                    dp = (double)(pi * s2[u]);
+                }
+                dp = warp_sum(dp);
+                if (lane == 0) part[cc[u]] = dp;
+            }
+        }
+    }
+    for (; ch < c.t.c1; ch += NW) {
         const int i = ch * kChunk + lane;
         const T s = row_spmv<T>(c.d, val, ch, lane, pol, gather);
         double dp = 0.0;

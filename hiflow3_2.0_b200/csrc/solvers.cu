@@ -371,6 +371,98 @@ extern "C" int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_
     return ctx_check_device_error(ctx);
 }
 
+// ------------------------------------------------------------------ MPIR with a GMRES correction
+
+extern "C" int b200la_mpir_gmres(b200la_ctx *ctx, const b200la_csr *A64, const b200la_csr *A32,
+                                 const b200la_precond *P32, int m, const double *b, double *x,
+                                 const b200la_control *outer, const b200la_control *inner, int max_outer,
+                                 b200la_result *res)
+{
+    if (!ctx || !A64 || !A32 || !b || !x || !outer || !inner || m < 1 || max_outer < 0 ||
+        A64->dtype != B200LA_F64 || A32->dtype != B200LA_F32 || A64->n != A64->m || A32->n != A64->n ||
+        (P32 && (P32->dtype != B200LA_F32 || P32->n != A64->n)))
+        return ctx_fail(ctx, B200LA_ERR_ARG, "mpir_gmres: invalid argument", cudaSuccess);
+    const int n = A64->n;
+    const size_t v8 = ((8 * (size_t)std::max(n, 1) + 255) / 256) * 256, v4 = ((4 * (size_t)std::max(n, 1) + 255) / 256) * 256;
+    void *wk;
+    int rc = ctx_work_outer(ctx, v8 + 2 * v4, &wk);
+    if (rc) return rc;
+    char *base = static_cast<char *>(wk);
+    double *r = reinterpret_cast<double *>(base);
+    float *rl = reinterpret_cast<float *>(base + v8);
+    float *cl = reinterpret_cast<float *>(base + v8 + v4);
+    const long long l0 = ctx->launches;
+    // own events: the inner GMRES times itself with the context's
+    struct Ev {
+        cudaEvent_t a = nullptr, b = nullptr;
+        ~Ev()
+        {
+            if (a) cudaEventDestroy(a);
+            if (b) cudaEventDestroy(b);
+        }
+    } ev;
+    SK(cudaEventCreate(&ev.a));
+    SK(cudaEventCreate(&ev.b));
+    SK(cudaEventRecord(ev.a, ctx->stream));
+    auto residual = [&](double *out) -> int {
+        // r = b - A x in FP64 and ||r||   (mpir.cc:125-128, 271-273)
+        SpmvOp op;
+        op.epi = EPI_RESID;
+        op.fin = FIN_STORE;
+        op.x = x;
+        op.y = r;
+        op.b = b;
+        op.dot_out = ctx->dscal;
+        int r2 = spmv_run(ctx, A64, A64->all, op);
+        if (r2) return r2;
+        SK(cudaMemcpyAsync(ctx->hscal, ctx->dscal, sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        SK(cudaStreamSynchronize(ctx->stream));
+        *out = std::sqrt(ctx->hscal[0]);
+        return B200LA_OK;
+    };
+    double rnorm;
+    rc = residual(&rnorm);
+    if (rc) return rc;
+    const double res0 = rnorm;
+    int n_outer = 0, inner_total = 0, inner_launches = 0;
+    while (rnorm > outer->abstol && rnorm > outer->reltol * res0 && rnorm < outer->divtol && n_outer < max_outer) {
+        ++n_outer;
+        // resl = (float) resh; corl = 0   (mpir.cc:169-170)
+        SK(launch_cast_residual(n, r, rl, cl, ctx->stream));
+        ctx->launches += 1;
+        // low-precision error correction: GMRES(m) on A32 with P32 (mpir.cc:193)
+        b200la_result ir;
+        std::memset(&ir, 0, sizeof ir);
+        rc = b200la_gmres(ctx, A32, P32, m, rl, cl, inner, &ir);
+        if (rc) return rc;
+        inner_total += ir.iters;
+        inner_launches += ir.launches;
+        // x += (double) corl   (mpir.cc:223, 253)
+        SK(launch_add_correction(n, cl, x, ctx->stream));
+        ctx->launches += 1;
+        rc = residual(&rnorm);
+        if (rc) return rc;
+    }
+    SK(cudaEventRecord(ev.b, ctx->stream));
+    SK(cudaEventSynchronize(ev.b));
+    float ms = 0.f;
+    SK(cudaEventElapsedTime(&ms, ev.a, ev.b));
+    if (res) {
+        res->iters = inner_total;
+        res->outer = n_outer;
+        res->res0 = res0;
+        res->res = rnorm;
+        res->status = rnorm < outer->abstol ? B200LA_SUCCESS_ABS
+                      : rnorm < outer->reltol * res0 ? B200LA_SUCCESS_REL
+                      : rnorm >= outer->divtol     ? B200LA_FAIL_DIV
+                                                   : B200LA_FAIL_MAXITS;
+        res->launches = (int)(ctx->launches - l0);
+        res->solve_ms = ms;
+    }
+    (void)inner_launches;
+    return ctx_check_device_error(ctx);
+}
+
 // ------------------------------------------------------------------ GMRES
 
 namespace {

@@ -515,9 +515,129 @@ void launch_tile(int grid, const CsrView &A, const Seg &seg, const SpmvOp &op, c
         <<<grid, kBlock, ST * TileSmem<CAP>::template stage_bytes<T>() + ST * 8, st>>>(A, seg, op, s);
 }
 
+template <typename T, int W>
+struct StencilVec;
+template <>
+struct StencilVec<double, 1> {
+    using type = double;
+    static __device__ __forceinline__ void load(const double *p, uint64_t pol, double *o) { o[0] = ld_stream(p, pol); }
+};
+template <>
+struct StencilVec<float, 4> {
+    using type = float4;
+    static __device__ __forceinline__ void load(const float4 *p, uint64_t pol, float *o)
+    {
+        float4 v;
+        asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+            : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w)
+            : "l"(p), "l"(pol));
+        o[0] = v.x;
+        o[1] = v.y;
+        o[2] = v.z;
+        o[3] = v.w;
+    }
+};
+
+// Stencil SpMV (structured operators): the row patterns' offsets lie in NB
+// bands of three consecutive columns.  One warp per 32-row chunk, one row per
+// lane; for each band a lane gathers only the band centre x[i + c_b] (32
+// consecutive entries), its left / right neighbours come from lanes -1 / +1
+// by shuffle and lanes 0 / 31 load the one column beyond the chunk.  The
+// values arrive k-major (three 128- or 256-byte lines per band) with no
+// index of any kind; products are added in column order.  Columns outside
+// [0, n) belong to zero entries and are clamped into range.
+template <typename T, int EPI, int NB>
+__global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp op, Scratch sc)
+{
+    if (gate_closed(op.gate)) return;
+    // positions per lane and load: FP32 values come in groups of four (one
+    // 16-byte load per lane), FP64 one by one
+    constexpr int W = stencil_group<T>();
+    constexpr int L = 3 * NB, G = (L + W - 1) / W;
+    using V = typename StencilVec<T, W>::type;
+    const V *__restrict__ sv = static_cast<const V *>(A.st_val);
+    const T *__restrict__ x = static_cast<const T *>(op.x);
+    const uint64_t pol = l2_policy(0);
+    const int lane = threadIdx.x & 31;
+    const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
+    const int nw = gridDim.x * (kBlock / 32);
+    const int n = A.n_rows, last = n - 1, nch = (n + 31) >> 5;
+    const bool edge = lane == 0 || lane == 31;
+    int cen[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) cen[b] = A.st_center[b];
+    double acc = 0.0;
+    for (int c = gw; c < nch; c += nw) {
+        const int r0 = c << 5, r = r0 + lane;
+        const int he = lane == 0 ? r0 - 1 : r0 + 32;
+        const V *v = sv + (size_t)c * (32 * G) + lane;
+        T s = T(0);
+        if constexpr (W > 1) {
+            // FP32: the whole row's values first (G vector loads), then the bands
+            T a[G * W];
+#pragma unroll
+            for (int g = 0; g < G; ++g) StencilVec<T, W>::load(v + 32 * g, pol, a + W * g);
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const int d = cen[b];
+                const T w = ld_keep(x + min(max(r + d, 0), last), pol);
+                const T h = edge ? ld_keep(x + min(max(he + d, 0), last), pol) : T(0);
+                T left = __shfl_up_sync(0xffffffffu, w, 1);
+                T right = __shfl_down_sync(0xffffffffu, w, 1);
+                if (lane == 0) left = h;
+                if (lane == 31) right = h;
+                s += a[3 * b] * left;
+                s += a[3 * b + 1] * w;
+                s += a[3 * b + 2] * right;
+            }
+        } else {
+            // FP64: groups of three bands, their value loads and gathers issued together
+#pragma unroll
+            for (int b0 = 0; b0 < NB; b0 += 3) {
+                T a[9], w[3], h[3];
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb) {
+                    const int d = cen[b0 + bb];
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) StencilVec<T, W>::load(v + 32 * (3 * (b0 + bb) + m), pol, a + 3 * bb + m);
+                    w[bb] = ld_keep(x + min(max(r + d, 0), last), pol);
+                    h[bb] = edge ? ld_keep(x + min(max(he + d, 0), last), pol) : T(0);
+                }
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb) {
+                    T left = __shfl_up_sync(0xffffffffu, w[bb], 1);
+                    T right = __shfl_down_sync(0xffffffffu, w[bb], 1);
+                    if (lane == 0) left = h[bb];
+                    if (lane == 31) right = h[bb];
+                    s += a[3 * bb] * left;
+                    s += a[3 * bb + 1] * w[bb];
+                    s += a[3 * bb + 2] * right;
+                }
+            }
+        }
+        if (r < n) epilogue<T, EPI>(r, s, op, acc);
+    }
+    if constexpr (reduces<EPI>()) {
+        double vv[1] = {acc}, out[1];
+        if (grid_reduce<1>(vv, sc.partials, sc.ticket, out)) finalize(op, out[0]);
+    }
+}
+
 template <typename T, int EPI>
 void launch_epi(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st)
 {
+    if constexpr (EPI == EPI_SET || EPI == EPI_ADD || EPI == EPI_DOT_X || EPI == EPI_RESID) {
+        if (A.st_use && A.st_val && seg.r0 == 0 && seg.r1 == A.n_rows && (A.st_nb == 3 || A.st_nb == 9)) {
+            const int chunks = (A.n_rows + 31) >> 5;
+            int grid = (chunks + kBlock / 32 - 1) / (kBlock / 32);
+            const int cap = s.num_sms * 8;
+            if (grid > cap) grid = cap;
+            if (grid < 1) grid = 1;
+            if (A.st_nb == 3) spmv_stencil_kernel<T, EPI, 3><<<grid, kBlock, 0, st>>>(A, op, s);
+            else spmv_stencil_kernel<T, EPI, 9><<<grid, kBlock, 0, st>>>(A, op, s);
+            return;
+        }
+    }
     const int ntiles = seg.t1 - seg.t0, nlong = seg.l1 - seg.l0;
     const int stage_elems = (kBlock / 32) * 32 * A.sell_lmax;
     const size_t sell_sm = (((A.npat + 1 + A.ndelta) * 4 + 127) & ~127) +
@@ -625,6 +745,43 @@ cudaError_t launch_csr_to_sell(int dtype, int n, const int *row, const void *val
         csr_to_sell_kernel<double><<<g, kBlock, 0, st>>>(n, row, (const double *)val, sell_off, (double *)sv);
     else
         csr_to_sell_kernel<float><<<g, kBlock, 0, st>>>(n, row, (const float *)val, sell_off, (float *)sv);
+    return cudaGetLastError();
+}
+
+namespace {
+struct StencilUnion {
+    int u[3 * kMaxBands];
+};
+
+template <typename T>
+__global__ void csr_to_stencil_kernel(int n, const int *__restrict__ row, const int *__restrict__ col,
+                                      const T *__restrict__ val, StencilUnion un, int L, T *__restrict__ out)
+{
+    constexpr int W = stencil_group<T>();
+    const int G = (L + W - 1) / W;
+    for (int r = blockIdx.x * kBlock + threadIdx.x; r < n; r += gridDim.x * kBlock) {
+        const size_t base = (size_t)(r >> 5) * 32 * G * W + (size_t)(r & 31) * W;
+        for (int j = row[r]; j < row[r + 1]; ++j) {
+            const int dl = col[j] - r;
+            for (int k = 0; k < L; ++k)
+                if (un.u[k] == dl) out[base + (size_t)(k / W) * 32 * W + k % W] = val[j];
+        }
+    }
+}
+}  // namespace
+
+cudaError_t launch_csr_to_stencil(int dtype, int n, const int *row, const int *col, const void *val, const int *uni,
+                                  int nb, void *out, cudaStream_t st)
+{
+    StencilUnion un;
+    const int L = 3 * nb;
+    for (int k = 0; k < 3 * kMaxBands; ++k) un.u[k] = k < L ? uni[k] : 0;
+    const int g = (n + kBlock - 1) / kBlock < 148 * 8 ? (n + kBlock - 1) / kBlock : 148 * 8;
+    if (g < 1) return cudaSuccess;
+    if (dtype == 0)
+        csr_to_stencil_kernel<double><<<g, kBlock, 0, st>>>(n, row, col, (const double *)val, un, L, (double *)out);
+    else
+        csr_to_stencil_kernel<float><<<g, kBlock, 0, st>>>(n, row, col, (const float *)val, un, L, (float *)out);
     return cudaGetLastError();
 }
 

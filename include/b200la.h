@@ -126,7 +126,9 @@ int b200la_csr_info(const b200la_csr *A, int *n_rows, int *n_cols, int *nnz, int
                     int *n_tiles, int *n_long_rows);
 /* Storage form the SpMV uses: *npat = number of distinct row patterns in the
  * matrix's row-pattern dictionary (0: none), *uses_dict = 1 when SpMV reads
- * the dictionary instead of the explicit column indices. */
+ * the dictionary instead of the explicit column indices, 2 when it reads the
+ * stencil layout (row patterns within 3 or 9 bands of three consecutive
+ * column offsets: values only, no indices). */
 int b200la_csr_format(const b200la_csr *A, int *npat, int *uses_dict);
 /* lMatrix::CopyTo a host CSR (host arrays, val of the matrix dtype). */
 int b200la_csr_download(b200la_ctx *ctx, const b200la_csr *A, int *row, int *col, void *val);
@@ -268,6 +270,14 @@ int b200la_gmres(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P, 
  * outer->reltol is relative to ||b - A x0||. */
 int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_csr *A32, const double *b, double *x,
                 const b200la_control *outer, const b200la_control *inner, int max_outer, b200la_result *res);
+/* MPIR<LAD_high, LAD_low>::Solve with a GMRES(m) error correction in FP32
+ * (mpir.cc:69-326 with a GMRES<LAD_low> inner solver): A64 and A32 the same
+ * operator (in the numbering of P32, e.g. the level-scheduled permutation of
+ * an FP32 ILU(0)), P32 an FP32 preconditioner or NULL.  Nonsymmetric systems
+ * in the mixed form: FP32 factors and Arnoldi, FP64 outer residual. */
+int b200la_mpir_gmres(b200la_ctx *ctx, const b200la_csr *A64, const b200la_csr *A32, const b200la_precond *P32,
+                      int m, const double *b, double *x, const b200la_control *outer, const b200la_control *inner,
+                      int max_outer, b200la_result *res);
 
 /* ---------------------------------------------------------------- serving */
 

@@ -128,15 +128,20 @@ def test_spmv_lane_layouts(pf, b200, oracle, lanes, monkeypatch):
     assert spmv_ok(yv.numpy(), oracle.spmv(row, col, val, x), row_scale(row, col, val, x), 1e-13)
 
 
-@pytest.mark.parametrize("mode,stage,tma", [("0", "0", "0"), ("2", "0", "0"), ("2", "1", "0"), ("2", "0", "1")])
-@pytest.mark.parametrize("dim,N,kind", [(3, 10, 0), (2, 33, 1), (3, 21, 0)])
-def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, tma, dim, N, kind, monkeypatch):
+@pytest.mark.parametrize("mode,stage,tma,stencil", [("0", "0", "0", "0"), ("2", "0", "0", "0"), ("2", "1", "0", "0"),
+                                                   ("2", "0", "1", "0"), ("0", "0", "0", "2"), ("2", "0", "0", "2")])
+@pytest.mark.parametrize("dim,N,kind", [(3, 10, 0), (2, 33, 1), (3, 21, 0), (2, 1, 0), (3, 40, 1)])
+def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, tma, stencil, dim, N, kind, monkeypatch):
     """SpMV through the row-pattern dictionary (mode 2, both precisions; sliced
     layout read directly or by bulk-copy tiles, or CSR value order with x
-    staged in shared memory) equals SpMV through explicit column indices."""
+    staged in shared memory) and through the index-free stencil layout
+    (stencil 2) equals SpMV through explicit column indices."""
     monkeypatch.setenv("B200LA_PATTERN", mode)
     monkeypatch.setenv("B200LA_STAGE_X", stage)
     monkeypatch.setenv("B200LA_SELL_TMA", tma)
+    monkeypatch.setenv("B200LA_STENCIL", stencil)
+    stencil_ok = N > 1     # N = 1: every row is a corner, the padding exceeds the limit
+    want = "stencil" if (stencil == "2" and stencil_ok) else "dictionary" if mode == "2" else "csr"
     row, col, val = oracle.q1_assemble(dim, N, kind, None, nu=1e-3, beta=(1.0, 0.5))
     n = len(row) - 1
     x = np.random.default_rng(4).uniform(-1, 1, n)
@@ -144,13 +149,13 @@ def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, tma, dim, N, kin
     y_ref = oracle.spmv(row, col, val, x)
     A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
     info = A.info()
-    assert info["row_patterns"] == (27 if dim == 3 else 9)   # interior, faces, edges, corners
-    assert info["uses_pattern_dictionary"] == (mode == "2")
+    assert info["row_patterns"] == ((27 if dim == 3 else 9) if N > 1 else 2 ** dim)   # interior, faces, edges, corners
+    assert info["storage"] == want
     yv = pf.vector(n)
     A.VectorMult(pf.vector(x), yv)
     assert spmv_ok(yv.numpy(), y_ref, sc, 1e-13)
     A32 = A.CastFrom(b200.F32)
-    assert A32.info()["uses_pattern_dictionary"] == (mode == "2")
+    assert A32.info()["storage"] == want
     x32 = x.astype(np.float32)
     y32 = pf.vector(n, b200.F32)
     A32.VectorMult(pf.vector(x32, b200.F32), y32)

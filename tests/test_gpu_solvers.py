@@ -246,3 +246,36 @@ def test_full_size_cg_property(pf, b200, oracle):
     assert cg.Solve(pf.vector(b), x) == b200.SUCCESS_REL
     r = b - oracle.spmv(row, col, val, x.numpy())
     assert np.linalg.norm(r) <= 2e-10 * np.linalg.norm(b)
+
+
+def test_mpir_gmres_ilu_mixed_convdiff(pf, b200):
+    """Mixed form of the nonsymmetric configuration: FP32 ILU(0) factors and
+    Arnoldi inside FP64 defect correction reach the FP64 stop on the true
+    residual and agree with the FP64 GMRES solution."""
+    row, col, val = b200.q1_assemble(2, 64, 1, None, 1e-3, (1.0, 0.5))
+    bh = b200.q1_rhs(7, 2, 64)
+    P64 = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS)
+    P32 = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS, dtype=b200.F32)
+    assert np.array_equal(P64.perm, P32.perm)
+    bp = bh[P64.perm]
+    gm = b200.GMRES(pf, 30)
+    gm.SetupOperator(P64.A_perm)
+    gm.SetupPreconditioner(P64)
+    gm.InitControl(5000, 0.0, 1e-9, 1e6)
+    x64 = pf.vector(len(bp))
+    assert gm.Solve(pf.vector(bp), x64) == b200.SUCCESS_REL
+    m = b200.MPIR(pf, max_outer=30)
+    m.SetupOperator(P64.A_perm)
+    m.SetupLowPrecisionOperator(P32.A_perm)
+    m.SetupInnerGMRES(30, P32)
+    m.InitControl(30, 0.0, 1e-9, 1e6)
+    m.InitInnerControl(5000, 0.0, 1e-4, 1e6)
+    x = pf.vector(len(bp))
+    bv = pf.vector(bp)
+    assert m.Solve(bv, x) == b200.SUCCESS_REL
+    assert m.result.outer >= 2 and m.result.res <= 1e-9 * m.result.res0
+    r = pf.vector(len(bp))
+    true = np.sqrt(P64.A_perm.Residual(bv, x, r))
+    assert true <= 1.0001e-9 * np.linalg.norm(bp)
+    xs, xr = x.numpy(), x64.numpy()
+    assert np.linalg.norm(xs - xr) <= 1e-6 * np.linalg.norm(xr)
