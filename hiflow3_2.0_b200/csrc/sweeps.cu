@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <cstring>
 #include <string>
 #include <vector>
 
@@ -142,11 +143,149 @@ __global__ void __launch_bounds__(kBlock) syncfree_sweep_kernel(SyncFreeArgs a)
     }
 }
 
+// Level sweep in one CTA, for operators with many small levels (the
+// level-scheduled ILU(0) of a 2-D grid: ~1,500 levels of ~200 rows).  The
+// levels are taken in dependency order, each level's rows by the CTA's 512
+// threads, a CTA barrier between levels: no flags, no waits.  The most
+// recently solved kLevelRing rows stay in a shared-memory ring, so the
+// dependency gathers of a row (on the last few levels) come from shared
+// memory; older columns are read from L2.  Forward: rows ascend, a column cc
+// of the current level [r0, r1) is in the ring when cc >= r1 - ring (slots of
+// rows >= r0 - ring are being rewritten by this level).  Backward: rows
+// descend, cc is in the ring when cc < r0 + ring.
+constexpr int kLevelRing = 8192;
+constexpr int kLevelThreads = 512;
+constexpr int kLevelMaxLevels = 24576;   // level offsets kept in shared memory
+
+struct LevelSweepArgs {
+    const int *row, *col;
+    const void *val;
+    const int *off;       // level offsets [nlev + 1] (rows of level l: [off[l], off[l+1]))
+    int nlev;
+    const void *r;
+    void *z;
+    const void *d1, *d2;
+    int backward, sgs;
+    const int *gate;
+};
+
+// Row data of one thread in one level, loaded ahead of the level (up to
+// kLevelPre entries in registers; longer rows read the rest directly).
+constexpr int kLevelPre = 8;
+template <typename T>
+struct LevelRow {
+    int rr, j0, j1;
+    int c[kLevelPre];
+    T v[kLevelPre];
+    T own, e1, e2;   // r_i (forward) or z_i (backward), d1_i, d2_i
+};
+
+template <typename T>
+__global__ void __launch_bounds__(kLevelThreads) level_sweep_cta_kernel(LevelSweepArgs a)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    T *ring = reinterpret_cast<T *>(s_raw);
+    int *s_off = reinterpret_cast<int *>(s_raw + kLevelRing * sizeof(T));
+    if (gate_closed(a.gate)) return;
+    for (int i = threadIdx.x; i <= a.nlev; i += kLevelThreads) {
+        s_off[i] = __ldg(a.off + i);
+    }
+    __syncthreads();
+    const T *__restrict__ val = static_cast<const T *>(a.val);
+    const T *__restrict__ r = static_cast<const T *>(a.r);
+    const T *__restrict__ d1 = static_cast<const T *>(a.d1);
+    const T *__restrict__ d2 = static_cast<const T *>(a.d2);
+    T *z = static_cast<T *>(a.z);
+    const int tid = threadIdx.x, nlev = a.nlev;
+    auto level_of = [&](int k) { return a.backward ? nlev - 1 - k : k; };
+    // row of this thread in level k (or -1), its row-pointer pair, its entries
+    auto first_row = [&](int k) {
+        if (k >= nlev) return -1;
+        const int l = level_of(k), rr = s_off[l] + tid;
+        return rr < s_off[l + 1] ? rr : -1;
+    };
+    auto load_entries = [&](LevelRow<T> &q) {
+#pragma unroll
+        for (int e = 0; e < kLevelPre; ++e) {
+            if (q.rr >= 0 && q.j0 + e < q.j1) {
+                q.c[e] = __ldg(a.col + q.j0 + e);
+                q.v[e] = __ldg(val + q.j0 + e);
+            }
+        }
+        if (q.rr >= 0) {
+            // the row's own inputs: r_i, or the forward result z_i (written by
+            // the previous launch), and the diagonal scalings
+            q.own = a.backward ? __ldcg(z + q.rr) : r[q.rr];
+            q.e1 = d1 ? d1[q.rr] : T(0);
+            q.e2 = (a.sgs && a.backward) ? d2[q.rr] : T(0);
+        }
+    };
+    auto row_value = [&](int rr, int j0, int j1, const int *cp, const T *vp, int r0, int r1, T own, T e1, T e2) {
+        T s = T(0);
+#pragma unroll
+        for (int e = 0; e < kLevelPre; ++e) {
+            if (j0 + e < j1) {
+                const int cc = cp[e];
+                const bool in_ring = a.backward ? cc < r0 + kLevelRing : cc >= r1 - kLevelRing;
+                s += vp[e] * (in_ring ? ring[cc & (kLevelRing - 1)] : __ldcg(z + cc));
+            }
+        }
+        for (int j = j0 + kLevelPre; j < j1; ++j) {
+            const int cc = __ldg(a.col + j);
+            const bool in_ring = a.backward ? cc < r0 + kLevelRing : cc >= r1 - kLevelRing;
+            s += __ldg(val + j) * (in_ring ? ring[cc & (kLevelRing - 1)] : __ldcg(z + cc));
+        }
+        T out;
+        if (!a.backward) out = a.sgs ? (-own + s) * e1 : -(-own + s);
+        else out = a.sgs ? (own * e2 + s) * e1 : (-own + s) * e1;
+        ring[rr & (kLevelRing - 1)] = out;
+        __stcg(z + rr, out);
+    };
+    // software pipeline: entries of level k + 1 and row pointers of level
+    // k + 2 are in flight while level k is solved
+    LevelRow<T> cur, nxt;
+    cur.rr = first_row(0);
+    cur.j0 = cur.rr >= 0 ? __ldg(a.row + cur.rr) : 0;
+    cur.j1 = cur.rr >= 0 ? __ldg(a.row + cur.rr + 1) : 0;
+    load_entries(cur);
+    nxt.rr = first_row(1);
+    nxt.j0 = nxt.rr >= 0 ? __ldg(a.row + nxt.rr) : 0;
+    nxt.j1 = nxt.rr >= 0 ? __ldg(a.row + nxt.rr + 1) : 0;
+    for (int k = 0; k < nlev; ++k) {
+        const int l = level_of(k), r0 = s_off[l], r1 = s_off[l + 1];
+        const int r2 = first_row(k + 2);
+        const int p0 = r2 >= 0 ? __ldg(a.row + r2) : 0, p1 = r2 >= 0 ? __ldg(a.row + r2 + 1) : 0;
+        load_entries(nxt);
+        if (cur.rr >= 0) row_value(cur.rr, cur.j0, cur.j1, cur.c, cur.v, r0, r1, cur.own, cur.e1, cur.e2);
+        // rows of a level beyond the first kLevelThreads (no look-ahead)
+        for (int rr = r0 + tid + kLevelThreads; rr < r1; rr += kLevelThreads) {
+            LevelRow<T> q;
+            q.rr = rr;
+            q.j0 = __ldg(a.row + rr);
+            q.j1 = __ldg(a.row + rr + 1);
+            load_entries(q);
+            row_value(rr, q.j0, q.j1, q.c, q.v, r0, r1, q.own, q.e1, q.e2);
+        }
+        __syncthreads();
+        cur = nxt;
+        nxt.rr = r2;
+        nxt.j0 = p0;
+        nxt.j1 = p1;
+    }
+}
+
 }  // namespace
 
 namespace b200 {
 
-cudaError_t sweeps_configure() { return cudaSuccess; }
+cudaError_t sweeps_configure()
+{
+    cudaError_t e = cudaFuncSetAttribute(level_sweep_cta_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(kLevelRing * sizeof(double) + sizeof(int) * (kLevelMaxLevels + 1)));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(level_sweep_cta_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(kLevelRing * sizeof(float) + sizeof(int) * (kLevelMaxLevels + 1)));
+}
 
 cudaError_t launch_invdiag(int dtype, int n, const int *row, const int *col, const void *val, void *out,
                            cudaStream_t st)
@@ -178,6 +317,8 @@ struct SyncFreePlan {
     int2 *fwd = nullptr, *bwd = nullptr;
     int nf = 0, nb = 0;
     int lg_l = 0, lg_u = 0;
+    int *lev_off = nullptr;   // single-CTA level sweep: level offsets (null: chunk tickets)
+    int nlev = 0;
 };
 
 static int lanes_for(const b200la_csr *M)
@@ -194,6 +335,24 @@ int syncfree_setup(b200la_ctx *ctx, b200la_precond *P)
     bool use = P->nblocks > 64;
     if (env) use = std::atoi(env) != 0;
     if (!use) return B200LA_OK;
+    // many small levels: one CTA walks them (B200LA_SWEEP=cta / tickets to force)
+    bool cta = P->nblocks > 64 && P->nblocks <= kLevelMaxLevels && P->n / std::max(P->nblocks, 1) <= 4 * kLevelThreads;
+    if (const char *sw = std::getenv("B200LA_SWEEP")) cta = std::strcmp(sw, "cta") == 0 && P->nblocks <= kLevelMaxLevels;
+    if (cta) {
+        SyncFreePlan *plan = new SyncFreePlan();
+        plan->nlev = P->nblocks;
+        cudaError_t e;
+        if ((e = cudaMalloc(&plan->lev_off, sizeof(int) * (P->nblocks + 1))) ||
+            (e = cudaMemcpy(plan->lev_off, P->block_off.data(), sizeof(int) * (P->nblocks + 1),
+                            cudaMemcpyHostToDevice))) {
+            if (plan->lev_off) cudaFree(plan->lev_off);
+            delete plan;
+            return ctx_fail(ctx, B200LA_ERR_ALLOC, "level sweep setup", e);
+        }
+        P->syncfree_plan = plan;
+        P->use_syncfree = 1;
+        return B200LA_OK;
+    }
     const int lgL = lanes_for(P->L), lgU = lanes_for(P->U);
     // chunks of at most 32 >> lg rows, never crossing a block (level) boundary
     auto chunks = [&](int lg, bool reverse) {
@@ -232,8 +391,9 @@ void syncfree_free(b200la_precond *P)
 {
     SyncFreePlan *plan = static_cast<SyncFreePlan *>(P->syncfree_plan);
     if (!plan) return;
-    cudaFree(plan->fwd);
-    cudaFree(plan->bwd);
+    if (plan->fwd) cudaFree(plan->fwd);
+    if (plan->bwd) cudaFree(plan->bwd);
+    if (plan->lev_off) cudaFree(plan->lev_off);
     delete plan;
     P->syncfree_plan = nullptr;
 }
@@ -241,6 +401,34 @@ void syncfree_free(b200la_precond *P)
 int syncfree_apply(b200la_ctx *ctx, const b200la_precond *P, const void *r, void *z, const int *gate)
 {
     const SyncFreePlan *plan = static_cast<const SyncFreePlan *>(P->syncfree_plan);
+    if (plan->lev_off) {
+        LevelSweepArgs a;
+        a.off = plan->lev_off;
+        a.nlev = plan->nlev;
+        a.r = r;
+        a.z = z;
+        a.d1 = P->iDv;
+        a.d2 = P->Dv;
+        a.sgs = P->kind == B200LA_PRECOND_MCSGS;
+        a.gate = gate;
+        for (int dir = 0; dir < 2; ++dir) {
+            const b200la_csr *M = dir ? P->U : P->L;
+            a.row = M->row;
+            a.col = M->col;
+            a.val = M->val;
+            a.backward = dir;
+            if (P->dtype == B200LA_F64)
+                level_sweep_cta_kernel<double>
+                    <<<1, kLevelThreads, kLevelRing * sizeof(double) + sizeof(int) * (plan->nlev + 1), ctx->stream>>>(a);
+            else
+                level_sweep_cta_kernel<float>
+                    <<<1, kLevelThreads, kLevelRing * sizeof(float) + sizeof(int) * (plan->nlev + 1), ctx->stream>>>(a);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_CUDA, "level sweep", e);
+            ctx->launches += 1;
+        }
+        return B200LA_OK;
+    }
     SyncFreeArgs a;
     a.r = r;
     a.z = z;

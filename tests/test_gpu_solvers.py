@@ -107,10 +107,11 @@ def test_mcsgs_pcg_vs_reference(pf, b200, golden, dim, N):
     assert np.linalg.norm(x.numpy() - xr) <= 1e-7 * np.linalg.norm(xr)
 
 
-@pytest.mark.parametrize("syncfree", ["0", "1"])
+@pytest.mark.parametrize("syncfree,sweep", [("0", "tickets"), ("1", "tickets"), ("1", "cta")])
 @pytest.mark.parametrize("dim,N,tag", [(2, 17, "cd"), (3, 7, "p"), (2, 8, "pk")])
-def test_ilu0_ls_apply(pf, b200, golden, dim, N, tag, syncfree, monkeypatch):
+def test_ilu0_ls_apply(pf, b200, golden, dim, N, tag, syncfree, sweep, monkeypatch):
     monkeypatch.setenv("B200LA_SYNCFREE", syncfree)
+    monkeypatch.setenv("B200LA_SWEEP", sweep)
     key = f"{dim}d{N}_{tag}"
     row, col, val = golden[key + "_row"], golden[key + "_col"], golden[key + "_val"]
     P = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS)
@@ -118,7 +119,7 @@ def test_ilu0_ls_apply(pf, b200, golden, dim, N, tag, syncfree, monkeypatch):
     assert np.array_equal(P.block_sizes, golden[key + "_iluls_sizes"])
     r = golden[key + "_x"]
     z = pf.vector(len(r))
-    for _ in range(3):   # repeated applies (epochs of the sync-free sweep)
+    for _ in range(3):   # repeated applies (epochs of the sync-free sweep; the ring of the level sweep)
         P.ApplyPreconditioner(pf.vector(r), z)
         zr = golden[key + "_iluls_z"]
         assert np.max(np.abs(z.numpy() - zr)) <= 1e-12 * np.max(np.abs(zr))
@@ -136,9 +137,10 @@ def test_ilu0_mc_apply(pf, b200, golden):
     assert np.max(np.abs(z.numpy() - zr)) <= 1e-12 * np.max(np.abs(zr))
 
 
-@pytest.mark.parametrize("syncfree", ["0", "1"])
-def test_gmres_ilu_ls_vs_reference(pf, b200, golden, syncfree, monkeypatch):
+@pytest.mark.parametrize("syncfree,sweep", [("0", "tickets"), ("1", "tickets"), ("1", "cta")])
+def test_gmres_ilu_ls_vs_reference(pf, b200, golden, syncfree, sweep, monkeypatch):
     monkeypatch.setenv("B200LA_SYNCFREE", syncfree)
+    monkeypatch.setenv("B200LA_SWEEP", sweep)
     row, col, val = b200.q1_assemble(2, 32, 1, None, 1e-3, (1.0, 0.5))
     P = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS)
     b = golden["gmres2d32_b"][P.perm]
@@ -279,3 +281,24 @@ def test_mpir_gmres_ilu_mixed_convdiff(pf, b200):
     assert true <= 1.0001e-9 * np.linalg.norm(bp)
     xs, xr = x.numpy(), x64.numpy()
     assert np.linalg.norm(xs - xr) <= 1e-6 * np.linalg.norm(xr)
+
+
+@pytest.mark.parametrize("dim,N,kind", [(2, 160, 1), (3, 26, 0)])
+def test_ilu0_level_sweep_beyond_ring(pf, b200, dim, N, kind, monkeypatch):
+    """The single-CTA level sweep on operators larger than its shared-memory
+    ring (columns read from the ring and from L2) equals the ticketed
+    sync-free sweep (and the preconditioned residual test of GMRES)."""
+    row, col, val = b200.q1_assemble(dim, N, kind, None, 1e-2, (1.0, 0.5, 0.25))
+    n = len(row) - 1
+    assert n > 8192
+    r = np.random.default_rng(3).uniform(-1, 1, n)
+    out = {}
+    for sweep in ("tickets", "cta"):
+        monkeypatch.setenv("B200LA_SYNCFREE", "1")
+        monkeypatch.setenv("B200LA_SWEEP", sweep)
+        P = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS)
+        z = pf.vector(n)
+        for _ in range(2):
+            P.ApplyPreconditioner(pf.vector(r[P.perm]), z)
+        out[sweep] = z.numpy()
+    assert np.max(np.abs(out["cta"] - out["tickets"])) <= 1e-11 * np.max(np.abs(out["tickets"]))
