@@ -33,12 +33,12 @@
 #include "serve.cuh"
 
 using b200::srv::SysDesc;
+using b200::srv::SysRun;
 using b200::srv::SysState;
-using b200::srv::Tile;
 
 namespace {
 
-constexpr int kTileCap = 1 << 18;   // tiles one round may list
+constexpr int kTabCap = 1 << 16;    // systems one round may list
 
 size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -50,6 +50,7 @@ struct Req {
     // layout decided at submission
     int n = 0, fmt = 0, nchunks = 0;
     long long nnz = 0, slen = 0;      // stored entries (SELL: padded)
+    long long slen32 = 0;             // stored FP32 entries (mixed; stencil: groups of four)
     std::vector<int> sell_off;        // SELL chunk offsets
     size_t bytes = 0, temp_bytes = 0; // resident / admission scratch
     double iter_bytes = 0;            // streamed by one batch iteration
@@ -60,7 +61,6 @@ struct Slot {
     Req *req = nullptr;
     void *block = nullptr;
     SysDesc desc{};
-    int ntiles = 0;
 };
 
 // Row lengths of the structured Q1 operator: w(ix) w(iy) w(iz), w = 2 on the boundary.
@@ -90,7 +90,7 @@ struct b200la_server {
     int *d_tiles = nullptr, *h_tiles = nullptr;
     cudaGraphExec_t graph = nullptr;
     // kernel shape
-    int nw = 8, ctas_per_sm = 2, cpw = 4, iters = 16;
+    int nw = 8, ctas_per_sm = 4, cpw = 4, iters = 16;
     double active_cap = 512.0 * 1024 * 1024;
     int max_active = 1024;
 
@@ -142,8 +142,10 @@ int plan_request(b200la_server *S, Req *q)
     q->nchunks = (n + b200::srv::kChunk - 1) / b200::srv::kChunk;
     if (!r.row) {
         // structured Q1 operator: stencil layout, no indices
+        const int L = r.q1_dim == 3 ? 27 : 9;
         q->fmt = b200::srv::FMT_STENCIL;
-        q->slen = (long long)q->nchunks * b200::srv::kChunk * (r.q1_dim == 3 ? 27 : 9);
+        q->slen = (long long)q->nchunks * b200::srv::kChunk * L;
+        q->slen32 = (long long)q->nchunks * b200::srv::kChunk * 4 * ((L + 3) / 4);
     }
     int maxlen = 0;
     for (int v : len) maxlen = std::max(maxlen, v);
@@ -162,10 +164,10 @@ int plan_request(b200la_server *S, Req *q)
     } else if (maxlen <= b200::srv::kMaxRowSell && slen <= 2 * std::max<long long>(q->nnz, 1) &&
                slen < (1LL << 31)) {
         q->fmt = b200::srv::FMT_SELL;
-        q->slen = slen;
+        q->slen = q->slen32 = slen;
     } else {
         q->fmt = b200::srv::FMT_CSRW;
-        q->slen = q->nnz;
+        q->slen = q->slen32 = q->nnz;
         q->sell_off.clear();
     }
     const size_t v8 = al256(8 * (size_t)n), v4 = al256(4 * (size_t)n);
@@ -175,14 +177,15 @@ int plan_request(b200la_server *S, Req *q)
                                                         : al256(4 * (size_t)(n + 1));
     const size_t colb = stencil ? 0 : al256(4 * (size_t)q->slen);
     const size_t pst = (size_t)((q->nchunks + 1) & ~1);
-    size_t b = offb + colb + al256(8 * (size_t)q->slen) + al256(24 * pst);
-    if (mixed) b += al256(4 * (size_t)q->slen) + 2 * v8 + 7 * v4;
+    const size_t ng = (size_t)((q->nchunks + b200::srv::kGroup - 1) / b200::srv::kGroup), gst = (ng + 1) & ~size_t(1);
+    size_t b = offb + colb + al256(8 * (size_t)q->slen) + al256(24 * pst) + al256(24 * gst) + al256(4 * ng);
+    if (mixed) b += al256(4 * (size_t)q->slen32) + 2 * v8 + 7 * v4;
     else b += 8 * v8;
     q->bytes = b;
     q->temp_bytes = al256(4 * (size_t)(n + 1)) + al256(4 * (size_t)q->nnz) + al256(8 * (size_t)q->nnz) +
                     ((!r.row && r.q1_kcell) ? al256(8 * q1_cells(r.q1_dim, r.q1_N)) : 0);
     const double ib = stencil ? 0.0 : 4.0;   // index bytes per stored entry
-    q->iter_bytes = mixed ? (4.0 + ib) * q->slen + 48.0 * n : (8.0 + ib) * q->slen + 96.0 * n;   // vectors: 32n (SpMV) + 64n (update)
+    q->iter_bytes = mixed ? 4.0 * q->slen32 + ib * q->slen + 48.0 * n : (8.0 + ib) * q->slen + 96.0 * n;   // vectors: 32n (SpMV) + 64n (update)
     return B200LA_OK;
 }
 
@@ -227,6 +230,8 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
     d.mixed = mixed;
     d.fmt = q->fmt;
     d.pstride = (q->nchunks + 1) & ~1;
+    d.ngroups = (q->nchunks + b200::srv::kGroup - 1) / b200::srv::kGroup;
+    d.gstride = (d.ngroups + 1) & ~1;
     const bool sell = q->fmt == b200::srv::FMT_SELL;
     const bool stencil = q->fmt == b200::srv::FMT_STENCIL;
     if (stencil) {
@@ -238,8 +243,10 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
         d.col = reinterpret_cast<int *>(take(4 * (size_t)q->slen));
     }
     d.val64 = reinterpret_cast<double *>(take(8 * (size_t)q->slen));
-    d.val32 = mixed ? reinterpret_cast<float *>(take(4 * (size_t)q->slen)) : nullptr;
+    d.val32 = mixed ? reinterpret_cast<float *>(take(4 * (size_t)q->slen32)) : nullptr;
     d.part = reinterpret_cast<double *>(take(24 * (size_t)d.pstride));
+    d.gpart = reinterpret_cast<double *>(take(24 * (size_t)d.gstride));
+    d.gcnt = reinterpret_cast<unsigned *>(take(4 * (size_t)d.ngroups));
     d.b = reinterpret_cast<double *>(take(8 * (size_t)n));
     char *vec0 = p;   // vectors that start at zero
     d.x = reinterpret_cast<double *>(take(8 * (size_t)n));
@@ -277,7 +284,7 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
     }
     if (stencil) {
         SV(cudaMemsetAsync(const_cast<double *>(d.val64), 0, 8 * (size_t)q->slen, st));
-        if (mixed) SV(cudaMemsetAsync(const_cast<float *>(d.val32), 0, 4 * (size_t)q->slen, st));
+        if (mixed) SV(cudaMemsetAsync(const_cast<float *>(d.val32), 0, 4 * (size_t)q->slen32, st));
     } else if (sell) {
         SV(cudaMemcpyAsync(const_cast<int *>(d.off), q->sell_off.data(), 4 * (size_t)(q->nchunks + 1),
                            cudaMemcpyHostToDevice, st));
@@ -303,13 +310,12 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
     hs.phase = mixed ? b200::srv::PH_OUTER : b200::srv::PH_CG_START;
     SV(cudaMemcpyAsync(S->d_state + sl->idx, &hs, sizeof hs, cudaMemcpyHostToDevice, st));
     SV(cudaMemsetAsync(d.ticket, 0, sizeof(unsigned) * b200::srv::kTicketWords, st));
+    SV(cudaMemsetAsync(d.gcnt, 0, sizeof(unsigned) * (size_t)d.ngroups, st));
     SV(cudaMemsetAsync(d.done, 0, sizeof(int), st));
     SV(cudaMemcpyAsync(S->d_sys + sl->idx, &d, sizeof d, cudaMemcpyHostToDevice, st));
     SV(cudaFreeAsync(tmp, st));
     SV(cudaStreamSynchronize(st));
     sl->desc = d;
-    const int cpt = S->nw * S->cpw;
-    sl->ntiles = (q->nchunks + cpt - 1) / cpt;
     return 0;
 }
 
@@ -434,22 +440,32 @@ void admit_loop(b200la_server *S)
 }
 
 struct ActiveSys {
-    int idx, nchunks, ntiles;
+    int idx, nchunks;
 };
+
+// System table of the active set: header [systems, chunks, chunks per warp range].
+int write_table(b200la_server *S, const std::vector<ActiveSys> &act)
+{
+    int *h = S->h_tiles;
+    SysRun *tab = reinterpret_cast<SysRun *>(h + b200::srv::kTabHdrWords);
+    int nt = 0, tot = 0;
+    for (const ActiveSys &a : act) {
+        tab[nt++] = SysRun{a.idx, tot, a.nchunks, 0};
+        tot += a.nchunks;
+    }
+    h[0] = nt;
+    h[1] = tot;
+    h[2] = S->cpw;
+    h[3] = 0;
+    return nt;
+}
 
 int run_round(b200la_server *S, const std::vector<ActiveSys> &act)
 {
-    // tile table of the active set
+    const int nt = write_table(S, act);
     int *h = S->h_tiles;
-    Tile *tl = reinterpret_cast<Tile *>(h + b200::srv::kTileHdrWords);
-    int nt = 0;
-    const int cpt = S->nw * S->cpw;
-    for (const ActiveSys &a : act) {
-        for (int c0 = 0; c0 < a.nchunks; c0 += cpt) tl[nt++] = Tile{a.idx, c0, std::min(a.nchunks, c0 + cpt), a.ntiles};
-    }
-    h[0] = nt;
     cudaStream_t st = S->s_comp;
-    SV(cudaMemcpyAsync(S->d_tiles, h, sizeof(int) * b200::srv::kTileHdrWords + sizeof(Tile) * (size_t)nt,
+    SV(cudaMemcpyAsync(S->d_tiles, h, sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * (size_t)nt,
                        cudaMemcpyHostToDevice, st));
     SV(cudaEventRecord(S->ev_a, st));
     SV(cudaGraphLaunch(S->graph, st));
@@ -472,26 +488,24 @@ void round_loop(b200la_server *S)
             S->cv_round.wait(lk, [S] { return S->quit || !S->ready.empty() || !S->active.empty(); });
             if (S->quit && S->active.empty() && S->ready.empty()) return;
             double wb = 0.0;
-            long long tiles = 0;
-            const int cpt = S->nw * S->cpw;
+            long long chunks = 0;
             for (Slot *sl : S->active) {
                 wb += sl->req->iter_bytes;
-                tiles += sl->ntiles;
+                chunks += sl->desc.nchunks;
             }
-            while (!S->ready.empty() && (int)S->active.size() < S->max_active) {
+            while (!S->ready.empty() && (int)S->active.size() < std::min(S->max_active, kTabCap)) {
                 Slot *sl = S->ready.front();
                 const bool room = S->active.empty() || wb + sl->req->iter_bytes <= S->active_cap;
-                if (!room || tiles + sl->ntiles > kTileCap) break;
+                if (!room || chunks + sl->desc.nchunks >= (1LL << 31)) break;
                 wb += sl->req->iter_bytes;
-                tiles += sl->ntiles;
+                chunks += sl->desc.nchunks;
                 S->ready.pop_front();
                 S->active.push_back(sl);
             }
-            (void)cpt;
             S->peak_active = std::max(S->peak_active, (int)S->active.size());
             if (S->active.empty()) continue;
             act.clear();
-            for (Slot *sl : S->active) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks, sl->ntiles});
+            for (Slot *sl : S->active) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks});
         }
         const int rc = S->fatal ? S->fatal : run_round(S, act);
         std::lock_guard<std::mutex> lk(S->mu);
@@ -678,26 +692,20 @@ int autotune(b200la_server *S)
     struct Shape {
         int nw, cps, cpw;
     };
-    const Shape shapes[] = {{8, 2, 2}, {8, 2, 4}, {8, 2, 8}, {4, 4, 2}, {4, 4, 4},
-                            {4, 4, 8}, {8, 4, 4}, {4, 8, 4}, {8, 3, 4}, {4, 6, 4}};
+    const Shape shapes[] = {{8, 4, 2}, {8, 4, 4}, {8, 4, 8}, {8, 4, 16}, {8, 2, 4},
+                            {4, 8, 2}, {4, 8, 4}, {4, 8, 8}, {8, 3, 4}, {8, 6, 4}};
     float best = 1e30f;
     Shape pick{S->nw, S->ctas_per_sm, S->cpw};
+    std::vector<ActiveSys> act;
+    for (Slot *sl : slots) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks});
     for (const Shape &sh : shapes) {
         if (rc) break;
         S->nw = sh.nw;
         S->ctas_per_sm = sh.cps;
         S->cpw = sh.cpw;
-        int *h = S->h_tiles;
-        Tile *tl = reinterpret_cast<Tile *>(h + b200::srv::kTileHdrWords);
-        int nt = 0;
-        const int cpt = sh.nw * sh.cpw;
-        for (Slot *sl : slots) {
-            const int nch = sl->desc.nchunks, ntl = (nch + cpt - 1) / cpt;
-            for (int c0 = 0; c0 < nch; c0 += cpt) tl[nt++] = Tile{sl->idx, c0, std::min(nch, c0 + cpt), ntl};
-        }
-        h[0] = nt;
+        const int nt = write_table(S, act);
         cudaStream_t st = S->s_comp;
-        if (cudaMemcpyAsync(S->d_tiles, h, sizeof(int) * b200::srv::kTileHdrWords + sizeof(Tile) * (size_t)nt,
+        if (cudaMemcpyAsync(S->d_tiles, S->h_tiles, sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * (size_t)nt,
                             cudaMemcpyHostToDevice, st) != cudaSuccess) {
             rc = -1;
             break;
@@ -797,11 +805,11 @@ extern "C" int b200la_serve_start(const b200la_serve_config *cfg, b200la_server 
          cudaMalloc(&S->d_state, sizeof(SysState) * ms) == cudaSuccess &&
          cudaMalloc(&S->d_ticket, sizeof(unsigned) * b200::srv::kTicketWords * ms) == cudaSuccess &&
          cudaMalloc(&S->d_done, sizeof(int) * ms) == cudaSuccess &&
-         cudaMalloc(&S->d_tiles, sizeof(int) * b200::srv::kTileHdrWords + sizeof(Tile) * kTileCap) == cudaSuccess &&
+         cudaMalloc(&S->d_tiles, sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * kTabCap) == cudaSuccess &&
          cudaMallocHost(&S->h_done, sizeof(int) * ms) == cudaSuccess &&
-         cudaMallocHost(&S->h_tiles, sizeof(int) * b200::srv::kTileHdrWords + sizeof(Tile) * kTileCap) == cudaSuccess;
+         cudaMallocHost(&S->h_tiles, sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * kTabCap) == cudaSuccess;
     ok = ok && cudaMemset(S->d_done, 0, sizeof(int) * ms) == cudaSuccess &&
-         cudaMemset(S->d_tiles, 0, sizeof(int) * b200::srv::kTileHdrWords) == cudaSuccess &&
+         cudaMemset(S->d_tiles, 0, sizeof(int) * b200::srv::kTabHdrWords) == cudaSuccess &&
          cudaMemset(S->d_sys, 0, sizeof(SysDesc) * ms) == cudaSuccess;
     if (!ok) {
         destroy_server(S);

@@ -5,15 +5,16 @@
 // (chunk c holds its rows' entries k-major, sell[off[c] + 32 k + lane], rows
 // zero-padded to the chunk's longest row) or, for rows too long for that, the
 // CSR with one warp per row.  Two batched kernels advance every active
-// system by one iteration of its Krylov recurrence; a tile table lists which
-// chunks of which systems a launch covers.
+// system by one iteration of its Krylov recurrence; a system table lists the
+// active systems and where their chunks start in the batch's chunk sequence.
 //
 // Determinism: a system's arithmetic never depends on the batch it is in.
 // Row sums run in a fixed order (one thread per row in column order, or a
-// fixed shuffle tree per row), reductions go through one partial per 32-row
-// chunk, and the CTA that completes a system's tiles sums those partials in a
-// fixed order over 256 virtual lanes.  Tile size, block size, grid size and
-// the other systems of the batch change only the schedule.
+// fixed shuffle tree per row).  Reductions go through one partial per 32-row
+// chunk; the warp that completes a group of 32 chunks sums them by a fixed
+// shuffle tree, and the warp that completes the last group sums the group
+// partials in a fixed order.  Warp ranges, block size, grid size and the
+// other systems of the batch change only the schedule.
 #pragma once
 
 #include <cstdint>
@@ -33,14 +34,17 @@ namespace srv {
 enum Phase : int { PH_CG_START = 0, PH_CG = 1, PH_OUTER = 2, PH_INNER = 3, PH_CORRECT = 4, PH_DONE = 5 };
 // FMT_STENCIL: a structured Q1 operator stored by stencil position: entry k
 // of row i is the coupling to column i + delta_k (the 9 / 27 offsets
-// (dk P + dj) P + di in column order, P = N + 1 nodes per line), chunk c at
-// val[32 L c + 32 k + lane], zero where the row has no such neighbour.  No
-// column indices or offsets are stored or loaded.
+// (dk P + dj) P + di in column order, P = N + 1 nodes per line), zero where
+// the row has no such neighbour; FP64 values at val64[32 L c + 32 k + lane],
+// FP32 values in groups of four positions per lane at
+// val32[128 G c + 128 (k / 4) + 4 lane + k % 4], G = ceil(L / 4).  No column
+// indices or offsets are stored or loaded.
 enum Fmt : int { FMT_SELL = 0, FMT_CSRW = 1, FMT_STENCIL = 2 };
 
 constexpr int kChunk = 32;          // rows per chunk
 constexpr int kFinLanes = 256;      // virtual lanes of the per-system final sums
-constexpr int kTicketWords = 64;    // two ticket counters per slot, 128 bytes apart
+constexpr int kTicketWords = 32;    // the system ticket of a slot, alone on its 128-byte line
+constexpr int kGroup = 32;          // chunks per reduction group
 constexpr int kMaxRowSell = 64;     // longest row kept in the SELL layout
 
 struct SysState {
@@ -59,6 +63,7 @@ struct SysDesc {
     int n, nchunks, mixed, fmt;
     int pstride;           // chunk partials per quantity (nchunks rounded up to even)
     int sdim, sP, sL;      // FMT_STENCIL: dimension, nodes per line, stencil width
+    int ngroups, gstride;  // reduction groups of kGroup chunks; group partials per quantity
     const int *off;        // SELL: chunk offsets [nchunks + 1]; CSRW: row pointer [n + 1]
     const int *col;
     const double *val64;
@@ -68,7 +73,9 @@ struct SysDesc {
     void *r, *z, *p0, *p1, *ap, *xl;  // FP64 system: double r, z = D^-1 r, p, Ap; mixed: float ... and x_low
     const void *invd;      // 1 / a_ii: double, or float for mixed
     double *part;          // [3][pstride] chunk partials
-    unsigned *ticket;      // kTicketWords words
+    double *gpart;         // [3][gstride] group partials
+    unsigned *gcnt;        // [ngroups] chunks reported per group (0 between launches)
+    unsigned *ticket;      // groups completed (0 between launches)
     int *done;             // final status word polled by the host (0 while running)
 };
 
@@ -78,16 +85,18 @@ __host__ __device__ __forceinline__ int stencil_delta(int dim, int P, int k)
     return dim == 3 ? ((k / 9 - 1) * P + (k / 3 % 3 - 1)) * P + (k % 3 - 1) : (k / 3 - 1) * P + (k % 3 - 1);
 }
 
-struct Tile {
-    int sys, c0, c1, ntiles;   // chunks [c0, c1) of slot sys, which has ntiles tiles
+// Active system: slot, first chunk in the batch's chunk sequence, chunk count.
+struct SysRun {
+    int slot, cbeg, nch, pad;
 };
 
-// Tile table in device memory: word 0 the tile count, tiles from word 4.
-constexpr int kTileHdrWords = 4;
+// System table in device memory: words [0] systems, [1] chunks in total,
+// [2] chunks per warp range; entries from word 4 (ascending cbeg).
+constexpr int kTabHdrWords = 4;
 
-// One batch iteration (SpMV kernel, update kernel) over the tile table.
+// One batch iteration (SpMV kernel, update kernel) over the system table.
 // SysDesc and SysState tables are indexed by slot.
-cudaError_t launch_round(int nw, int grid, const SysDesc *sys, SysState *state, const int *tiles, cudaStream_t st);
+cudaError_t launch_round(int nw, int grid, const SysDesc *sys, SysState *state, const int *tab, cudaStream_t st);
 // CSR (device, FP64) -> the slot's chunk layout, 1 / a_ii, and FP32 values when mixed.
 cudaError_t launch_build_slot(const SysDesc &d, const int *row, const int *col, const double *val,
                               cudaStream_t st);

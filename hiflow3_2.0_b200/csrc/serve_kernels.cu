@@ -1,32 +1,37 @@
 // serve_kernels.cu -- batched Krylov kernels of the solve server (sm_100a).
 //
-// One batch iteration is two launches over the tile table:
-//   k1  SpMV  Ap = A p_new with p_new = beta p + D^-1 r formed on the fly at
-//       every gathered column (and stored for the own rows into the other of
-//       two p buffers), with the chunk partials of p_new.Ap; the CTA
-//       completing a system's tiles sets alpha = rho / p.Ap and flips the p
-//       buffer (CG, inner CG).  Mixed systems between two inner solves apply
-//       the correction x += (double) x_low here.
-//   k2  update x += alpha p, r -= alpha Ap with the partials of r.r and
-//       r.(D^-1 r); the completing CTA runs IterateControl::Check
-//       (src/common/iterate_control.cc:84-110) and sets beta, rho.  Start
-//       phases (CG: r = b; mixed: r = b - A x in FP64, r_low = (float) r)
-//       run here too.
+// One batch iteration is two launches over the system table:
+//   k1  SpMV  Ap = A p_new with p_new = beta p + z formed on the fly at every
+//       gathered column (and stored for the own rows into the other of two p
+//       buffers), with the partials of p_new.Ap; on completion of a system
+//       alpha = rho / p.Ap and the p buffer flips (CG, inner CG).  Mixed
+//       systems between two inner solves apply x += (double) x_low here.
+//   k2  update x += alpha p, r -= alpha Ap, z = D^-1 r with the partials of
+//       r.r and r.z; on completion IterateControl::Check
+//       (src/common/iterate_control.cc:84-110) and beta, rho.  Start phases
+//       (CG: r = b; mixed: r = b - A x in FP64, r_low = (float) r) run here.
 // Folding the p-update of CG<LAD> (cg.cc:240-246) into the next product
 // removes a launch and a pass per iteration; the update is written with
 // explicit roundings so that every gathering thread forms the same p_new as
 // the thread that stores it.
-// Each CTA takes a contiguous range of tiles and keeps the current system's
-// descriptor and state in shared memory while consecutive tiles share it.
-// Systems whose phase has no work in a launch skip their tiles.  Operator
-// values and indices are streamed past L1; gathered vectors go through L1.
+//
+// Work split: the active systems' 32-row chunks form one sequence; each warp
+// takes one contiguous range of it, with no CTA barrier.  A warp loads a
+// system's descriptor and state into its own shared-memory slot when its
+// range enters the system.  Reductions: one partial per chunk; a warp reports
+// its run of each system's chunks to the run's groups of 32 chunks, the warp
+// completing a group sums its partials (fixed shuffle tree) and reports the
+// group to the system, and the warp completing the last group sums the group
+// partials in a fixed order and runs the finaliser.  Counters are reset by
+// their completers.  Operator values and indices are streamed past L1,
+// gathered vectors go through L1.
 #include <cuda_runtime.h>
 
 #include "common.cuh"
 #include "serve.cuh"
 
 #ifndef B200LA_SRV_MINCTA
-#define B200LA_SRV_MINCTA 2
+#define B200LA_SRV_MINCTA 4
 #endif
 
 namespace b200 {
@@ -48,123 +53,23 @@ __device__ __forceinline__ int check_cg(double v, int step, double res0, double 
     return 0;
 }
 
-struct TileCtx {
+struct WarpCtx {
     SysDesc d;
     SysState s;
-    Tile t;
-    int next_sys;    // system of the CTA's next tile (-1: none)
 };
 
-// Tile walk of one CTA over its contiguous range [t0, t1).  Warp 0 keeps the
-// next tile's entry in flight while the current tile is processed; the
-// system's descriptor and state are fetched only when the system changes
-// (consecutive tiles of one system share them).  All threads call next().
-struct TileWalk {
-    int t, t1, cached;
-    int nx;          // warp 0, lanes 0..3: word `lane` of tile t + 1
-    __device__ __forceinline__ void prefetch(const Tile *tiles)
-    {
-        if (threadIdx.x < 4) nx = (t + 1 < t1) ? __ldcg(reinterpret_cast<const int *>(tiles + t + 1) + threadIdx.x) : -1;
-    }
-    // Make tile t current in c (first call: loads it; later calls: commits
-    // the prefetched entry), then prefetch t + 1.
-    __device__ __forceinline__ void enter(const SysDesc *sys, const SysState *state, const Tile *tiles, TileCtx &c,
-                                          bool first)
-    {
-        __syncthreads();
-        if (threadIdx.x < 32) {
-            const int lane = threadIdx.x;
-            int w = -1;
-            if (first) {
-                if (lane < 4) w = __ldcg(reinterpret_cast<const int *>(tiles + t) + lane);
-            } else {
-                w = nx;
-            }
-            const int s = __shfl_sync(0xffffffffu, w, 0);
-            if (lane < 4) reinterpret_cast<int *>(&c.t)[lane] = w;
-            if (s != cached) {
-                constexpr int dw = (int)(sizeof(SysDesc) / sizeof(int));
-                constexpr int sw = (int)(sizeof(SysState) / sizeof(int));
-                const int *src = reinterpret_cast<const int *>(sys + s);
-                const int *sst = reinterpret_cast<const int *>(state + s);
-                for (int k = lane; k < dw; k += 32) reinterpret_cast<int *>(&c.d)[k] = __ldcg(src + k);
-                for (int k = lane; k < sw; k += 32) reinterpret_cast<int *>(&c.s)[k] = __ldcg(sst + k);
-            }
-            prefetch(tiles);
-        }
-        __syncthreads();
-        cached = c.t.sys;
-    }
-    // After the tile's work: publish the next tile's system (the prefetched
-    // entry has arrived by now) for the end-of-run test.
-    __device__ __forceinline__ void publish_next(TileCtx &c)
-    {
-        if (threadIdx.x < 32) {
-            const int ns = __shfl_sync(0xffffffffu, nx, 0);
-            if (threadIdx.x == 0) c.next_sys = (t + 1 < t1) ? ns : -1;
-        }
-        __syncthreads();
-    }
-};
-
-// Ticket of a system's tiles in one launch: a CTA reports a run of `run`
-// consecutive tiles of one system at once.  The writers of the run's chunk
-// partials (lane 0 of every warp) fence them first.
-__device__ __forceinline__ bool run_done(unsigned *ticket, int run, int ntiles, bool &s_last)
-{
-    if ((threadIdx.x & 31) == 0) __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const bool l = atomicAdd(ticket, (unsigned)run) + (unsigned)run == (unsigned)ntiles;
-        if (l) atomicExch(ticket, 0u);
-        s_last = l;
-    }
-    __syncthreads();
-    const bool l = s_last;
-    if (l) __threadfence();
-    return l;
-}
-
-// Sum of the chunk partials part[q][0..nch) (rows of pstride) in a fixed
-// order: virtual lane v of 256 sums the chunk pairs (2v, 2v+1), (2v+512,
-// 2v+513), ... in index order; the 8 virtual warps fold by a fixed shuffle
-// tree and their sums add in order.  The order is the same for 128 or 256
-// threads; the result is on thread 0.
-template <int NQ, int NW>
-__device__ __forceinline__ void fin_sum(const double *part, int nch, int pstride, double (&o)[NQ], double *sm)
+// Descriptor and state of slot `slot` into the warp's context (all lanes).
+__device__ __forceinline__ void warp_load(const SysDesc *sys, const SysState *state, int slot, WarpCtx &c)
 {
     const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int rep = 0; rep < kFinLanes / (NW * 32); ++rep) {
-        const int v = threadIdx.x + rep * NW * 32;
-        double w[NQ];
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) w[q] = 0.0;
-#pragma unroll 4
-        for (int c = 2 * v; c < nch; c += 2 * kFinLanes) {
-#pragma unroll
-            for (int q = 0; q < NQ; ++q) {
-                const double2 a = __ldcg(reinterpret_cast<const double2 *>(part + (size_t)q * pstride + c));
-                w[q] += a.x;
-                if (c + 1 < nch) w[q] += a.y;
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            const double s = warp_sum(w[q]);
-            if (lane == 0) sm[q * 8 + (v >> 5)] = s;
-        }
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {
-#pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            double s = 0.0;
-            for (int k = 0; k < 8; ++k) s += sm[q * 8 + k];
-            o[q] = s;
-        }
-    }
+    constexpr int dw = (int)(sizeof(SysDesc) / sizeof(int));
+    constexpr int sw = (int)(sizeof(SysState) / sizeof(int));
+    const int *src = reinterpret_cast<const int *>(sys + slot);
+    const int *sst = reinterpret_cast<const int *>(state + slot);
+    __syncwarp();
+    for (int k = lane; k < dw; k += 32) reinterpret_cast<int *>(&c.d)[k] = __ldcg(src + k);
+    for (int k = lane; k < sw; k += 32) reinterpret_cast<int *>(&c.s)[k] = __ldcg(sst + k);
+    __syncwarp();
 }
 
 // p_new(j) = beta p_old(j) + z(j), rounded the same wherever it is formed.
@@ -181,115 +86,94 @@ __device__ __forceinline__ float pnew_at(float beta, const float *__restrict__ p
 __device__ __forceinline__ double zmul(double r, double d) { return __dmul_rn(r, d); }
 __device__ __forceinline__ float zmul(float r, float d) { return __fmul_rn(r, d); }
 
-// SELL row sum, entries added in column order in batches of 9: every load of
-// a batch is issued before its first product.
+// One band of a stencil row: centre w gathered by every lane, neighbours by
+// shuffle, lanes 0 / 31 gather their halo column; products in column order.
+// Columns outside [0, n) belong to zero entries and are clamped into range.
 template <typename T, typename G>
-__device__ __forceinline__ T sell_row(const int *__restrict__ cp, const T *__restrict__ vp, int L, uint64_t pol,
-                                      G gather)
+__device__ __forceinline__ void band(T &s, T a0, T a1, T a2, int i, int he, int d, int n, int lane, G gather)
 {
-    constexpr int B = 9;
-    T s = T(0);
-    for (int k0 = 0; k0 < L; k0 += B) {
-        int cj[B];
-        T a[B];
+    const int last = n - 1;
+    const T w = gather(min(max(i + d, 0), last));
+    const T h = (lane == 0 || lane == 31) ? gather(min(max(he + d, 0), last)) : T(0);
+    T left = __shfl_up_sync(0xffffffffu, w, 1);
+    T right = __shfl_down_sync(0xffffffffu, w, 1);
+    if (lane == 0) left = h;
+    if (lane == 31) right = h;
+    s += a0 * left;
+    s += a1 * w;
+    s += a2 * right;
+}
+
+__device__ __forceinline__ int band_offset(int dim, int P, int b)
+{
+    return dim == 3 ? ((b / 3 - 1) * P + (b % 3 - 1)) * P : (b - 1) * P;
+}
+
+// Stencil row, FP64: groups of three bands, value loads and gathers of a
+// group issued together.
+template <int NB, typename G>
+__device__ __forceinline__ double stencil_row(const double *__restrict__ val, int c, int lane, int n, int P,
+                                              uint64_t pol, G gather)
+{
+    constexpr int DIM = NB == 9 ? 3 : 2;
+    const int r0 = c * kChunk, i = r0 + lane, he = lane == 0 ? r0 - 1 : r0 + 32;
+    const double *v = val + (size_t)c * kChunk * 3 * NB + lane;
+    double s = 0.0;
 #pragma unroll
-        for (int k = 0; k < B; ++k) {
-            if (k0 + k < L) {
-                cj[k] = ld_stream(cp + 32 * (k0 + k), pol);
-                a[k] = ld_stream(vp + 32 * (k0 + k), pol);
-            }
-        }
+    for (int b0 = 0; b0 < NB; b0 += 3) {
+        double a[9];
 #pragma unroll
-        for (int k = 0; k < B; ++k)
-            if (k0 + k < L) s += a[k] * gather(cj[k]);
+        for (int k = 0; k < 9; ++k) a[k] = ld_stream(v + 32 * (3 * b0 + k), pol);
+#pragma unroll
+        for (int bb = 0; bb < 3; ++bb)
+            band(s, a[3 * bb], a[3 * bb + 1], a[3 * bb + 2], i, he, band_offset(DIM, P, b0 + bb), n, lane, gather);
     }
     return s;
 }
 
-// Stencil row sum (FMT_STENCIL).  The positions form bands of three
-// consecutive columns (di = -1, 0, 1 around i + d); lane l gathers only the
-// band centre i + d, takes its left / right neighbours from lanes l - 1 /
-// l + 1, and lanes 0 / 31 gather the one column beyond the chunk.  Products
-// are added in column order, each gathered value formed by gather(j) exactly
-// as a direct gather would.  Columns outside [0, n) belong to zero entries
-// and are clamped into range.
-template <typename T, int DIM, int U, typename G>
-__device__ __forceinline__ void stencil_rows(const T *__restrict__ val, int L, const int (&cc)[U], int lane, int n,
-                                             int P, uint64_t pol, G gather, T (&s)[U])
+// Stencil row, FP32: the row's positions in groups of four per lane (one
+// 16-byte load each), then the bands.
+template <int NB, typename G>
+__device__ __forceinline__ float stencil_row(const float *__restrict__ val, int c, int lane, int n, int P,
+                                             uint64_t pol, G gather)
 {
-    constexpr int NB = DIM == 3 ? 9 : 3;
-    const bool edge = lane == 0 || lane == 31;
+    constexpr int DIM = NB == 9 ? 3 : 2, L = 3 * NB, GR = (L + 3) / 4;
+    const int r0 = c * kChunk, i = r0 + lane, he = lane == 0 ? r0 - 1 : r0 + 32;
+    const float4 *v = reinterpret_cast<const float4 *>(val + (size_t)c * kChunk * 4 * GR) + lane;
+    float a[4 * GR];
 #pragma unroll
-    for (int u = 0; u < U; ++u) s[u] = T(0);
-#pragma unroll
-    for (int b0 = 0; b0 < NB; b0 += 3) {
-        T a[U][9], w[U][3], h[U][3];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int r0 = cc[u] * kChunk, i = r0 + lane;
-            const int he = lane == 0 ? r0 - 1 : r0 + 32;     // halo column before the band offset
-            const T *vp = val + (size_t)cc[u] * kChunk * L + lane;
-#pragma unroll
-            for (int bb = 0; bb < 3; ++bb) {
-                const int band = b0 + bb;
-                const int d = DIM == 3 ? ((band / 3 - 1) * P + (band % 3 - 1)) * P : (band - 1) * P;
-#pragma unroll
-                for (int m = 0; m < 3; ++m) a[u][3 * bb + m] = ld_stream(vp + 32 * (3 * band + m), pol);
-                w[u][bb] = gather(min(max(i + d, 0), n - 1));
-                h[u][bb] = edge ? gather(min(max(he + d, 0), n - 1)) : T(0);
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-#pragma unroll
-            for (int bb = 0; bb < 3; ++bb) {
-                T left = __shfl_up_sync(0xffffffffu, w[u][bb], 1);
-                T right = __shfl_down_sync(0xffffffffu, w[u][bb], 1);
-                if (lane == 0) left = h[u][bb];
-                if (lane == 31) right = h[u][bb];
-                s[u] += a[u][3 * bb] * left;
-                s[u] += a[u][3 * bb + 1] * w[u][bb];
-                s[u] += a[u][3 * bb + 2] * right;
-            }
-        }
-        // keep one group of three bands in flight at a time (register budget)
-        if (b0 + 3 < NB) asm volatile("" ::: "memory");
+    for (int g = 0; g < GR; ++g) {
+        float4 q;
+        asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+            : "=f"(q.x), "=f"(q.y), "=f"(q.z), "=f"(q.w)
+            : "l"(v + 32 * g), "l"(pol));
+        a[4 * g] = q.x;
+        a[4 * g + 1] = q.y;
+        a[4 * g + 2] = q.z;
+        a[4 * g + 3] = q.w;
     }
+    float s = 0.0f;
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+        band(s, a[3 * b], a[3 * b + 1], a[3 * b + 2], i, he, band_offset(DIM, P, b), n, lane, gather);
+    return s;
 }
 
+// SELL and CSRW rows (uploaded CSR requests), out of line.
 template <typename T, typename G>
-__device__ __noinline__ T row_spmv_indexed(const SysDesc &d, const T *__restrict__ val, int c, int lane,
-                                           uint64_t pol, G gather);
-
-// Row 32 c + lane of A v, v given by gather(j).  SELL / STENCIL: one thread
-// per row, entries in column order.  CSRW: one warp per row, lanes strided
-// over the row, a fixed xor tree.
-template <typename T, typename G>
-__device__ __forceinline__ T row_spmv(const SysDesc &d, const T *__restrict__ val, int c, int lane, uint64_t pol,
+__device__ __noinline__ T row_indexed(const SysDesc &d, const T *__restrict__ val, int c, int lane, uint64_t pol,
                                       G gather)
 {
-    const int fmt = d.fmt, n = d.n;
-    if (fmt == FMT_STENCIL) {
-        const int cc[1] = {c};
-        T s[1];
-        if (d.sdim == 3) stencil_rows<T, 3, 1>(val, d.sL, cc, lane, n, d.sP, pol, gather, s);
-        else stencil_rows<T, 2, 1>(val, d.sL, cc, lane, n, d.sP, pol, gather, s);
-        return s[0];
-    }
-    return row_spmv_indexed<T>(d, val, c, lane, pol, gather);
-}
-
-// SELL and CSRW rows (uploaded CSR requests), out of line so that their
-// registers do not constrain the stencil path.
-template <typename T, typename G>
-__device__ __noinline__ T row_spmv_indexed(const SysDesc &d, const T *__restrict__ val, int c, int lane,
-                                           uint64_t pol, G gather)
-{
-    const int fmt = d.fmt, n = d.n;
+    const int n = d.n;
     const int *off = d.off, *col = d.col;
-    if (fmt == FMT_SELL) {
+    if (d.fmt == FMT_SELL) {
         const int b = __ldg(off + c), L = (__ldg(off + c + 1) - b) >> 5;
-        return sell_row<T>(col + b + lane, val + b + lane, L, pol, gather);
+        const int *cp = col + b + lane;
+        const T *vp = val + b + lane;
+        T s = T(0);
+#pragma unroll 3
+        for (int k = 0; k < L; ++k) s += ld_stream(vp + 32 * k, pol) * gather(ld_stream(cp + 32 * k, pol));
+        return s;
     }
     T mine = T(0);
     const int r0 = c * kChunk;
@@ -305,46 +189,117 @@ __device__ __noinline__ T row_spmv_indexed(const SysDesc &d, const T *__restrict
     return mine;
 }
 
+// Row 32 c + lane of A v, v given by gather(j).
+template <typename T, typename G>
+__device__ __forceinline__ T row_spmv(const SysDesc &d, const T *__restrict__ val, int c, int lane, uint64_t pol,
+                                      G gather)
+{
+    if (d.fmt == FMT_STENCIL) {
+        if (d.sdim == 3) return stencil_row<9>(val, c, lane, d.n, d.sP, pol, gather);
+        return stencil_row<3>(val, c, lane, d.n, d.sP, pol, gather);
+    }
+    return row_indexed<T>(d, val, c, lane, pol, gather);
+}
+
+// ------------------------------------------------------------------ system table
+
+constexpr int kTabSmem = 2048;   // first chunks of up to this many systems kept in shared memory
+
+// First chunk of every active system into shared memory (one barrier).
+__device__ __forceinline__ void load_cbeg(const SysRun *tab, int nsys, int *s_cbeg)
+{
+    for (int k = threadIdx.x; k < min(nsys, kTabSmem); k += blockDim.x) s_cbeg[k] = __ldcg(&tab[k].cbeg);
+    __syncthreads();
+}
+
+// The system whose chunks contain g (binary search; shared memory when the
+// table fits).
+__device__ __forceinline__ int find_system(const SysRun *tab, int nsys, const int *s_cbeg, int g)
+{
+    int lo = 0, hi = nsys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        const int cb = nsys <= kTabSmem ? s_cbeg[mid] : __ldcg(&tab[mid].cbeg);
+        if (cb <= g) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------------ reporting
+
+// After the warp has written the partials of chunks [c0, c1) of its system
+// (lane 0 writes them): report them to their groups; a completed group is
+// summed; the completion of the last group runs fin(o) on the warp (o valid
+// on every lane).  NQ quantities.
+template <int NQ, typename F>
+__device__ __forceinline__ void report(const WarpCtx &c, int c0, int c1, F fin)
+{
+    const int lane = threadIdx.x & 31;
+    const SysDesc &d = c.d;
+    if (lane == 0) __threadfence();
+    for (int g = c0 / kGroup; g * kGroup < c1; ++g) {
+        const int a = max(c0, g * kGroup), b = min(c1, (g + 1) * kGroup);
+        const int gsize = min(d.nchunks, (g + 1) * kGroup) - g * kGroup;
+        int done = 0;
+        if (lane == 0) {
+            const unsigned old = atomicAdd(d.gcnt + g, (unsigned)(b - a));
+            done = old + (unsigned)(b - a) == (unsigned)gsize;
+        }
+        done = __shfl_sync(0xffffffffu, done, 0);
+        if (!done) continue;
+        // group g complete: sum its chunk partials (fixed xor tree)
+        __threadfence();
+        double v[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            const int ch = g * kGroup + lane;
+            v[q] = warp_sum(ch < d.nchunks ? __ldcg(d.part + (size_t)q * d.pstride + ch) : 0.0);
+        }
+        int last = 0;
+        if (lane == 0) {
+#pragma unroll
+            for (int q = 0; q < NQ; ++q) d.gpart[(size_t)q * d.gstride + g] = v[q];
+            d.gcnt[g] = 0u;
+            __threadfence();
+            const unsigned old = atomicAdd(d.ticket, 1u);
+            last = old + 1u == (unsigned)d.ngroups;
+            if (last) d.ticket[0] = 0u;
+        }
+        last = __shfl_sync(0xffffffffu, last, 0);
+        if (!last) continue;
+        // all groups complete: lane l sums groups l, l + 32, ... in order
+        __threadfence();
+        double o[NQ];
+#pragma unroll
+        for (int q = 0; q < NQ; ++q) {
+            double w = 0.0;
+            for (int k = lane; k < d.ngroups; k += 32) w += __ldcg(d.gpart + (size_t)q * d.gstride + k);
+            o[q] = warp_sum(w);
+        }
+        fin(o);
+    }
+}
+
 // ------------------------------------------------------------------ k1
 
-template <typename T, int NW>
-__device__ __forceinline__ void k1_chunks(const TileCtx &c, const T *val, uint64_t pol)
+template <typename T>
+__device__ __forceinline__ void k1_range(const WarpCtx &c, SysState *st, int c0, int c1, uint64_t pol)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n = c.d.n;
+    const int lane = threadIdx.x & 31;
+    const SysDesc &d = c.d;
+    const int n = d.n;
     const T beta = (T)c.s.beta;
     const bool b0 = c.s.pbuf == 0;
-    const T *po = static_cast<const T *>(b0 ? c.d.p0 : c.d.p1);
-    T *pn = static_cast<T *>(b0 ? c.d.p1 : c.d.p0);
-    const T *z = static_cast<const T *>(c.d.z);
-    T *ap = static_cast<T *>(c.d.ap);
-    double *part = c.d.part;
+    const T *po = static_cast<const T *>(b0 ? d.p0 : d.p1);
+    T *pn = static_cast<T *>(b0 ? d.p1 : d.p0);
+    const T *z = static_cast<const T *>(d.z);
+    T *ap = static_cast<T *>(d.ap);
+    const T *val = sizeof(T) == 8 ? reinterpret_cast<const T *>(d.val64) : reinterpret_cast<const T *>(d.val32);
     auto gather = [=](int j) { return pnew_at(beta, po, z, j); };
-    int ch = c.t.c0 + warp;
-    if (c.d.fmt == FMT_STENCIL && c.d.sdim == 2) {
-        // 2-D stencil: two chunks per warp with their loads in flight together
-        for (; ch + NW < c.t.c1; ch += 2 * NW) {
-            const int cc[2] = {ch, ch + NW};
-            T s2[2];
-            stencil_rows<T, 2, 2>(val, c.d.sL, cc, lane, n, c.d.sP, pol, gather, s2);
-#pragma unroll
-            for (int u = 0; u < 2; ++u) {
-                const int i = cc[u] * kChunk + lane;
-                double dp = 0.0;
-                if (i < n) {
-                    const T pi = pnew_at(beta, po, z, i);
-                    pn[i] = pi;
-                    ap[i] = s2[u];
-                    dp = (double)(pi * s2[u]);
-                }
-                dp = warp_sum(dp);
-                if (lane == 0) part[cc[u]] = dp;
-            }
-        }
-    }
-    for (; ch < c.t.c1; ch += NW) {
+    for (int ch = c0; ch < c1; ++ch) {
         const int i = ch * kChunk + lane;
-        const T s = row_spmv<T>(c.d, val, ch, lane, pol, gather);
+        const T s = row_spmv<T>(d, val, ch, lane, pol, gather);
         double dp = 0.0;
         if (i < n) {
             const T pi = pnew_at(beta, po, z, i);
@@ -353,183 +308,70 @@ __device__ __forceinline__ void k1_chunks(const TileCtx &c, const T *val, uint64
             dp = (double)(pi * s);
         }
         dp = warp_sum(dp);
-        if (lane == 0) part[ch] = dp;
+        if (lane == 0) d.part[ch] = dp;
     }
+    const double rho = c.s.rho;
+    const int pbuf = c.s.pbuf;
+    report<1>(c, c0, c1, [&](const double *o) {
+        if (lane == 0) {
+            st->alpha = rho / o[0];
+            st->pbuf = pbuf ^ 1;
+        }
+    });
 }
 
-template <int NW>
-__device__ __forceinline__ void k1_correct(const TileCtx &c)
+__device__ __forceinline__ void k1_correct(const WarpCtx &c, int c0, int c1)
 {
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31;
     const int n = c.d.n;
     double *x = c.d.x;
     const float *xl = static_cast<const float *>(c.d.xl);
-    for (int ch = c.t.c0 + warp; ch < c.t.c1; ch += NW) {
+    for (int ch = c0; ch < c1; ++ch) {
         const int i = ch * kChunk + lane;
         if (i < n) x[i] += (double)xl[i];
     }
 }
 
 template <int NW>
-__global__ void __launch_bounds__(NW * 32, kMinCta256 * 8 / NW) k1_kernel(const SysDesc *__restrict__ sys, SysState *state,
-                                                     const int *__restrict__ tb)
+__global__ void __launch_bounds__(NW * 32, kMinCta256 * 8 / NW) k1_kernel(const SysDesc *__restrict__ sys,
+                                                                       SysState *state, const int *__restrict__ tb)
 {
-    __shared__ TileCtx c;
-    __shared__ double sm[8 * 3];
-    __shared__ bool last;
-    const int ntiles = __ldcg(tb);
-    const Tile *tiles = reinterpret_cast<const Tile *>(tb + kTileHdrWords);
+    __shared__ WarpCtx ctx[NW];
+    __shared__ int s_cbeg[kTabSmem];
+    WarpCtx &c = ctx[threadIdx.x >> 5];
+    const int nsys = __ldcg(tb), T = __ldcg(tb + 1), C = __ldcg(tb + 2);
+    const SysRun *tab = reinterpret_cast<const SysRun *>(tb + kTabHdrWords);
+    load_cbeg(tab, nsys, s_cbeg);
     const uint64_t pol = l2_policy(0);
-    const int t0 = (int)((long long)blockIdx.x * ntiles / gridDim.x);
-    const int t1 = (int)((long long)(blockIdx.x + 1) * ntiles / gridDim.x);
-    TileWalk w{t0, t1, -1, -1};
-    int run = 0;
-    for (; w.t < t1; ++w.t) {
-        w.enter(sys, state, tiles, c, w.t == t0);
-        const int ph = c.s.phase;
-        if (ph == PH_CORRECT) {
-            k1_correct<NW>(c);
-            continue;
-        }
-        if (ph != PH_CG && ph != PH_INNER) continue;
-        if (ph == PH_CG) k1_chunks<double, NW>(c, c.d.val64, pol);
-        else k1_chunks<float, NW>(c, c.d.val32, pol);
-        ++run;
-        w.publish_next(c);
-        if (c.next_sys == c.t.sys) continue;
-        const int r = run;
-        run = 0;
-        if (run_done(c.d.ticket, r, c.t.ntiles, last)) {
-            double o[1];
-            fin_sum<1, NW>(c.d.part, c.d.nchunks, c.d.pstride, o, sm);
-            if (threadIdx.x == 0) {
-                SysState *st = state + c.t.sys;
-                st->alpha = c.s.rho / o[0];
-                st->pbuf = c.s.pbuf ^ 1;
+    const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nw = gridDim.x * NW;
+    (void)C;
+    // one contiguous range of the chunk sequence per warp: runs within a
+    // system are long, so a warp reports about once per system it touches
+    const int g0 = (int)((long long)gw * T / nw), g1 = (int)((long long)(gw + 1) * T / nw);
+    int si = 0, loaded = -1;
+    if (g0 < g1) {
+        si = find_system(tab, nsys, s_cbeg, g0);
+        for (int g = g0; g < g1;) {
+            const int slot = __ldcg(&tab[si].slot), cb = __ldcg(&tab[si].cbeg), nch = __ldcg(&tab[si].nch);
+            const int e = min(g1, cb + nch);
+            if (slot != loaded) {
+                warp_load(sys, state, slot, c);
+                loaded = slot;
             }
+            const int ph = c.s.phase, c0 = g - cb, c1 = e - cb;
+            if (ph == PH_CG) k1_range<double>(c, state + slot, c0, c1, pol);
+            else if (ph == PH_INNER) k1_range<float>(c, state + slot, c0, c1, pol);
+            else if (ph == PH_CORRECT) k1_correct(c, c0, c1);
+            g = e;
+            if (g < g1) ++si;
         }
     }
 }
 
 // ------------------------------------------------------------------ k2
 
-template <typename T, int NW>
-__device__ __forceinline__ void k2_update(const TileCtx &c, T *x)
-{
-    constexpr int U = 4;   // chunks per warp with loads in flight together
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n = c.d.n, ps = c.d.pstride, c1 = c.t.c1;
-    const T alpha = (T)c.s.alpha;
-    T *r = static_cast<T *>(c.d.r), *z = static_cast<T *>(c.d.z);
-    const T *p = static_cast<const T *>(c.s.pbuf == 0 ? c.d.p0 : c.d.p1);
-    const T *ap = static_cast<const T *>(c.d.ap), *dv = static_cast<const T *>(c.d.invd);
-    double *part = c.d.part;
-    for (int ch0 = c.t.c0 + warp; ch0 < c1; ch0 += U * NW) {
-        T xv[U], rv[U], pv[U], av[U], dd[U];
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int ch = ch0 + u * NW, i = ch * kChunk + lane;
-            if (ch < c1 && i < n) {
-                xv[u] = x[i];
-                rv[u] = r[i];
-                pv[u] = p[i];
-                av[u] = __ldcs(ap + i);
-                dd[u] = dv[i];
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const int ch = ch0 + u * NW, i = ch * kChunk + lane;
-            if (ch >= c1) break;
-            double rr = 0.0, rz = 0.0;
-            if (i < n) {
-                const T xi = xv[u] + alpha * pv[u];
-                const T ri = rv[u] - alpha * av[u];
-                const T zi = zmul(ri, dd[u]);
-                x[i] = xi;
-                r[i] = ri;
-                z[i] = zi;
-                rr = (double)(ri * ri);
-                rz = (double)(ri * zi);
-            }
-            rr = warp_sum(rr);
-            rz = warp_sum(rz);
-            if (lane == 0) {
-                part[ch] = rr;
-                part[ps + ch] = rz;
-            }
-        }
-    }
-}
-
-template <int NW>
-__device__ __forceinline__ void k2_start(const TileCtx &c)
-{
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n = c.d.n, ps = c.d.pstride;
-    double *r = static_cast<double *>(c.d.r), *z = static_cast<double *>(c.d.z);
-    const double *b = c.d.b, *dv = static_cast<const double *>(c.d.invd);
-    double *part = c.d.part;
-    for (int ch = c.t.c0 + warp; ch < c.t.c1; ch += NW) {
-        const int i = ch * kChunk + lane;
-        double rr = 0.0, rz = 0.0;
-        if (i < n) {
-            const double ri = b[i];
-            const double zi = zmul(ri, dv[i]);
-            r[i] = ri;
-            z[i] = zi;
-            rr = ri * ri;
-            rz = ri * zi;
-        }
-        rr = warp_sum(rr);
-        rz = warp_sum(rz);
-        if (lane == 0) {
-            part[ch] = rr;
-            part[ps + ch] = rz;
-        }
-    }
-}
-
-// Runs once per outer step of a mixed system: kept out of line so that its
-// registers do not constrain the per-iteration update.
-template <int NW>
-__device__ __noinline__ void k2_outer(const TileCtx &c, uint64_t pol)
-{
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int n = c.d.n, ps = c.d.pstride;
-    const double *b = c.d.b, *x = c.d.x, *val = c.d.val64;
-    float *rl = static_cast<float *>(c.d.r), *zl = static_cast<float *>(c.d.z), *xl = static_cast<float *>(c.d.xl);
-    const float *dv = static_cast<const float *>(c.d.invd);
-    double *part = c.d.part;
-    auto gather = [=](int j) { return __ldg(x + j); };
-    for (int ch = c.t.c0 + warp; ch < c.t.c1; ch += NW) {
-        const int i = ch * kChunk + lane;
-        const double s = row_spmv<double>(c.d, val, ch, lane, pol, gather);
-        double q0 = 0.0, q1 = 0.0, q2 = 0.0;
-        if (i < n) {
-            const double r = b[i] - s;
-            const float f = (float)r;
-            const float zf = zmul(f, dv[i]);
-            rl[i] = f;
-            zl[i] = zf;
-            xl[i] = 0.0f;
-            q0 = r * r;
-            q1 = (double)(f * zf);
-            q2 = (double)(f * f);
-        }
-        q0 = warp_sum(q0);
-        q1 = warp_sum(q1);
-        q2 = warp_sum(q2);
-        if (lane == 0) {
-            part[ch] = q0;
-            part[ps + ch] = q1;
-            part[2 * ps + ch] = q2;
-        }
-    }
-}
-
-// Thread 0 of the CTA completing a system's update tiles.  cs: the state as
-// read at the tile start (nothing else writes it during this launch).
+// Lane 0 of the completing warp.  cs: the state as read before this launch
+// changed it (nothing else writes it during the launch).
 __device__ __forceinline__ void k2_finish(const SysState &cs, SysState *st, int *done, int ph, const double *o)
 {
     if (ph == PH_CG) {
@@ -600,62 +442,152 @@ __device__ __forceinline__ void k2_finish(const SysState &cs, SysState *st, int 
     }
 }
 
-// The completing CTA of a system's update tiles (out of line: once per
-// system and launch).
-template <int NW>
-__device__ __noinline__ void k2_final(const TileCtx &c, SysState *state, int ph, int nq, double *sm)
+template <typename T>
+__device__ __forceinline__ void k2_update(const WarpCtx &c, SysState *st, int c0, int c1)
 {
-    double o[3] = {0.0, 0.0, 0.0};
-    if (nq == 2) {
-        double o2[2];
-        fin_sum<2, NW>(c.d.part, c.d.nchunks, c.d.pstride, o2, sm);
-        o[0] = o2[0];
-        o[1] = o2[1];
-    } else {
-        fin_sum<3, NW>(c.d.part, c.d.nchunks, c.d.pstride, o, sm);
+    const int lane = threadIdx.x & 31;
+    const SysDesc &d = c.d;
+    const int n = d.n, ps = d.pstride;
+    const T alpha = (T)c.s.alpha;
+    T *x = sizeof(T) == 8 ? reinterpret_cast<T *>(d.x) : static_cast<T *>(d.xl);
+    T *r = static_cast<T *>(d.r), *z = static_cast<T *>(d.z);
+    const T *p = static_cast<const T *>(c.s.pbuf == 0 ? d.p0 : d.p1);
+    const T *ap = static_cast<const T *>(d.ap), *dv = static_cast<const T *>(d.invd);
+    for (int ch = c0; ch < c1; ++ch) {
+        const int i = ch * kChunk + lane;
+        double rr = 0.0, rz = 0.0;
+        if (i < n) {
+            const T xi = x[i] + alpha * p[i];
+            const T ri = r[i] - alpha * __ldcs(ap + i);
+            const T zi = zmul(ri, dv[i]);
+            x[i] = xi;
+            r[i] = ri;
+            z[i] = zi;
+            rr = (double)(ri * ri);
+            rz = (double)(ri * zi);
+        }
+        rr = warp_sum(rr);
+        rz = warp_sum(rz);
+        if (lane == 0) {
+            d.part[ch] = rr;
+            d.part[ps + ch] = rz;
+        }
     }
-    if (threadIdx.x == 0) k2_finish(c.s, state + c.t.sys, c.d.done, ph, o);
+    const SysState cs = c.s;
+    const int ph = cs.phase;
+    report<2>(c, c0, c1, [&](const double *o) {
+        if (lane == 0) k2_finish(cs, st, d.done, ph, o);
+    });
+}
+
+__device__ __forceinline__ void k2_start(const WarpCtx &c, SysState *st, int c0, int c1)
+{
+    const int lane = threadIdx.x & 31;
+    const SysDesc &d = c.d;
+    const int n = d.n, ps = d.pstride;
+    double *r = static_cast<double *>(d.r), *z = static_cast<double *>(d.z);
+    const double *b = d.b, *dv = static_cast<const double *>(d.invd);
+    for (int ch = c0; ch < c1; ++ch) {
+        const int i = ch * kChunk + lane;
+        double rr = 0.0, rz = 0.0;
+        if (i < n) {
+            const double ri = b[i];
+            const double zi = zmul(ri, dv[i]);
+            r[i] = ri;
+            z[i] = zi;
+            rr = ri * ri;
+            rz = ri * zi;
+        }
+        rr = warp_sum(rr);
+        rz = warp_sum(rz);
+        if (lane == 0) {
+            d.part[ch] = rr;
+            d.part[ps + ch] = rz;
+        }
+    }
+    const SysState cs = c.s;
+    report<2>(c, c0, c1, [&](const double *o) {
+        if (lane == 0) k2_finish(cs, st, d.done, PH_CG_START, o);
+    });
+}
+
+// Runs once per outer step of a mixed system: kept out of line so that its
+// registers do not constrain the per-iteration update.
+__device__ __noinline__ void k2_outer(const WarpCtx &c, SysState *st, int c0, int c1, uint64_t pol)
+{
+    const int lane = threadIdx.x & 31;
+    const SysDesc &d = c.d;
+    const int n = d.n, ps = d.pstride;
+    const double *b = d.b, *x = d.x;
+    float *rl = static_cast<float *>(d.r), *zl = static_cast<float *>(d.z), *xl = static_cast<float *>(d.xl);
+    const float *dv = static_cast<const float *>(d.invd);
+    auto gather = [=](int j) { return __ldg(x + j); };
+    for (int ch = c0; ch < c1; ++ch) {
+        const int i = ch * kChunk + lane;
+        const double s = row_spmv<double>(d, d.val64, ch, lane, pol, gather);
+        double q0 = 0.0, q1 = 0.0, q2 = 0.0;
+        if (i < n) {
+            const double r = b[i] - s;
+            const float f = (float)r;
+            const float zf = zmul(f, dv[i]);
+            rl[i] = f;
+            zl[i] = zf;
+            xl[i] = 0.0f;
+            q0 = r * r;
+            q1 = (double)(f * zf);
+            q2 = (double)(f * f);
+        }
+        q0 = warp_sum(q0);
+        q1 = warp_sum(q1);
+        q2 = warp_sum(q2);
+        if (lane == 0) {
+            d.part[ch] = q0;
+            d.part[ps + ch] = q1;
+            d.part[2 * ps + ch] = q2;
+        }
+    }
+    const SysState cs = c.s;
+    const int ph = cs.phase;
+    report<3>(c, c0, c1, [&](const double *o) {
+        if (lane == 0) k2_finish(cs, st, d.done, ph, o);
+    });
 }
 
 template <int NW>
-__global__ void __launch_bounds__(NW * 32, kMinCta256 * 8 / NW) k2_kernel(const SysDesc *__restrict__ sys, SysState *state,
-                                                     const int *__restrict__ tb)
+__global__ void __launch_bounds__(NW * 32, kMinCta256 * 8 / NW) k2_kernel(const SysDesc *__restrict__ sys,
+                                                                       SysState *state, const int *__restrict__ tb)
 {
-    __shared__ TileCtx c;
-    __shared__ double sm[8 * 3];
-    __shared__ bool last;
-    const int ntiles = __ldcg(tb);
-    const Tile *tiles = reinterpret_cast<const Tile *>(tb + kTileHdrWords);
+    __shared__ WarpCtx ctx[NW];
+    __shared__ int s_cbeg[kTabSmem];
+    WarpCtx &c = ctx[threadIdx.x >> 5];
+    const int nsys = __ldcg(tb), T = __ldcg(tb + 1), C = __ldcg(tb + 2);
+    const SysRun *tab = reinterpret_cast<const SysRun *>(tb + kTabHdrWords);
+    load_cbeg(tab, nsys, s_cbeg);
     const uint64_t pol = l2_policy(0);
-    const int t0 = (int)((long long)blockIdx.x * ntiles / gridDim.x);
-    const int t1 = (int)((long long)(blockIdx.x + 1) * ntiles / gridDim.x);
-    TileWalk w{t0, t1, -1, -1};
-    int run = 0;
-    for (; w.t < t1; ++w.t) {
-        w.enter(sys, state, tiles, c, w.t == t0);
-        const int ph = c.s.phase;
-        int nq;
-        if (ph == PH_CG) {
-            k2_update<double, NW>(c, c.d.x);
-            nq = 2;
-        } else if (ph == PH_INNER) {
-            k2_update<float, NW>(c, static_cast<float *>(c.d.xl));
-            nq = 2;
-        } else if (ph == PH_CG_START) {
-            k2_start<NW>(c);
-            nq = 2;
-        } else if (ph == PH_OUTER || ph == PH_CORRECT) {
-            k2_outer<NW>(c, pol);
-            nq = 3;
-        } else {
-            continue;
+    const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nw = gridDim.x * NW;
+    (void)C;
+    // one contiguous range of the chunk sequence per warp: runs within a
+    // system are long, so a warp reports about once per system it touches
+    const int g0 = (int)((long long)gw * T / nw), g1 = (int)((long long)(gw + 1) * T / nw);
+    int si = 0, loaded = -1;
+    if (g0 < g1) {
+        si = find_system(tab, nsys, s_cbeg, g0);
+        for (int g = g0; g < g1;) {
+            const int slot = __ldcg(&tab[si].slot), cb = __ldcg(&tab[si].cbeg), nch = __ldcg(&tab[si].nch);
+            const int e = min(g1, cb + nch);
+            if (slot != loaded) {
+                warp_load(sys, state, slot, c);
+                loaded = slot;
+            }
+            const int ph = c.s.phase, c0 = g - cb, c1 = e - cb;
+            SysState *st = state + slot;
+            if (ph == PH_CG) k2_update<double>(c, st, c0, c1);
+            else if (ph == PH_INNER) k2_update<float>(c, st, c0, c1);
+            else if (ph == PH_CG_START) k2_start(c, st, c0, c1);
+            else if (ph == PH_OUTER || ph == PH_CORRECT) k2_outer(c, st, c0, c1, pol);
+            g = e;
+            if (g < g1) ++si;
         }
-        ++run;
-        w.publish_next(c);
-        if (c.next_sys == c.t.sys) continue;
-        const int r = run;
-        run = 0;
-        if (run_done(c.d.ticket + 32, r, c.t.ntiles, last)) k2_final<NW>(c, state, ph, nq, sm);
     }
 }
 
@@ -674,16 +606,17 @@ __global__ void build_slot_kernel(SysDesc d, const int *__restrict__ row, const 
         if (d.fmt == FMT_STENCIL) {
             // values zero-filled before; each stored entry to its position
             if (i < n) {
-                const int c = i / kChunk, lane = i % kChunk;
-                const size_t base = (size_t)c * kChunk * d.sL + lane;
+                const int c = i / kChunk, lane = i % kChunk, L = d.sL, GR = (L + 3) / 4;
+                const size_t base = (size_t)c * kChunk * L + lane;
+                const size_t base32 = (size_t)c * kChunk * 4 * GR + 4 * lane;
                 double *ov = const_cast<double *>(d.val64);
                 float *of = const_cast<float *>(d.val32);
                 for (int j = rb; j < re; ++j) {
                     const int dl = col[j] - i;
-                    for (int k = 0; k < d.sL; ++k)
+                    for (int k = 0; k < L; ++k)
                         if (stencil_delta(d.sdim, d.sP, k) == dl) {
                             ov[base + (size_t)kChunk * k] = val[j];
-                            if (d.mixed) of[base + (size_t)kChunk * k] = (float)val[j];
+                            if (d.mixed) of[base32 + (size_t)(k / 4) * 128 + k % 4] = (float)val[j];
                         }
                 }
             }
@@ -728,14 +661,14 @@ __global__ void build_slot_kernel(SysDesc d, const int *__restrict__ row, const 
 
 }  // namespace
 
-cudaError_t launch_round(int nw, int grid, const SysDesc *sys, SysState *state, const int *tiles, cudaStream_t st)
+cudaError_t launch_round(int nw, int grid, const SysDesc *sys, SysState *state, const int *tab, cudaStream_t st)
 {
     if (nw == 4) {
-        k1_kernel<4><<<grid, 128, 0, st>>>(sys, state, tiles);
-        k2_kernel<4><<<grid, 128, 0, st>>>(sys, state, tiles);
+        k1_kernel<4><<<grid, 128, 0, st>>>(sys, state, tab);
+        k2_kernel<4><<<grid, 128, 0, st>>>(sys, state, tab);
     } else {
-        k1_kernel<8><<<grid, 256, 0, st>>>(sys, state, tiles);
-        k2_kernel<8><<<grid, 256, 0, st>>>(sys, state, tiles);
+        k1_kernel<8><<<grid, 256, 0, st>>>(sys, state, tab);
+        k2_kernel<8><<<grid, 256, 0, st>>>(sys, state, tab);
     }
     return cudaGetLastError();
 }

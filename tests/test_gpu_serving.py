@@ -142,7 +142,9 @@ def test_serve_continuous_admission(b200, srv):
         # runs exactly 4000 iterations (no tolerance can be met)
         big = s.submit(q1=dict(dim=2, N=256), rhs_seed=1, ctl=(4000, 0.0, 0.0, 1e300))
         import time
-        time.sleep(0.005)
+        t0 = time.time()
+        while s.stats()["rounds"] < 2 and time.time() - t0 < 30.0:   # the big request is iterating
+            time.sleep(0.001)
         small = [s.submit(q1=dict(dim=2, N=40 + k), rhs_seed=2 + k) for k in range(6)]
         rs = [s.wait(i) for i in small]
         rb = s.wait(big)
