@@ -274,13 +274,173 @@ __global__ void __launch_bounds__(kLevelThreads) level_sweep_cta_kernel(LevelSwe
     }
 }
 
+// The level sweep with a deeper look-ahead through the async-copy engine.
+// At set-up every row of L / U is packed into kp fixed slots (columns and
+// values, the entry count beside).  Each thread copies its row of level
+// k + kStages - 1 (packed entries, count, own input and scalings) into a
+// shared-memory stage with cp.async while level k is solved, so the loads of
+// a level arrive kStages - 1 levels early and only the ring gathers, the
+// solve and the level barrier remain on the critical path.
+constexpr int kStages = 4;
+constexpr int kRingStaged = 4096;
+constexpr int kStagedMaxLevels = 4096;
+constexpr int kStagedSlots = 4;    // packed entries per row (rows of L and U with at most this many)
+
+struct LevelStagedArgs {
+    const int *pcol;      // packed columns [n][kp]
+    const void *pval;     // packed values [n][kp]
+    const int *pcnt;      // entries per row
+    const int *off;
+    int nlev, n;
+    const void *r;
+    void *z;
+    const void *d1, *d2;
+    int backward, sgs;
+    const int *gate;
+};
+
+__device__ __forceinline__ void cp_async(void *dst, const void *src, int bytes)
+{
+    const unsigned d = smem_u32(dst);
+    if (bytes == 16) asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(src) : "memory");
+    else if (bytes == 8) asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+    else asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+template <typename T, int KP>
+struct StageRec {
+    int col[KP];
+    T val[KP];
+    T own, e1, e2;
+    int cnt;
+};
+
+template <typename T, int KP>
+__global__ void __launch_bounds__(kLevelThreads) level_sweep_staged_kernel(LevelStagedArgs a)
+{
+    extern __shared__ __align__(16) unsigned char s_raw[];
+    using Rec = StageRec<T, KP>;
+    Rec *stage = reinterpret_cast<Rec *>(s_raw);                             // [kStages][kLevelThreads]
+    T *ring = reinterpret_cast<T *>(s_raw + sizeof(Rec) * kStages * kLevelThreads);
+    int *s_off = reinterpret_cast<int *>(ring + kRingStaged);
+    if (gate_closed(a.gate)) return;
+    for (int i = threadIdx.x; i <= a.nlev; i += kLevelThreads) s_off[i] = __ldg(a.off + i);
+    __syncthreads();
+    const int tid = threadIdx.x, nlev = a.nlev;
+    const T *pval = static_cast<const T *>(a.pval);
+    const T *r = static_cast<const T *>(a.r);
+    const T *d1 = static_cast<const T *>(a.d1);
+    const T *d2 = static_cast<const T *>(a.d2);
+    T *z = static_cast<T *>(a.z);
+    const bool need_e1 = a.backward || a.sgs, need_e2 = a.backward && a.sgs;
+    auto level_of = [&](int k) { return a.backward ? nlev - 1 - k : k; };
+    // this thread's row of level k into stage k % kStages (one commit group per level)
+    auto issue = [&](int k) {
+        if (k < nlev) {
+            const int l = level_of(k), rr = s_off[l] + tid;
+            if (rr < s_off[l + 1]) {
+                Rec &q = stage[(k % kStages) * kLevelThreads + tid];
+#pragma unroll
+                for (int b = 0; b < KP * 4; b += 16) cp_async(reinterpret_cast<char *>(q.col) + b,
+                                                              reinterpret_cast<const char *>(a.pcol + (size_t)rr * KP) + b, 16);
+#pragma unroll
+                for (int b = 0; b < KP * (int)sizeof(T); b += 16)
+                    cp_async(reinterpret_cast<char *>(q.val) + b, reinterpret_cast<const char *>(pval + (size_t)rr * KP) + b,
+                             16);
+                cp_async(&q.cnt, a.pcnt + rr, 4);
+                cp_async(&q.own, (a.backward ? static_cast<const T *>(z) : r) + rr, (int)sizeof(T));
+                if (need_e1) cp_async(&q.e1, d1 + rr, (int)sizeof(T));
+                if (need_e2) cp_async(&q.e2, d2 + rr, (int)sizeof(T));
+            }
+        }
+        cp_async_commit();
+    };
+    auto solve = [&](int rr, const int *cols, const T *vals, int cnt, T own, T e1, T e2, int r0, int r1) {
+        T s = T(0);
+#pragma unroll
+        for (int e = 0; e < KP; ++e) {
+            if (e < cnt) {
+                const int cc = cols[e];
+                const bool in_ring = a.backward ? cc < r0 + kRingStaged : cc >= r1 - kRingStaged;
+                s += vals[e] * (in_ring ? ring[cc & (kRingStaged - 1)] : __ldcg(z + cc));
+            }
+        }
+        T out;
+        if (!a.backward) out = a.sgs ? (-own + s) * e1 : -(-own + s);
+        else out = a.sgs ? (own * e2 + s) * e1 : (-own + s) * e1;
+        ring[rr & (kRingStaged - 1)] = out;
+        __stcg(z + rr, out);
+    };
+#pragma unroll
+    for (int k = 0; k < kStages - 1; ++k) issue(k);
+    for (int k = 0; k < nlev; ++k) {
+        issue(k + kStages - 1);
+        cp_async_wait<kStages - 1>();
+        const int l = level_of(k), r0 = s_off[l], r1 = s_off[l + 1];
+        const int rr = r0 + tid;
+        if (rr < r1) {
+            const Rec &q = stage[(k % kStages) * kLevelThreads + tid];
+            solve(rr, q.col, q.val, q.cnt, q.own, need_e1 ? q.e1 : T(0), need_e2 ? q.e2 : T(0), r0, r1);
+        }
+        // rows of a level beyond the first kLevelThreads: read directly
+        for (int r2 = rr + kLevelThreads; r2 < r1; r2 += kLevelThreads) {
+            int cols[KP];
+            T vals[KP];
+#pragma unroll
+            for (int e = 0; e < KP; ++e) {
+                cols[e] = __ldg(a.pcol + (size_t)r2 * KP + e);
+                vals[e] = __ldg(pval + (size_t)r2 * KP + e);
+            }
+            const T own = a.backward ? __ldcg(z + r2) : r[r2];
+            solve(r2, cols, vals, __ldg(a.pcnt + r2), own, need_e1 ? d1[r2] : T(0), need_e2 ? d2[r2] : T(0), r0, r1);
+        }
+        __syncthreads();
+    }
+    cp_async_wait<0>();
+}
+
+// Pack the rows of a CSR into kp fixed slots (columns, values; unused slots
+// column 0, value 0) with the entry count beside.
+template <typename T>
+__global__ void pack_rows_kernel(int n, int kp, const int *__restrict__ row, const int *__restrict__ col,
+                                 const T *__restrict__ val, int *__restrict__ pcol, T *__restrict__ pval,
+                                 int *__restrict__ pcnt)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int b = row[i], e = row[i + 1];
+        for (int k = 0; k < kp; ++k) {
+            const bool in = b + k < e;
+            pcol[(size_t)i * kp + k] = in ? col[b + k] : 0;
+            pval[(size_t)i * kp + k] = in ? val[b + k] : T(0);
+        }
+        pcnt[i] = e - b;
+    }
+}
+
+template <typename T, int KP>
+size_t staged_smem(int nlev)
+{
+    return sizeof(StageRec<T, KP>) * kStages * kLevelThreads + sizeof(T) * kRingStaged + sizeof(int) * (nlev + 1);
+}
+
 }  // namespace
 
 namespace b200 {
 
 cudaError_t sweeps_configure()
 {
-    cudaError_t e = cudaFuncSetAttribute(level_sweep_cta_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(level_sweep_staged_kernel<double, kStagedSlots>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)staged_smem<double, kStagedSlots>(kStagedMaxLevels))) ||
+        (e = cudaFuncSetAttribute(level_sweep_staged_kernel<float, kStagedSlots>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)staged_smem<float, kStagedSlots>(kStagedMaxLevels))))
+        return e;
+    e = cudaFuncSetAttribute(level_sweep_cta_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(kLevelRing * sizeof(double) + sizeof(int) * (kLevelMaxLevels + 1)));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(level_sweep_cta_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -319,6 +479,10 @@ struct SyncFreePlan {
     int lg_l = 0, lg_u = 0;
     int *lev_off = nullptr;   // single-CTA level sweep: level offsets (null: chunk tickets)
     int nlev = 0;
+    // staged variant: rows of L / U packed into kStagedSlots slots
+    int staged = 0;
+    int *pcol[2] = {nullptr, nullptr}, *pcnt[2] = {nullptr, nullptr};
+    void *pval[2] = {nullptr, nullptr};
 };
 
 static int lanes_for(const b200la_csr *M)
@@ -335,9 +499,22 @@ int syncfree_setup(b200la_ctx *ctx, b200la_precond *P)
     bool use = P->nblocks > 64;
     if (env) use = std::atoi(env) != 0;
     if (!use) return B200LA_OK;
-    // many small levels: one CTA walks them (B200LA_SWEEP=cta / tickets to force)
-    bool cta = P->nblocks > 64 && P->nblocks <= kLevelMaxLevels && P->n / std::max(P->nblocks, 1) <= 4 * kLevelThreads;
-    if (const char *sw = std::getenv("B200LA_SWEEP")) cta = std::strcmp(sw, "cta") == 0 && P->nblocks <= kLevelMaxLevels;
+    // many small levels: one CTA walks them, with the async-copy look-ahead
+    // when every row of L and U fits kStagedSlots slots (B200LA_SWEEP =
+    // staged / cta / tickets to force a variant)
+    auto maxlen = [](const b200la_csr *M) {
+        int m = 0;
+        for (int i = 0; i < M->n; ++i) m = std::max(m, M->h_row[i + 1] - M->h_row[i]);
+        return m;
+    };
+    const bool few = P->nblocks > 64 && P->n / std::max(P->nblocks, 1) <= 4 * kLevelThreads;
+    const bool can_stage = P->nblocks <= kStagedMaxLevels && maxlen(P->L) <= kStagedSlots &&
+                           maxlen(P->U) <= kStagedSlots;
+    bool cta = few && P->nblocks <= kLevelMaxLevels, staged = few && can_stage;
+    if (const char *sw = std::getenv("B200LA_SWEEP")) {
+        staged = std::strcmp(sw, "staged") == 0 && can_stage;
+        cta = (std::strcmp(sw, "cta") == 0 || std::strcmp(sw, "staged") == 0) && P->nblocks <= kLevelMaxLevels;
+    }
     if (cta) {
         SyncFreePlan *plan = new SyncFreePlan();
         plan->nlev = P->nblocks;
@@ -348,6 +525,33 @@ int syncfree_setup(b200la_ctx *ctx, b200la_precond *P)
             if (plan->lev_off) cudaFree(plan->lev_off);
             delete plan;
             return ctx_fail(ctx, B200LA_ERR_ALLOC, "level sweep setup", e);
+        }
+        if (staged) {
+            const size_t es = P->dtype == B200LA_F64 ? 8 : 4, n = (size_t)P->n;
+            for (int m = 0; m < 2 && e == cudaSuccess; ++m) {
+                const b200la_csr *M = m ? P->U : P->L;
+                if ((e = cudaMalloc(&plan->pcol[m], sizeof(int) * kStagedSlots * n)) ||
+                    (e = cudaMalloc(&plan->pval[m], es * kStagedSlots * n)) ||
+                    (e = cudaMalloc(&plan->pcnt[m], sizeof(int) * n)))
+                    break;
+                const int g = std::max(1, std::min((P->n + 255) / 256, 148 * 16));
+                if (P->dtype == B200LA_F64)
+                    pack_rows_kernel<double><<<g, 256, 0, ctx->stream>>>(P->n, kStagedSlots, M->row, M->col,
+                                                                         (const double *)M->val, plan->pcol[m],
+                                                                         (double *)plan->pval[m], plan->pcnt[m]);
+                else
+                    pack_rows_kernel<float><<<g, 256, 0, ctx->stream>>>(P->n, kStagedSlots, M->row, M->col,
+                                                                        (const float *)M->val, plan->pcol[m],
+                                                                        (float *)plan->pval[m], plan->pcnt[m]);
+                e = cudaGetLastError();
+            }
+            if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+            if (e != cudaSuccess) {
+                P->syncfree_plan = plan;
+                syncfree_free(P);
+                return ctx_fail(ctx, B200LA_ERR_ALLOC, "staged level sweep setup", e);
+            }
+            plan->staged = 1;
         }
         P->syncfree_plan = plan;
         P->use_syncfree = 1;
@@ -394,6 +598,11 @@ void syncfree_free(b200la_precond *P)
     if (plan->fwd) cudaFree(plan->fwd);
     if (plan->bwd) cudaFree(plan->bwd);
     if (plan->lev_off) cudaFree(plan->lev_off);
+    for (int m = 0; m < 2; ++m) {
+        if (plan->pcol[m]) cudaFree(plan->pcol[m]);
+        if (plan->pval[m]) cudaFree(plan->pval[m]);
+        if (plan->pcnt[m]) cudaFree(plan->pcnt[m]);
+    }
     delete plan;
     P->syncfree_plan = nullptr;
 }
@@ -401,6 +610,34 @@ void syncfree_free(b200la_precond *P)
 int syncfree_apply(b200la_ctx *ctx, const b200la_precond *P, const void *r, void *z, const int *gate)
 {
     const SyncFreePlan *plan = static_cast<const SyncFreePlan *>(P->syncfree_plan);
+    if (plan->staged) {
+        LevelStagedArgs a;
+        a.off = plan->lev_off;
+        a.nlev = plan->nlev;
+        a.n = P->n;
+        a.r = r;
+        a.z = z;
+        a.d1 = P->iDv;
+        a.d2 = P->Dv;
+        a.sgs = P->kind == B200LA_PRECOND_MCSGS;
+        a.gate = gate;
+        for (int dir = 0; dir < 2; ++dir) {
+            a.pcol = plan->pcol[dir];
+            a.pval = plan->pval[dir];
+            a.pcnt = plan->pcnt[dir];
+            a.backward = dir;
+            if (P->dtype == B200LA_F64)
+                level_sweep_staged_kernel<double, kStagedSlots>
+                    <<<1, kLevelThreads, staged_smem<double, kStagedSlots>(plan->nlev), ctx->stream>>>(a);
+            else
+                level_sweep_staged_kernel<float, kStagedSlots>
+                    <<<1, kLevelThreads, staged_smem<float, kStagedSlots>(plan->nlev), ctx->stream>>>(a);
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_CUDA, "staged level sweep", e);
+            ctx->launches += 1;
+        }
+        return B200LA_OK;
+    }
     if (plan->lev_off) {
         LevelSweepArgs a;
         a.off = plan->lev_off;

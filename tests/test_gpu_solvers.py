@@ -107,7 +107,7 @@ def test_mcsgs_pcg_vs_reference(pf, b200, golden, dim, N):
     assert np.linalg.norm(x.numpy() - xr) <= 1e-7 * np.linalg.norm(xr)
 
 
-@pytest.mark.parametrize("syncfree,sweep", [("0", "tickets"), ("1", "tickets"), ("1", "cta")])
+@pytest.mark.parametrize("syncfree,sweep", [("0", "tickets"), ("1", "tickets"), ("1", "cta"), ("1", "staged")])
 @pytest.mark.parametrize("dim,N,tag", [(2, 17, "cd"), (3, 7, "p"), (2, 8, "pk")])
 def test_ilu0_ls_apply(pf, b200, golden, dim, N, tag, syncfree, sweep, monkeypatch):
     monkeypatch.setenv("B200LA_SYNCFREE", syncfree)
@@ -137,7 +137,7 @@ def test_ilu0_mc_apply(pf, b200, golden):
     assert np.max(np.abs(z.numpy() - zr)) <= 1e-12 * np.max(np.abs(zr))
 
 
-@pytest.mark.parametrize("syncfree,sweep", [("0", "tickets"), ("1", "tickets"), ("1", "cta")])
+@pytest.mark.parametrize("syncfree,sweep", [("0", "tickets"), ("1", "tickets"), ("1", "cta"), ("1", "staged")])
 def test_gmres_ilu_ls_vs_reference(pf, b200, golden, syncfree, sweep, monkeypatch):
     monkeypatch.setenv("B200LA_SYNCFREE", syncfree)
     monkeypatch.setenv("B200LA_SWEEP", sweep)
@@ -293,7 +293,7 @@ def test_ilu0_level_sweep_beyond_ring(pf, b200, dim, N, kind, monkeypatch):
     assert n > 8192
     r = np.random.default_rng(3).uniform(-1, 1, n)
     out = {}
-    for sweep in ("tickets", "cta"):
+    for sweep in ("tickets", "cta", "staged"):
         monkeypatch.setenv("B200LA_SYNCFREE", "1")
         monkeypatch.setenv("B200LA_SWEEP", sweep)
         P = b200.Preconditioner.ILU0(pf, row, col, val, b200.PRECOND_ILU0_LS)
@@ -301,4 +301,5 @@ def test_ilu0_level_sweep_beyond_ring(pf, b200, dim, N, kind, monkeypatch):
         for _ in range(2):
             P.ApplyPreconditioner(pf.vector(r[P.perm]), z)
         out[sweep] = z.numpy()
-    assert np.max(np.abs(out["cta"] - out["tickets"])) <= 1e-11 * np.max(np.abs(out["tickets"]))
+    for sweep in ("cta", "staged"):
+        assert np.max(np.abs(out[sweep] - out["tickets"])) <= 1e-11 * np.max(np.abs(out["tickets"]))
