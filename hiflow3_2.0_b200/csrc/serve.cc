@@ -54,6 +54,7 @@ struct Req {
     std::vector<int> sell_off;        // SELL chunk offsets
     size_t bytes = 0, temp_bytes = 0; // resident / admission scratch
     double iter_bytes = 0;            // streamed by one batch iteration
+    int w1 = 1, w2 = 1;               // chunk weights of the SpMV and update kernels (bytes per row)
 };
 
 struct Slot {
@@ -186,6 +187,17 @@ int plan_request(b200la_server *S, Req *q)
                     ((!r.row && r.q1_kcell) ? al256(8 * q1_cells(r.q1_dim, r.q1_N)) : 0);
     const double ib = stencil ? 0.0 : 4.0;   // index bytes per stored entry
     q->iter_bytes = mixed ? 4.0 * q->slen32 + ib * q->slen + 48.0 * n : (8.0 + ib) * q->slen + 96.0 * n;   // vectors: 32n (SpMV) + 64n (update)
+    // per-row costs of the two kernels: operator + gathers and stores (k1),
+    // the update's vector traffic (k2); warp-per-row CSR counts double
+    const double rows = 32.0 * q->nchunks;
+    const double op = mixed ? (4.0 * q->slen32 + ib * q->slen) / rows : (8.0 + ib) * q->slen / rows;
+    const double k1 = (op + (mixed ? 16.0 : 32.0)) * (q->fmt == b200::srv::FMT_CSRW ? 2.0 : 1.0);
+    q->w1 = std::max(1, (int)std::lround(k1));
+    q->w2 = mixed ? 32 : 64;
+    // a system's weighted span stays below 2^30 (positions are int32)
+    const long long wcap = std::max<long long>(1, (1LL << 30) / std::max(q->nchunks, 1));
+    q->w1 = (int)std::min<long long>(q->w1, wcap);
+    q->w2 = (int)std::min<long long>(q->w2, wcap);
     return B200LA_OK;
 }
 
@@ -440,7 +452,7 @@ void admit_loop(b200la_server *S)
 }
 
 struct ActiveSys {
-    int idx, nchunks;
+    int idx, nchunks, w1, w2;
 };
 
 // System table of the active set: header [systems, chunks, chunks per warp range].
@@ -448,15 +460,20 @@ int write_table(b200la_server *S, const std::vector<ActiveSys> &act)
 {
     int *h = S->h_tiles;
     SysRun *tab = reinterpret_cast<SysRun *>(h + b200::srv::kTabHdrWords);
-    int nt = 0, tot = 0;
+    int nt = 0, tot = 0, W1 = 0, W2 = 0;
     for (const ActiveSys &a : act) {
-        tab[nt++] = SysRun{a.idx, tot, a.nchunks, 0};
+        tab[nt++] = SysRun{a.idx, tot, a.nchunks, a.w1, a.w2, W1, W2, 0};
         tot += a.nchunks;
+        W1 += a.nchunks * a.w1;
+        W2 += a.nchunks * a.w2;
     }
     h[0] = nt;
     h[1] = tot;
     h[2] = S->cpw;
     h[3] = 0;
+    h[4] = W1;
+    h[5] = W2;
+    h[6] = h[7] = 0;
     return nt;
 }
 
@@ -488,24 +505,25 @@ void round_loop(b200la_server *S)
             S->cv_round.wait(lk, [S] { return S->quit || !S->ready.empty() || !S->active.empty(); });
             if (S->quit && S->active.empty() && S->ready.empty()) return;
             double wb = 0.0;
-            long long chunks = 0;
+            long long wsum = 0;   // weighted chunk positions (int32 in the table)
             for (Slot *sl : S->active) {
                 wb += sl->req->iter_bytes;
-                chunks += sl->desc.nchunks;
+                wsum += (long long)sl->desc.nchunks * std::max(sl->req->w1, sl->req->w2);
             }
             while (!S->ready.empty() && (int)S->active.size() < std::min(S->max_active, kTabCap)) {
                 Slot *sl = S->ready.front();
                 const bool room = S->active.empty() || wb + sl->req->iter_bytes <= S->active_cap;
-                if (!room || chunks + sl->desc.nchunks >= (1LL << 31)) break;
+                const long long ws = (long long)sl->desc.nchunks * std::max(sl->req->w1, sl->req->w2);
+                if (!room || wsum + ws >= (1LL << 31)) break;
                 wb += sl->req->iter_bytes;
-                chunks += sl->desc.nchunks;
+                wsum += ws;
                 S->ready.pop_front();
                 S->active.push_back(sl);
             }
             S->peak_active = std::max(S->peak_active, (int)S->active.size());
             if (S->active.empty()) continue;
             act.clear();
-            for (Slot *sl : S->active) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks});
+            for (Slot *sl : S->active) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks, sl->req->w1, sl->req->w2});
         }
         const int rc = S->fatal ? S->fatal : run_round(S, act);
         std::lock_guard<std::mutex> lk(S->mu);
@@ -692,12 +710,11 @@ int autotune(b200la_server *S)
     struct Shape {
         int nw, cps, cpw;
     };
-    const Shape shapes[] = {{8, 4, 2}, {8, 4, 4}, {8, 4, 8}, {8, 4, 16}, {8, 2, 4},
-                            {4, 8, 2}, {4, 8, 4}, {4, 8, 8}, {8, 3, 4}, {8, 6, 4}};
+    const Shape shapes[] = {{8, 4, 4}, {8, 2, 4}, {8, 3, 4}, {8, 6, 4}, {4, 8, 4}, {4, 4, 4}};
     float best = 1e30f;
     Shape pick{S->nw, S->ctas_per_sm, S->cpw};
     std::vector<ActiveSys> act;
-    for (Slot *sl : slots) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks});
+    for (Slot *sl : slots) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks, sl->req->w1, sl->req->w2});
     for (const Shape &sh : shapes) {
         if (rc) break;
         S->nw = sh.nw;

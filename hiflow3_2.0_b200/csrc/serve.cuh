@@ -56,7 +56,8 @@ struct SysState {
     int status;      // B200LA_ITERATE / SUCCESS_* / FAIL_*
     int phase, maxits, in_maxits, max_outer;
     int pbuf;        // which of the two search-direction buffers holds p
-    int pad[3];
+    int corr;        // mixed: the update kernel applies x += x_low (1) or only clears x_low (2)
+    int pad[2];
 };
 
 struct SysDesc {
@@ -85,14 +86,19 @@ __host__ __device__ __forceinline__ int stencil_delta(int dim, int P, int k)
     return dim == 3 ? ((k / 9 - 1) * P + (k / 3 % 3 - 1)) * P + (k % 3 - 1) : (k / 3 - 1) * P + (k % 3 - 1);
 }
 
-// Active system: slot, first chunk in the batch's chunk sequence, chunk count.
+// Active system: slot, first chunk in the batch's chunk sequence, chunk
+// count, and per kernel (SpMV k1, update k2) the cost weight of one chunk
+// (bytes per row it streams) and the system's first position in the
+// weighted sequence (ascending).  Warps split the weighted sequence evenly,
+// so a 3-D FP64 chunk counts for about five 2-D FP32 ones.
 struct SysRun {
-    int slot, cbeg, nch, pad;
+    int slot, cbeg, nch, w1, w2, wb1, wb2, pad;
 };
 
 // System table in device memory: words [0] systems, [1] chunks in total,
-// [2] chunks per warp range; entries from word 4 (ascending cbeg).
-constexpr int kTabHdrWords = 4;
+// [2] unused, [3] unused, [4] total weight of k1, [5] total weight of k2;
+// entries from word 8.
+constexpr int kTabHdrWords = 8;
 
 // One batch iteration (SpMV kernel, update kernel) over the system table.
 // SysDesc and SysState tables are indexed by slot.

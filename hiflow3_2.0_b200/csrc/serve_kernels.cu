@@ -4,19 +4,22 @@
 //   k1  SpMV  Ap = A p_new with p_new = beta p + z formed on the fly at every
 //       gathered column (and stored for the own rows into the other of two p
 //       buffers), with the partials of p_new.Ap; on completion of a system
-//       alpha = rho / p.Ap and the p buffer flips (CG, inner CG).  Mixed
-//       systems between two inner solves apply x += (double) x_low here.
+//       alpha = rho / p.Ap and the p buffer flips (CG, inner CG).  The outer
+//       step of a mixed system runs here too: r = b - A (x + x_low) in FP64
+//       with x + x_low formed at every gathered column, r_low = (float) r,
+//       and the outer test on completion.
 //   k2  update x += alpha p, r -= alpha Ap, z = D^-1 r with the partials of
 //       r.r and r.z; on completion IterateControl::Check
-//       (src/common/iterate_control.cc:84-110) and beta, rho.  Start phases
-//       (CG: r = b; mixed: r = b - A x in FP64, r_low = (float) r) run here.
+//       (src/common/iterate_control.cc:84-110) and beta, rho.  The CG start
+//       (r = b) runs here, and after an outer step x += x_low, x_low = 0.
 // Folding the p-update of CG<LAD> (cg.cc:240-246) into the next product
 // removes a launch and a pass per iteration; the update is written with
 // explicit roundings so that every gathering thread forms the same p_new as
 // the thread that stores it.
 //
-// Work split: the active systems' 32-row chunks form one sequence; each warp
-// takes one contiguous range of it, with no CTA barrier.  A warp loads a
+// Work split: the active systems' 32-row chunks form one sequence, each
+// chunk weighted by the bytes per row the kernel streams for its system; each
+// warp takes one contiguous range of equal weight, with no CTA barrier.  A warp loads a
 // system's descriptor and state into its own shared-memory slot when its
 // range enters the system.  Reductions: one partial per chunk; a warp reports
 // its run of each system's chunks to the run's groups of 32 chunks, the warp
@@ -203,27 +206,58 @@ __device__ __forceinline__ T row_spmv(const SysDesc &d, const T *__restrict__ va
 
 // ------------------------------------------------------------------ system table
 
-constexpr int kTabSmem = 2048;   // first chunks of up to this many systems kept in shared memory
+constexpr int kTabSmem = 2048;   // weighted starts of up to this many systems kept in shared memory
 
-// First chunk of every active system into shared memory (one barrier).
-__device__ __forceinline__ void load_cbeg(const SysRun *tab, int nsys, int *s_cbeg)
+// Weighted start of every active system into shared memory (one barrier).
+template <int K>
+__device__ __forceinline__ void load_wb(const SysRun *tab, int nsys, int *s_wb)
 {
-    for (int k = threadIdx.x; k < min(nsys, kTabSmem); k += blockDim.x) s_cbeg[k] = __ldcg(&tab[k].cbeg);
+    for (int k = threadIdx.x; k < min(nsys, kTabSmem); k += blockDim.x)
+        s_wb[k] = __ldcg(K == 1 ? &tab[k].wb1 : &tab[k].wb2);
     __syncthreads();
 }
 
-// The system whose chunks contain g (binary search; shared memory when the
-// table fits).
-__device__ __forceinline__ int find_system(const SysRun *tab, int nsys, const int *s_cbeg, int g)
+// The last system whose weighted start is <= pos (binary search; shared
+// memory when the table fits).
+template <int K>
+__device__ __forceinline__ int find_system(const SysRun *tab, int nsys, const int *s_wb, int pos)
 {
     int lo = 0, hi = nsys - 1;
     while (lo < hi) {
         const int mid = (lo + hi + 1) >> 1;
-        const int cb = nsys <= kTabSmem ? s_cbeg[mid] : __ldcg(&tab[mid].cbeg);
-        if (cb <= g) lo = mid;
+        const int wb = nsys <= kTabSmem ? s_wb[mid] : __ldcg(K == 1 ? &tab[mid].wb1 : &tab[mid].wb2);
+        if (wb <= pos) lo = mid;
         else hi = mid - 1;
     }
     return lo;
+}
+
+// The chunks of a system that one warp processes: first, first + step, ...
+// below c1, out of the run [c0, c1).
+struct Run {
+    int c0, c1, first, step;
+};
+
+// The warp's share of kernel K's weighted chunk sequence: one contiguous
+// range [P0, P1) of weight W / warps.  Chunk c of a system belongs to the
+// warp whose range holds the chunk's start wb + c w, so every chunk has one
+// owner.  body(slot, run) runs once per system the range touches.
+template <int K, int NW, typename F>
+__device__ __forceinline__ void for_warp_runs(const int *__restrict__ tb, const SysRun *tab, int nsys,
+                                              const int *s_wb, F body)
+{
+    const long long W = __ldcg(tb + 3 + K);
+    const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nw = gridDim.x * NW;
+    const int P0 = (int)((long long)gw * W / nw), P1 = (int)((long long)(gw + 1) * W / nw);
+    if (P0 >= P1 || nsys <= 0) return;
+    for (int si = find_system<K>(tab, nsys, s_wb, P0); si < nsys; ++si) {
+        const int wb = nsys <= kTabSmem ? s_wb[si] : __ldcg(K == 1 ? &tab[si].wb1 : &tab[si].wb2);
+        if (wb >= P1) break;
+        const int wt = __ldcg(K == 1 ? &tab[si].w1 : &tab[si].w2), nch = __ldcg(&tab[si].nch);
+        const int c0 = P0 > wb ? (P0 - wb + wt - 1) / wt : 0;
+        const int c1 = min(nch, (P1 - wb + wt - 1) / wt);
+        if (c0 < c1) body(__ldcg(&tab[si].slot), Run{c0, c1, c0, 1});
+    }
 }
 
 // ------------------------------------------------------------------ reporting
@@ -233,18 +267,22 @@ __device__ __forceinline__ int find_system(const SysRun *tab, int nsys, const in
 // summed; the completion of the last group runs fin(o) on the warp (o valid
 // on every lane).  NQ quantities.
 template <int NQ, typename F>
-__device__ __forceinline__ void report(const WarpCtx &c, int c0, int c1, F fin)
+__device__ __forceinline__ void report(const WarpCtx &c, const Run &R, F fin)
 {
     const int lane = threadIdx.x & 31;
     const SysDesc &d = c.d;
     if (lane == 0) __threadfence();
-    for (int g = c0 / kGroup; g * kGroup < c1; ++g) {
-        const int a = max(c0, g * kGroup), b = min(c1, (g + 1) * kGroup);
+    for (int g = R.first / kGroup; g * kGroup < R.c1; ++g) {
+        // the warp's chunks in group g: first + k step within [a, b)
+        const int a = max(R.first, g * kGroup), b = min(R.c1, (g + 1) * kGroup);
+        const int f = a + (R.first - a % R.step + R.step) % R.step;   // first chunk >= a of the residue
+        const int cnt = f < b ? (b - f + R.step - 1) / R.step : 0;
+        if (cnt == 0) continue;
         const int gsize = min(d.nchunks, (g + 1) * kGroup) - g * kGroup;
         int done = 0;
         if (lane == 0) {
-            const unsigned old = atomicAdd(d.gcnt + g, (unsigned)(b - a));
-            done = old + (unsigned)(b - a) == (unsigned)gsize;
+            const unsigned old = atomicAdd(d.gcnt + g, (unsigned)cnt);
+            done = old + (unsigned)cnt == (unsigned)gsize;
         }
         done = __shfl_sync(0xffffffffu, done, 0);
         if (!done) continue;
@@ -284,7 +322,7 @@ __device__ __forceinline__ void report(const WarpCtx &c, int c0, int c1, F fin)
 // ------------------------------------------------------------------ k1
 
 template <typename T>
-__device__ __forceinline__ void k1_range(const WarpCtx &c, SysState *st, int c0, int c1, uint64_t pol)
+__device__ __forceinline__ void k1_range(const WarpCtx &c, SysState *st, const Run R, uint64_t pol)
 {
     const int lane = threadIdx.x & 31;
     const SysDesc &d = c.d;
@@ -297,9 +335,8 @@ __device__ __forceinline__ void k1_range(const WarpCtx &c, SysState *st, int c0,
     T *ap = static_cast<T *>(d.ap);
     const T *val = sizeof(T) == 8 ? reinterpret_cast<const T *>(d.val64) : reinterpret_cast<const T *>(d.val32);
     auto gather = [=](int j) { return pnew_at(beta, po, z, j); };
-    for (int ch = c0; ch < c1; ++ch) {
+    auto finish_row = [&](int ch, T s) {
         const int i = ch * kChunk + lane;
-        const T s = row_spmv<T>(d, val, ch, lane, pol, gather);
         double dp = 0.0;
         if (i < n) {
             const T pi = pnew_at(beta, po, z, i);
@@ -307,28 +344,107 @@ __device__ __forceinline__ void k1_range(const WarpCtx &c, SysState *st, int c0,
             ap[i] = s;
             dp = (double)(pi * s);
         }
-        dp = warp_sum(dp);
+        return dp;
+    };
+    int ch = R.first;
+    if (sizeof(T) == 4 && d.fmt == FMT_STENCIL && d.sdim == 2) {
+        // FP32 2-D stencil rows stream few bytes per chunk: two chunks per
+        // step keep twice the loads in flight
+        for (; ch + R.step < R.c1; ch += 2 * R.step) {
+            const int chb = ch + R.step;
+            const T sa = stencil_row<3>(val, ch, lane, n, d.sP, pol, gather);
+            const T sb = stencil_row<3>(val, chb, lane, n, d.sP, pol, gather);
+            double da = finish_row(ch, sa), db = finish_row(chb, sb);
+            da = warp_sum(da);
+            db = warp_sum(db);
+            if (lane == 0) {
+                d.part[ch] = da;
+                d.part[chb] = db;
+            }
+        }
+    }
+    for (; ch < R.c1; ch += R.step) {
+        const double dp = warp_sum(finish_row(ch, row_spmv<T>(d, val, ch, lane, pol, gather)));
         if (lane == 0) d.part[ch] = dp;
     }
     const double rho = c.s.rho;
     const int pbuf = c.s.pbuf;
-    report<1>(c, c0, c1, [&](const double *o) {
+    report<1>(c, R, [&](const double *o) {
         if (lane == 0) {
             st->alpha = rho / o[0];
             st->pbuf = pbuf ^ 1;
+            st->corr = 0;
         }
     });
 }
 
-__device__ __forceinline__ void k1_correct(const WarpCtx &c, int c0, int c1)
+// x + (double) x_low as the outer correction forms it, everywhere the same
+// (a zero correction leaves x untouched)
+__device__ __forceinline__ double xcorr(double x, float xl) { return xl == 0.0f ? x : __dadd_rn(x, (double)xl); }
+
+__device__ void k2_finish(const SysState &cs, SysState *st, int *done, int ph, const double *o);
+
+// Outer step of a mixed system (mpir.cc:125-128, 271-273, 308-326): the FP64
+// residual of the corrected iterate, its FP32 copy and D^-1 r_low, the norms
+// for the outer and first inner tests.  x itself is corrected by the update
+// kernel, after every gather of this launch.  Out of line: runs once per
+// outer step.
+__device__ __noinline__ void k1_outer(const WarpCtx &c, SysState *st, const Run R, uint64_t pol)
 {
     const int lane = threadIdx.x & 31;
-    const int n = c.d.n;
-    double *x = c.d.x;
-    const float *xl = static_cast<const float *>(c.d.xl);
-    for (int ch = c0; ch < c1; ++ch) {
+    const SysDesc &d = c.d;
+    const int n = d.n, ps = d.pstride;
+    const double *b = d.b, *x = d.x;
+    const float *xl = static_cast<const float *>(d.xl);
+    float *rl = static_cast<float *>(d.r), *zl = static_cast<float *>(d.z);
+    const float *dv = static_cast<const float *>(d.invd);
+    auto gather = [=](int j) { return xcorr(__ldg(x + j), __ldg(xl + j)); };
+    for (int ch = R.first; ch < R.c1; ch += R.step) {
         const int i = ch * kChunk + lane;
-        if (i < n) x[i] += (double)xl[i];
+        const double s = row_spmv<double>(d, d.val64, ch, lane, pol, gather);
+        double q0 = 0.0, q1 = 0.0, q2 = 0.0;
+        if (i < n) {
+            const double r = b[i] - s;
+            const float f = (float)r;
+            const float zf = zmul(f, dv[i]);
+            rl[i] = f;
+            zl[i] = zf;
+            q0 = r * r;
+            q1 = (double)(f * zf);
+            q2 = (double)(f * f);
+        }
+        q0 = warp_sum(q0);
+        q1 = warp_sum(q1);
+        q2 = warp_sum(q2);
+        if (lane == 0) {
+            d.part[ch] = q0;
+            d.part[ps + ch] = q1;
+            d.part[2 * ps + ch] = q2;
+        }
+    }
+    const SysState cs = c.s;
+    const int ph = cs.phase;
+    report<3>(c, R, [&](const double *o) {
+        if (lane == 0) {
+            k2_finish(cs, st, d.done, ph, o);
+            st->corr = ph == PH_CORRECT ? 1 : 2;
+        }
+    });
+}
+
+// After an outer step: x += (double) x_low (corr 1), x_low = 0.
+__device__ __forceinline__ void k2_corr(const WarpCtx &c, const Run R)
+{
+    const int lane = threadIdx.x & 31;
+    const int n = c.d.n, corr = c.s.corr;
+    double *x = c.d.x;
+    float *xl = static_cast<float *>(c.d.xl);
+    for (int ch = R.first; ch < R.c1; ch += R.step) {
+        const int i = ch * kChunk + lane;
+        if (i < n) {
+            if (corr == 1) x[i] = xcorr(x[i], xl[i]);
+            xl[i] = 0.0f;
+        }
     }
 }
 
@@ -337,42 +453,26 @@ __global__ void __launch_bounds__(NW * 32, kMinCta256 * 8 / NW) k1_kernel(const 
                                                                        SysState *state, const int *__restrict__ tb)
 {
     __shared__ WarpCtx ctx[NW];
-    __shared__ int s_cbeg[kTabSmem];
+    __shared__ int s_wb[kTabSmem];
     WarpCtx &c = ctx[threadIdx.x >> 5];
-    const int nsys = __ldcg(tb), T = __ldcg(tb + 1), C = __ldcg(tb + 2);
+    const int nsys = __ldcg(tb);
     const SysRun *tab = reinterpret_cast<const SysRun *>(tb + kTabHdrWords);
-    load_cbeg(tab, nsys, s_cbeg);
+    load_wb<1>(tab, nsys, s_wb);
     const uint64_t pol = l2_policy(0);
-    const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nw = gridDim.x * NW;
-    (void)C;
-    // one contiguous range of the chunk sequence per warp: runs within a
-    // system are long, so a warp reports about once per system it touches
-    const int g0 = (int)((long long)gw * T / nw), g1 = (int)((long long)(gw + 1) * T / nw);
-    int si = 0, loaded = -1;
-    if (g0 < g1) {
-        si = find_system(tab, nsys, s_cbeg, g0);
-        for (int g = g0; g < g1;) {
-            const int slot = __ldcg(&tab[si].slot), cb = __ldcg(&tab[si].cbeg), nch = __ldcg(&tab[si].nch);
-            const int e = min(g1, cb + nch);
-            if (slot != loaded) {
-                warp_load(sys, state, slot, c);
-                loaded = slot;
-            }
-            const int ph = c.s.phase, c0 = g - cb, c1 = e - cb;
-            if (ph == PH_CG) k1_range<double>(c, state + slot, c0, c1, pol);
-            else if (ph == PH_INNER) k1_range<float>(c, state + slot, c0, c1, pol);
-            else if (ph == PH_CORRECT) k1_correct(c, c0, c1);
-            g = e;
-            if (g < g1) ++si;
-        }
-    }
+    for_warp_runs<1, NW>(tb, tab, nsys, s_wb, [&](int slot, const Run R) {
+        warp_load(sys, state, slot, c);
+        const int ph = c.s.phase;
+        if (ph == PH_CG) k1_range<double>(c, state + slot, R, pol);
+        else if (ph == PH_INNER) k1_range<float>(c, state + slot, R, pol);
+        else if (ph == PH_OUTER || ph == PH_CORRECT) k1_outer(c, state + slot, R, pol);
+    });
 }
 
 // ------------------------------------------------------------------ k2
 
 // Lane 0 of the completing warp.  cs: the state as read before this launch
 // changed it (nothing else writes it during the launch).
-__device__ __forceinline__ void k2_finish(const SysState &cs, SysState *st, int *done, int ph, const double *o)
+__device__ void k2_finish(const SysState &cs, SysState *st, int *done, int ph, const double *o)
 {
     if (ph == PH_CG) {
         // cg.cc:222-247 with IterateControl::Check on ||r||
@@ -443,7 +543,7 @@ __device__ __forceinline__ void k2_finish(const SysState &cs, SysState *st, int 
 }
 
 template <typename T>
-__device__ __forceinline__ void k2_update(const WarpCtx &c, SysState *st, int c0, int c1)
+__device__ __forceinline__ void k2_update(const WarpCtx &c, SysState *st, const Run R)
 {
     const int lane = threadIdx.x & 31;
     const SysDesc &d = c.d;
@@ -453,41 +553,72 @@ __device__ __forceinline__ void k2_update(const WarpCtx &c, SysState *st, int c0
     T *r = static_cast<T *>(d.r), *z = static_cast<T *>(d.z);
     const T *p = static_cast<const T *>(c.s.pbuf == 0 ? d.p0 : d.p1);
     const T *ap = static_cast<const T *>(d.ap), *dv = static_cast<const T *>(d.invd);
-    for (int ch = c0; ch < c1; ++ch) {
-        const int i = ch * kChunk + lane;
-        double rr = 0.0, rz = 0.0;
-        if (i < n) {
-            const T xi = x[i] + alpha * p[i];
-            const T ri = r[i] - alpha * __ldcs(ap + i);
-            const T zi = zmul(ri, dv[i]);
-            x[i] = xi;
-            r[i] = ri;
-            z[i] = zi;
-            rr = (double)(ri * ri);
-            rz = (double)(ri * zi);
+    // two chunks per step: the loads of both are in flight together
+    for (int ch = R.first; ch < R.c1; ch += 2 * R.step) {
+        const int chb = ch + R.step;
+        const int ia = ch * kChunk + lane, ib = chb * kChunk + lane;
+        const bool va = ia < n, vb = chb < R.c1 && ib < n;
+        T xa = T(0), pa = T(0), ra = T(0), aa = T(0), da = T(0);
+        T xb = T(0), pb = T(0), rb = T(0), ab = T(0), db = T(0);
+        if (va) {
+            xa = x[ia];
+            pa = p[ia];
+            ra = r[ia];
+            aa = __ldcs(ap + ia);
+            da = dv[ia];
         }
-        rr = warp_sum(rr);
-        rz = warp_sum(rz);
+        if (vb) {
+            xb = x[ib];
+            pb = p[ib];
+            rb = r[ib];
+            ab = __ldcs(ap + ib);
+            db = dv[ib];
+        }
+        double rra = 0.0, rza = 0.0, rrb = 0.0, rzb = 0.0;
+        if (va) {
+            const T ri = ra - alpha * aa, zi = zmul(ri, da);
+            x[ia] = xa + alpha * pa;
+            r[ia] = ri;
+            z[ia] = zi;
+            rra = (double)(ri * ri);
+            rza = (double)(ri * zi);
+        }
+        if (vb) {
+            const T ri = rb - alpha * ab, zi = zmul(ri, db);
+            x[ib] = xb + alpha * pb;
+            r[ib] = ri;
+            z[ib] = zi;
+            rrb = (double)(ri * ri);
+            rzb = (double)(ri * zi);
+        }
+        rra = warp_sum(rra);
+        rza = warp_sum(rza);
+        rrb = warp_sum(rrb);
+        rzb = warp_sum(rzb);
         if (lane == 0) {
-            d.part[ch] = rr;
-            d.part[ps + ch] = rz;
+            d.part[ch] = rra;
+            d.part[ps + ch] = rza;
+            if (chb < R.c1) {
+                d.part[chb] = rrb;
+                d.part[ps + chb] = rzb;
+            }
         }
     }
     const SysState cs = c.s;
     const int ph = cs.phase;
-    report<2>(c, c0, c1, [&](const double *o) {
+    report<2>(c, R, [&](const double *o) {
         if (lane == 0) k2_finish(cs, st, d.done, ph, o);
     });
 }
 
-__device__ __forceinline__ void k2_start(const WarpCtx &c, SysState *st, int c0, int c1)
+__device__ __forceinline__ void k2_start(const WarpCtx &c, SysState *st, const Run R)
 {
     const int lane = threadIdx.x & 31;
     const SysDesc &d = c.d;
     const int n = d.n, ps = d.pstride;
     double *r = static_cast<double *>(d.r), *z = static_cast<double *>(d.z);
     const double *b = d.b, *dv = static_cast<const double *>(d.invd);
-    for (int ch = c0; ch < c1; ++ch) {
+    for (int ch = R.first; ch < R.c1; ch += R.step) {
         const int i = ch * kChunk + lane;
         double rr = 0.0, rz = 0.0;
         if (i < n) {
@@ -506,50 +637,8 @@ __device__ __forceinline__ void k2_start(const WarpCtx &c, SysState *st, int c0,
         }
     }
     const SysState cs = c.s;
-    report<2>(c, c0, c1, [&](const double *o) {
+    report<2>(c, R, [&](const double *o) {
         if (lane == 0) k2_finish(cs, st, d.done, PH_CG_START, o);
-    });
-}
-
-// Runs once per outer step of a mixed system: kept out of line so that its
-// registers do not constrain the per-iteration update.
-__device__ __noinline__ void k2_outer(const WarpCtx &c, SysState *st, int c0, int c1, uint64_t pol)
-{
-    const int lane = threadIdx.x & 31;
-    const SysDesc &d = c.d;
-    const int n = d.n, ps = d.pstride;
-    const double *b = d.b, *x = d.x;
-    float *rl = static_cast<float *>(d.r), *zl = static_cast<float *>(d.z), *xl = static_cast<float *>(d.xl);
-    const float *dv = static_cast<const float *>(d.invd);
-    auto gather = [=](int j) { return __ldg(x + j); };
-    for (int ch = c0; ch < c1; ++ch) {
-        const int i = ch * kChunk + lane;
-        const double s = row_spmv<double>(d, d.val64, ch, lane, pol, gather);
-        double q0 = 0.0, q1 = 0.0, q2 = 0.0;
-        if (i < n) {
-            const double r = b[i] - s;
-            const float f = (float)r;
-            const float zf = zmul(f, dv[i]);
-            rl[i] = f;
-            zl[i] = zf;
-            xl[i] = 0.0f;
-            q0 = r * r;
-            q1 = (double)(f * zf);
-            q2 = (double)(f * f);
-        }
-        q0 = warp_sum(q0);
-        q1 = warp_sum(q1);
-        q2 = warp_sum(q2);
-        if (lane == 0) {
-            d.part[ch] = q0;
-            d.part[ps + ch] = q1;
-            d.part[2 * ps + ch] = q2;
-        }
-    }
-    const SysState cs = c.s;
-    const int ph = cs.phase;
-    report<3>(c, c0, c1, [&](const double *o) {
-        if (lane == 0) k2_finish(cs, st, d.done, ph, o);
     });
 }
 
@@ -558,37 +647,20 @@ __global__ void __launch_bounds__(NW * 32, kMinCta256 * 8 / NW) k2_kernel(const 
                                                                        SysState *state, const int *__restrict__ tb)
 {
     __shared__ WarpCtx ctx[NW];
-    __shared__ int s_cbeg[kTabSmem];
+    __shared__ int s_wb[kTabSmem];
     WarpCtx &c = ctx[threadIdx.x >> 5];
-    const int nsys = __ldcg(tb), T = __ldcg(tb + 1), C = __ldcg(tb + 2);
+    const int nsys = __ldcg(tb);
     const SysRun *tab = reinterpret_cast<const SysRun *>(tb + kTabHdrWords);
-    load_cbeg(tab, nsys, s_cbeg);
-    const uint64_t pol = l2_policy(0);
-    const int gw = blockIdx.x * NW + (threadIdx.x >> 5), nw = gridDim.x * NW;
-    (void)C;
-    // one contiguous range of the chunk sequence per warp: runs within a
-    // system are long, so a warp reports about once per system it touches
-    const int g0 = (int)((long long)gw * T / nw), g1 = (int)((long long)(gw + 1) * T / nw);
-    int si = 0, loaded = -1;
-    if (g0 < g1) {
-        si = find_system(tab, nsys, s_cbeg, g0);
-        for (int g = g0; g < g1;) {
-            const int slot = __ldcg(&tab[si].slot), cb = __ldcg(&tab[si].cbeg), nch = __ldcg(&tab[si].nch);
-            const int e = min(g1, cb + nch);
-            if (slot != loaded) {
-                warp_load(sys, state, slot, c);
-                loaded = slot;
-            }
-            const int ph = c.s.phase, c0 = g - cb, c1 = e - cb;
-            SysState *st = state + slot;
-            if (ph == PH_CG) k2_update<double>(c, st, c0, c1);
-            else if (ph == PH_INNER) k2_update<float>(c, st, c0, c1);
-            else if (ph == PH_CG_START) k2_start(c, st, c0, c1);
-            else if (ph == PH_OUTER || ph == PH_CORRECT) k2_outer(c, st, c0, c1, pol);
-            g = e;
-            if (g < g1) ++si;
-        }
-    }
+    load_wb<2>(tab, nsys, s_wb);
+    for_warp_runs<2, NW>(tb, tab, nsys, s_wb, [&](int slot, const Run R) {
+        warp_load(sys, state, slot, c);
+        const int ph = c.s.phase;
+        SysState *st = state + slot;
+        if (c.s.corr) k2_corr(c, R);   // the outer step ran in k1 (the phase is already the next one)
+        else if (ph == PH_CG) k2_update<double>(c, st, R);
+        else if (ph == PH_INNER) k2_update<float>(c, st, R);
+        else if (ph == PH_CG_START) k2_start(c, st, R);
+    });
 }
 
 // ------------------------------------------------------------ slot build
