@@ -39,6 +39,12 @@ using b200::srv::SysState;
 namespace {
 
 constexpr int kTabCap = 1 << 16;    // systems one round may list
+// The active set is split into lanes (3 by default, B200LA_SERVE_LANES from 1
+// to kLanes), each with its own system table and its own chain of kernels in
+// the round's graph: the chains run concurrently, so one lane's kernel tails
+// and reduction chains overlap another lane's streaming.
+constexpr int kLanes = 4;
+constexpr size_t kTabWords = b200::srv::kTabHdrWords + sizeof(SysRun) / sizeof(int) * (size_t)kTabCap;
 
 size_t al256(size_t b) { return (b + 255) & ~size_t(255); }
 
@@ -82,8 +88,9 @@ struct b200la_server {
     int device = 0, num_sms = 148;
     std::chrono::steady_clock::time_point t0;
     cudaMemPool_t pool = nullptr;
-    cudaStream_t s_comp = nullptr, s_copy = nullptr;
-    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    cudaStream_t s_comp = nullptr, s_copy = nullptr, s_lane[kLanes] = {};   // s_lane[0] unused (lane 0: s_comp)
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_fork = nullptr, ev_join[kLanes] = {};
+    int lanes = 3, lane_nt[kLanes] = {};
     SysDesc *d_sys = nullptr;
     SysState *d_state = nullptr;
     unsigned *d_ticket = nullptr;
@@ -92,7 +99,7 @@ struct b200la_server {
     cudaGraphExec_t graph = nullptr;
     // kernel shape
     int nw = 8, ctas_per_sm = 4, cpw = 4, iters = 16;
-    double active_cap = 512.0 * 1024 * 1024;
+    double active_cap = 4096.0 * 1024 * 1024;
     int max_active = 1024;
 
     std::mutex mu;
@@ -453,37 +460,61 @@ void admit_loop(b200la_server *S)
 
 struct ActiveSys {
     int idx, nchunks, w1, w2;
+    double ib;   // bytes streamed per batch iteration
 };
 
 // System table of the active set: header [systems, chunks, chunks per warp range].
+// The lanes' system tables (host side): each system goes to the lane with
+// the fewest bytes per batch iteration so far, in arrival order.
 int write_table(b200la_server *S, const std::vector<ActiveSys> &act)
 {
-    int *h = S->h_tiles;
-    SysRun *tab = reinterpret_cast<SysRun *>(h + b200::srv::kTabHdrWords);
-    int nt = 0, tot = 0, W1 = 0, W2 = 0;
+    double load[kLanes] = {};
+    int nt[kLanes] = {}, tot[kLanes] = {}, W1[kLanes] = {}, W2[kLanes] = {};
     for (const ActiveSys &a : act) {
-        tab[nt++] = SysRun{a.idx, tot, a.nchunks, a.w1, a.w2, W1, W2, 0};
-        tot += a.nchunks;
-        W1 += a.nchunks * a.w1;
-        W2 += a.nchunks * a.w2;
+        int l = 0;
+        for (int k = 1; k < S->lanes; ++k)
+            if (load[k] < load[l]) l = k;
+        load[l] += a.ib;
+        SysRun *tab = reinterpret_cast<SysRun *>(S->h_tiles + (size_t)l * kTabWords + b200::srv::kTabHdrWords);
+        tab[nt[l]++] = SysRun{a.idx, tot[l], a.nchunks, a.w1, a.w2, W1[l], W2[l], 0};
+        tot[l] += a.nchunks;
+        W1[l] += a.nchunks * a.w1;
+        W2[l] += a.nchunks * a.w2;
     }
-    h[0] = nt;
-    h[1] = tot;
-    h[2] = S->cpw;
-    h[3] = 0;
-    h[4] = W1;
-    h[5] = W2;
-    h[6] = h[7] = 0;
-    return nt;
+    int all = 0;
+    for (int l = 0; l < S->lanes; ++l) {
+        int *h = S->h_tiles + (size_t)l * kTabWords;
+        h[0] = nt[l];
+        h[1] = tot[l];
+        h[2] = S->cpw;
+        h[3] = 0;
+        h[4] = W1[l];
+        h[5] = W2[l];
+        h[6] = h[7] = 0;
+        S->lane_nt[l] = nt[l];
+        all += nt[l];
+    }
+    return all;
+}
+
+// Copy the used part of every lane's table to the device.
+cudaError_t upload_tables(b200la_server *S, cudaStream_t st)
+{
+    for (int l = 0; l < S->lanes; ++l) {
+        const size_t off = (size_t)l * kTabWords;
+        const cudaError_t e = cudaMemcpyAsync(S->d_tiles + off, S->h_tiles + off,
+                                              sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * (size_t)S->lane_nt[l],
+                                              cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 int run_round(b200la_server *S, const std::vector<ActiveSys> &act)
 {
-    const int nt = write_table(S, act);
-    int *h = S->h_tiles;
+    write_table(S, act);
     cudaStream_t st = S->s_comp;
-    SV(cudaMemcpyAsync(S->d_tiles, h, sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * (size_t)nt,
-                       cudaMemcpyHostToDevice, st));
+    SV(upload_tables(S, st));
     SV(cudaEventRecord(S->ev_a, st));
     SV(cudaGraphLaunch(S->graph, st));
     SV(cudaEventRecord(S->ev_b, st));
@@ -523,7 +554,8 @@ void round_loop(b200la_server *S)
             S->peak_active = std::max(S->peak_active, (int)S->active.size());
             if (S->active.empty()) continue;
             act.clear();
-            for (Slot *sl : S->active) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks, sl->req->w1, sl->req->w2});
+            for (Slot *sl : S->active)
+                act.push_back(ActiveSys{sl->idx, sl->desc.nchunks, sl->req->w1, sl->req->w2, sl->req->iter_bytes});
         }
         const int rc = S->fatal ? S->fatal : run_round(S, act);
         std::lock_guard<std::mutex> lk(S->mu);
@@ -663,9 +695,17 @@ int capture_graph(b200la_server *S)
     const int grid = S->num_sms * S->ctas_per_sm;
     cudaGraph_t g = nullptr;
     SV(cudaStreamBeginCapture(S->s_comp, cudaStreamCaptureModeThreadLocal));
-    cudaError_t e = cudaSuccess;
+    // lane 0 on the capture stream, the others forked onto their own streams
+    cudaError_t e = S->lanes > 1 ? cudaEventRecord(S->ev_fork, S->s_comp) : cudaSuccess;
+    for (int l = 1; l < S->lanes && e == cudaSuccess; ++l) e = cudaStreamWaitEvent(S->s_lane[l], S->ev_fork, 0);
     for (int k = 0; k < S->iters && e == cudaSuccess; ++k)
-        e = b200::srv::launch_round(S->nw, grid, S->d_sys, S->d_state, S->d_tiles, S->s_comp);
+        for (int l = 0; l < S->lanes && e == cudaSuccess; ++l)
+            e = b200::srv::launch_round(S->nw, grid, S->d_sys, S->d_state, S->d_tiles + (size_t)l * kTabWords,
+                                        l ? S->s_lane[l] : S->s_comp);
+    for (int l = 1; l < S->lanes && e == cudaSuccess; ++l) {
+        e = cudaEventRecord(S->ev_join[l], S->s_lane[l]);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(S->s_comp, S->ev_join[l], 0);
+    }
     const cudaError_t e2 = cudaStreamEndCapture(S->s_comp, &g);
     if (e != cudaSuccess) return -(int)e;
     if (e2 != cudaSuccess) return -(int)e2;
@@ -714,25 +754,29 @@ int autotune(b200la_server *S)
     float best = 1e30f;
     Shape pick{S->nw, S->ctas_per_sm, S->cpw};
     std::vector<ActiveSys> act;
-    for (Slot *sl : slots) act.push_back(ActiveSys{sl->idx, sl->desc.nchunks, sl->req->w1, sl->req->w2});
+    for (Slot *sl : slots)
+        act.push_back(ActiveSys{sl->idx, sl->desc.nchunks, sl->req->w1, sl->req->w2, sl->req->iter_bytes});
     for (const Shape &sh : shapes) {
         if (rc) break;
         S->nw = sh.nw;
         S->ctas_per_sm = sh.cps;
         S->cpw = sh.cpw;
-        const int nt = write_table(S, act);
+        write_table(S, act);
         cudaStream_t st = S->s_comp;
-        if (cudaMemcpyAsync(S->d_tiles, S->h_tiles, sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * (size_t)nt,
-                            cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        if (upload_tables(S, st) != cudaSuccess) {
             rc = -1;
             break;
         }
         const int grid = S->num_sms * sh.cps;
-        for (int k = 0; k < 3 && !rc; ++k)
-            if (b200::srv::launch_round(sh.nw, grid, S->d_sys, S->d_state, S->d_tiles, st) != cudaSuccess) rc = -1;
+        auto iter = [&] {
+            for (int l = 0; l < S->lanes && !rc; ++l)
+                if (b200::srv::launch_round(sh.nw, grid, S->d_sys, S->d_state, S->d_tiles + (size_t)l * kTabWords, st) !=
+                    cudaSuccess)
+                    rc = -1;
+        };
+        for (int k = 0; k < 3 && !rc; ++k) iter();
         cudaEventRecord(S->ev_a, st);
-        for (int k = 0; k < 12 && !rc; ++k)
-            if (b200::srv::launch_round(sh.nw, grid, S->d_sys, S->d_state, S->d_tiles, st) != cudaSuccess) rc = -1;
+        for (int k = 0; k < 12 && !rc; ++k) iter();
         cudaEventRecord(S->ev_b, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
         float ms = 0.f;
@@ -768,6 +812,11 @@ void destroy_server(b200la_server *S)
     cudaFreeHost(S->h_tiles);
     if (S->ev_a) cudaEventDestroy(S->ev_a);
     if (S->ev_b) cudaEventDestroy(S->ev_b);
+    if (S->ev_fork) cudaEventDestroy(S->ev_fork);
+    for (int l = 1; l < kLanes; ++l) {
+        if (S->ev_join[l]) cudaEventDestroy(S->ev_join[l]);
+        if (S->s_lane[l]) cudaStreamDestroy(S->s_lane[l]);
+    }
     if (S->s_comp) cudaStreamDestroy(S->s_comp);
     if (S->s_copy) cudaStreamDestroy(S->s_copy);
     if (S->pool) cudaMemPoolDestroy(S->pool);
@@ -789,7 +838,7 @@ extern "C" int b200la_serve_start(const b200la_serve_config *cfg, b200la_server 
     if (c.max_slots <= 0) c.max_slots = 4096;
     if (c.max_active <= 0) c.max_active = 1024;
     if (c.iters_per_round <= 0) c.iters_per_round = 16;
-    if (c.active_bytes <= 0) c.active_bytes = 512.0 * 1024 * 1024;
+    if (c.active_bytes <= 0) c.active_bytes = 4096.0 * 1024 * 1024;
     S->device = c.device;
     S->iters = c.iters_per_round;
     S->active_cap = c.active_bytes;
@@ -814,19 +863,24 @@ extern "C" int b200la_serve_start(const b200la_serve_config *cfg, b200la_server 
         uint64_t keep = ~0ULL;
         ok = cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess;
     }
+    if (const char *ln = std::getenv("B200LA_SERVE_LANES")) S->lanes = std::max(1, std::min(kLanes, std::atoi(ln)));
     ok = ok && cudaStreamCreateWithFlags(&S->s_comp, cudaStreamNonBlocking) == cudaSuccess &&
          cudaStreamCreateWithFlags(&S->s_copy, cudaStreamNonBlocking) == cudaSuccess &&
-         cudaEventCreate(&S->ev_a) == cudaSuccess && cudaEventCreate(&S->ev_b) == cudaSuccess;
+         cudaEventCreate(&S->ev_a) == cudaSuccess && cudaEventCreate(&S->ev_b) == cudaSuccess &&
+         cudaEventCreateWithFlags(&S->ev_fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int l = 1; l < kLanes; ++l)
+        ok = ok && cudaStreamCreateWithFlags(&S->s_lane[l], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&S->ev_join[l], cudaEventDisableTiming) == cudaSuccess;
     const size_t ms = (size_t)c.max_slots;
     ok = ok && cudaMalloc(&S->d_sys, sizeof(SysDesc) * ms) == cudaSuccess &&
          cudaMalloc(&S->d_state, sizeof(SysState) * ms) == cudaSuccess &&
          cudaMalloc(&S->d_ticket, sizeof(unsigned) * b200::srv::kTicketWords * ms) == cudaSuccess &&
          cudaMalloc(&S->d_done, sizeof(int) * ms) == cudaSuccess &&
-         cudaMalloc(&S->d_tiles, sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * kTabCap) == cudaSuccess &&
+         cudaMalloc(&S->d_tiles, sizeof(int) * kTabWords * kLanes) == cudaSuccess &&
          cudaMallocHost(&S->h_done, sizeof(int) * ms) == cudaSuccess &&
-         cudaMallocHost(&S->h_tiles, sizeof(int) * b200::srv::kTabHdrWords + sizeof(SysRun) * kTabCap) == cudaSuccess;
+         cudaMallocHost(&S->h_tiles, sizeof(int) * kTabWords * kLanes) == cudaSuccess;
     ok = ok && cudaMemset(S->d_done, 0, sizeof(int) * ms) == cudaSuccess &&
-         cudaMemset(S->d_tiles, 0, sizeof(int) * b200::srv::kTabHdrWords) == cudaSuccess &&
+         cudaMemset(S->d_tiles, 0, sizeof(int) * kTabWords * kLanes) == cudaSuccess &&
          cudaMemset(S->d_sys, 0, sizeof(SysDesc) * ms) == cudaSuccess;
     if (!ok) {
         destroy_server(S);

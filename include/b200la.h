@@ -298,7 +298,7 @@ typedef struct {
     int device;
     double budget_bytes;     /* device bytes resident requests may hold (0: 60e9) */
     int max_slots;           /* resident requests at most (0: 4096) */
-    double active_bytes;     /* bytes one batch iteration may stream (0: 512 MiB) */
+    double active_bytes;     /* bytes one batch iteration may stream (0: 4 GiB) */
     int max_active;          /* requests iterated together at most (0: 1024) */
     int iters_per_round;     /* batch iterations per graph replay (0: 16) */
     int autotune;            /* 1: time the kernel shapes on a calibration batch at start */
