@@ -511,7 +511,7 @@ def other_configs(b200, pf, wl):
     return out
 
 
-def serving_bench(b200, pf, nreq, sample=64, seed=2025, rank=0, world=1, dist=None):
+def serving_bench(b200, pf, nreq, sample=128, seed=2025, rank=0, world=1, dist=None):
     """The serving loop on the seeded request stream: saturation throughput
     (every request offered at t = 0), p50/p99 latency at Poisson arrival rates
     below saturation, and the drop-in FP64 Jacobi-CG solving a sample of the
