@@ -29,8 +29,9 @@ ITERATE, SUCCESS_ABS, SUCCESS_REL, FAIL_DIV, FAIL_MAXITS = range(5)
 STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "allocation failed",
           4: "no usable sm_100 device", 5: "malformed CSR", 6: "refused by memory budget",
           7: "bounded device wait gave up", 8: "preconditioner setup failed", 9: "unknown request",
-          10: "request pending"}
+          10: "request pending", 11: "file I/O failed", 12: "unsupported or malformed file"}
 PENDING = 10
+ERR_CSR, ERR_IO, ERR_FORMAT = 5, 11, 12
 SERVE_CG, SERVE_GMRES = 0, 1
 SERVE_F64, SERVE_MIXED = 0, 1
 
@@ -151,6 +152,12 @@ def lib():
         "b200la_scatter": ([_P, _I, _I, _P, _P, _P], _I),
         "b200la_permute": ([_P, _I, _I, _P, _P, _P], _I),
         "b200la_coo_to_csr": ([_I, _I, _P, _P, _P, _P, _P, _P], _I),
+        "b200la_mm_read_info": ([C.c_char_p, _P, _P, _P], _I),
+        "b200la_mm_read_csr": ([C.c_char_p, _I, _I, _P, _P, _P], _I),
+        "b200la_mm_write_csr": ([C.c_char_p, _I, _I, _I, _P, _P, _P], _I),
+        "b200la_vec_read_info": ([C.c_char_p, _P], _I),
+        "b200la_vec_read": ([C.c_char_p, _I, _P], _I),
+        "b200la_vec_write": ([C.c_char_p, _I, _P], _I),
         "b200la_add_values": ([_P, _P, _P, _P, _I, _P, _I, _P], _I),
         "b200la_zero_rows": ([_P, _P, _P, _P, _I, _D], _I),
         "b200la_multicoloring": ([_I, _P, _P, C.POINTER(_I), _P, _P], _I),
@@ -253,6 +260,49 @@ def coo_to_csr(n, coo_row, coo_col, coo_val=None):
     _check(lib().b200la_coo_to_csr(n, nnz, _np_ptr(coo_row), _np_ptr(coo_col), _np_ptr(cv), _np_ptr(row),
                                    _np_ptr(col), _np_ptr(val)), "coo_to_csr")
     return row, col, val
+
+
+# ----------------------------------------------------------------- file I/O
+# MatrixMarket matrices and plain-text vectors with the reference's reading
+# and writing rules (CPU_CSR_lMatrix::ReadFile / WriteFile,
+# lmp/lmatrix_csr_cpu.cc:1733-1765; CPU_lVector::ReadFile / WriteFile,
+# lmp/lvector_cpu.cc:582-663).  B200Error with B200LA_ERR_IO / _FORMAT / _CSR
+# where the reference would exit.
+
+def _path(path):
+    return os.fsencode(os.fspath(path))
+
+
+def read_matrix_market(path):
+    """(row, col, val, n_cols) of a MatrixMarket file, as the reference's CSR."""
+    n, m, nnz = C.c_int(), C.c_int(), C.c_int()
+    _check(lib().b200la_mm_read_info(_path(path), C.byref(n), C.byref(m), C.byref(nnz)), f"read {path}")
+    row, col, val = np.empty(n.value + 1, np.int32), np.empty(nnz.value, np.int32), np.empty(nnz.value)
+    _check(lib().b200la_mm_read_csr(_path(path), n.value, nnz.value, _np_ptr(row), _np_ptr(col), _np_ptr(val)),
+           f"read {path}")
+    return row, col, val, m.value
+
+
+def write_matrix_market(path, row, col, val, n_cols=None):
+    """Write a host CSR as the reference does (entries as "column row value")."""
+    row, col, val = _i32(row), _i32(col), _f64(val)
+    n = row.size - 1
+    _check(lib().b200la_mm_write_csr(_path(path), n, n if n_cols is None else int(n_cols), col.size, _np_ptr(row),
+                                     _np_ptr(col), _np_ptr(val)), f"write {path}")
+
+
+def read_vector(path):
+    """The values of a one-value-per-line text file, counted as the reference counts them."""
+    n = C.c_int()
+    _check(lib().b200la_vec_read_info(_path(path), C.byref(n)), f"read {path}")
+    x = np.empty(max(n.value, 0))
+    _check(lib().b200la_vec_read(_path(path), x.size, _np_ptr(x)), f"read {path}")
+    return x
+
+
+def write_vector(path, x):
+    x = _f64(x)
+    _check(lib().b200la_vec_write(_path(path), x.size, _np_ptr(x)), f"write {path}")
 
 
 def add_values(row, col, val, rows, cols, values):
@@ -362,6 +412,10 @@ class Platform:
         except Exception:
             pass
 
+    def vector_from_file(self, path, dtype=F64):
+        """A vector read from a one-value-per-line file (CPU_lVector::ReadFile)."""
+        return self.vector(read_vector(path), dtype)
+
     # vectors are torch CUDA tensors
     def vector(self, data_or_n, dtype=F64):
         torch = _torch()
@@ -398,6 +452,10 @@ class lVector:
     def numpy(self):
         self.pf.sync()
         return self.t.cpu().numpy()
+
+    def WriteFile(self, path):
+        """One value per line (CPU_lVector::WriteFile)."""
+        write_vector(path, self.numpy())
 
     def Zeros(self):
         self.pf.check(lib().b200la_memset_zero(self.pf.h, self.ptr, self.t.numel() * self.t.element_size()))
@@ -504,6 +562,17 @@ class CSR_lMatrix:
         h = C.c_void_p()
         self.pf.check(lib().b200la_csr_cast(self.pf.h, self.h, dtype, C.byref(h)), "CastFrom")
         return CSR_lMatrix(self.pf, h, self.n, self.m, self.nnz, dtype)
+
+    @classmethod
+    def ReadFile(cls, platform, path, dtype=F64):
+        """A MatrixMarket file on the device (CPU_CSR_lMatrix::ReadFile)."""
+        row, col, val, m = read_matrix_market(path)
+        return cls.from_csr(platform, row, col, val, n_cols=m, dtype=dtype)
+
+    def WriteFile(self, path):
+        """This matrix as a MatrixMarket file (CPU_CSR_lMatrix::WriteFile)."""
+        row, col, val = self.download()
+        write_matrix_market(path, row, col, val, n_cols=self.m)
 
     def download(self):
         row = np.empty(self.n + 1, np.int32)

@@ -249,6 +249,8 @@ extern "C" const char *b200la_status_string(int s)
     case B200LA_ERR_SETUP: return "preconditioner setup failed";
     case B200LA_ERR_NOTFOUND: return "unknown request";
     case B200LA_PENDING: return "request pending";
+    case B200LA_ERR_IO: return "file I/O failed";
+    case B200LA_ERR_FORMAT: return "unsupported or malformed file";
     default: return "unknown status";
     }
 }

@@ -40,7 +40,9 @@ typedef enum {
     B200LA_ERR_TIMEOUT = 7,    /* a bounded device wait gave up */
     B200LA_ERR_SETUP = 8,      /* preconditioner analysis failed (e.g. no colours / levels) */
     B200LA_ERR_NOTFOUND = 9,   /* unknown serving request id */
-    B200LA_PENDING = 10        /* serving request still queued or running */
+    B200LA_PENDING = 10,       /* serving request still queued or running */
+    B200LA_ERR_IO = 11,        /* a file could not be opened, read or written */
+    B200LA_ERR_FORMAT = 12     /* unsupported or malformed file contents */
 } b200la_status;
 
 /* IterateControl (src/common/iterate_control.h) */
@@ -278,6 +280,31 @@ int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_csr *A32, c
 int b200la_mpir_gmres(b200la_ctx *ctx, const b200la_csr *A64, const b200la_csr *A32, const b200la_precond *P32,
                       int m, const double *b, double *x, const b200la_control *outer, const b200la_control *inner,
                       int max_outer, b200la_result *res);
+
+/* ---------------------------------------------------------------- file I/O */
+/* Host arrays.  MatrixMarket matrices: replaces CPU_CSR_lMatrix::ReadFile / WriteFile
+ * (lmp/lmatrix_csr_cpu.cc:1733-1765) over CPU_COO_lMatrix::ReadFile /
+ * WriteFile (lmp/lmatrix_coo_cpu.cc:133-299) and lmp/mmio.cc.  Sparse real or
+ * integer coordinate files; "symmetric" files are expanded (each off-diagonal
+ * entry followed by its mirror), "skew-symmetric" ones read as general, as the
+ * reference does.  The CSR is the reference's (TransformFromCOO order).
+ * read_info parses the whole file and reports the CSR's sizes; read_csr fills
+ * row[n_rows + 1], col[nnz], val[nnz].  The writer emits the reference's text
+ * byte for byte, including its "column row value" entry order (a written file
+ * read back holds the transpose).  Errors: B200LA_ERR_IO (open/read/write),
+ * B200LA_ERR_FORMAT (banner, type, size line or an entry line), B200LA_ERR_CSR
+ * (entry index outside the declared size). */
+int b200la_mm_read_info(const char *path, int *n_rows, int *n_cols, int *nnz);
+int b200la_mm_read_csr(const char *path, int n_rows, int nnz, int *row, int *col, double *val);
+int b200la_mm_write_csr(const char *path, int n_rows, int n_cols, int nnz, const int *row, const int *col,
+                        const double *val);
+/* Plain-text vectors, one value per line: replaces CPU_lVector::ReadFile /
+ * WriteFile (lmp/lvector_cpu.cc:582-663), including the reference's count (a
+ * last value not followed by a line break is dropped) and its "%e"-style
+ * output (std::scientific, 6 digits). */
+int b200la_vec_read_info(const char *path, int *n);
+int b200la_vec_read(const char *path, int n, double *x);
+int b200la_vec_write(const char *path, int n, const double *x);
 
 /* ---------------------------------------------------------------- serving */
 

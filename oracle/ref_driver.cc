@@ -515,6 +515,53 @@ double ref_time_spmv(int nthreads, int reps, int n, int nnz, const int *row, con
 
 int ref_max_threads(void) { return omp_get_max_threads(); }
 
+// CPU_CSR_lMatrix::ReadFile (lmp/lmatrix_csr_cpu.cc:1733-1749) on a
+// MatrixMarket file the reference accepts; the CSR out (caps in entries).
+// Returns nnz, or -1 when the caps are too small.
+int ref_mm_read(const char *path, int *n, int *m, int *row, int *col, double *val, int cap_rows, int cap_nnz)
+{
+    CPUsimple_CSR_lMatrix<double> A;
+    A.ReadFile(path);
+    *n = A.get_num_row();
+    *m = A.get_num_col();
+    const int nnz = A.get_nnz();
+    if (*n > cap_rows || nnz > cap_nnz) return -1;
+    std::memcpy(row, A.matrix.row, sizeof(int) * (*n + 1));
+    std::memcpy(col, A.matrix.col, sizeof(int) * nnz);
+    std::memcpy(val, A.matrix.val, sizeof(double) * nnz);
+    return nnz;
+}
+
+// CPU_CSR_lMatrix::WriteFile (lmp/lmatrix_csr_cpu.cc:1751-1765).
+void ref_mm_write(const char *path, int n, int m, int nnz, const int *row, const int *col, const double *val)
+{
+    CPUsimple_CSR_lMatrix<double> A(nnz, n, m, "A");
+    std::memcpy(A.matrix.row, row, sizeof(int) * (n + 1));
+    std::memcpy(A.matrix.col, col, sizeof(int) * nnz);
+    std::memcpy(A.matrix.val, val, sizeof(double) * nnz);
+    A.WriteFile(path);
+}
+
+// CPU_lVector::ReadFile (lmp/lvector_cpu.cc:582-636): the values out, their
+// count returned (-1 when cap is too small).
+int ref_vec_read(const char *path, double *x, int cap)
+{
+    CPUsimple_lVector<double> v;
+    v.ReadFile(path);
+    const int n = v.get_size();
+    if (n > cap) return -1;
+    for (int i = 0; i < n; ++i) x[i] = v.buffer[i];
+    return n;
+}
+
+// CPU_lVector::WriteFile (lmp/lvector_cpu.cc:638-663).
+void ref_vec_write(const char *path, int n, const double *x)
+{
+    CPUsimple_lVector<double> v(n, "v");
+    for (int i = 0; i < n; ++i) v.buffer[i] = x[i];
+    v.WriteFile(path);
+}
+
 }  // extern "C"
 
 namespace {
