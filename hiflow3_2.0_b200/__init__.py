@@ -152,6 +152,9 @@ def lib():
         "b200la_scatter": ([_P, _I, _I, _P, _P, _P], _I),
         "b200la_permute": ([_P, _I, _I, _P, _P, _P], _I),
         "b200la_coo_to_csr": ([_I, _I, _P, _P, _P, _P, _P, _P], _I),
+        "b200la_gmg_residual": ([_P, _P, _P, _P, _P, _P, _P], _I),
+        "b200la_gmg_restriction": ([_P, _P, _P, _P, _P, _P], _I),
+        "b200la_gmg_prolongation_add": ([_P, _P, _P, _P, _P, _P], _I),
         "b200la_mm_read_info": ([C.c_char_p, _P, _P, _P], _I),
         "b200la_mm_read_csr": ([C.c_char_p, _I, _I, _P, _P, _P], _I),
         "b200la_mm_write_csr": ([C.c_char_p, _I, _I, _I, _P, _P, _P], _I),
@@ -616,6 +619,32 @@ class CSR_lMatrix:
             self.close()
         except Exception:
             pass
+
+
+def _h(m):
+    return m.h if m is not None else None
+
+
+def _vp(v):
+    return v.ptr if v is not None else None
+
+
+def gmg_residual(pf, A_diag, sol, rhs, res, A_offdiag=None, sol_ghost=None):
+    """res = rhs - A_diag sol - A_offdiag sol_ghost (lmp/cuda/cuda_gmg.h)."""
+    pf.check(lib().b200la_gmg_residual(pf.h, A_diag.h, _h(A_offdiag), sol.ptr, rhs.ptr, _vp(sol_ghost), res.ptr),
+             "gmg_residual")
+
+
+def gmg_restriction(pf, R_diag, tmp, res, R_offdiag=None, res_ghost=None):
+    """res = R_diag tmp + R_offdiag res_ghost."""
+    pf.check(lib().b200la_gmg_restriction(pf.h, R_diag.h, _h(R_offdiag), tmp.ptr, _vp(res_ghost), res.ptr),
+             "gmg_restriction")
+
+
+def gmg_prolongation_add(pf, P_diag, res, sol, P_offdiag=None, res_ghost=None):
+    """sol += P_diag res + P_offdiag res_ghost."""
+    pf.check(lib().b200la_gmg_prolongation_add(pf.h, P_diag.h, _h(P_offdiag), res.ptr, _vp(res_ghost), sol.ptr),
+             "gmg_prolongation_add")
 
 
 class Preconditioner:

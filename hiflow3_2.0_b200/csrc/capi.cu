@@ -832,6 +832,75 @@ extern "C" int b200la_residual(b200la_ctx *ctx, const b200la_csr *A, const void 
     return spmv_run(ctx, A, A->all, op);
 }
 
+// ------------------------------------------------------------------ GMG level steps
+
+// The grid-transfer steps of a geometric multigrid level on the B200
+// (lmp/cuda/cuda_gmg.h, kernels lmp/cuda/cuda_gmg_kernel.h): each operator
+// is split into its diagonal block (columns of this rank's vector) and an
+// optional off-diagonal block (columns of the ghost vector; null on one rank).
+static int gmg_args(b200la_ctx *ctx, const b200la_csr *D, const b200la_csr *O, const void *in, const void *ghost,
+                    const void *out, const char *what)
+{
+    if (!ctx || !D || !in || !out || in == out || (O && (!ghost || ghost == out)))
+        return ctx_msg(ctx, B200LA_ERR_ARG, std::string(what) + ": invalid argument");
+    if (O && (O->n != D->n || O->dtype != D->dtype))
+        return ctx_msg(ctx, B200LA_ERR_ARG, std::string(what) + ": blocks differ in rows or precision");
+    return B200LA_OK;
+}
+
+// res = rhs - A_diag sol - A_offdiag sol_ghost   (kernel_gmg_compute_residual)
+extern "C" int b200la_gmg_residual(b200la_ctx *ctx, const b200la_csr *A_diag, const b200la_csr *A_offdiag,
+                                   const void *sol, const void *rhs, const void *sol_ghost, void *res)
+{
+    int rc = gmg_args(ctx, A_diag, A_offdiag, sol, sol_ghost, res, "gmg_residual");
+    if (rc) return rc;
+    if (!rhs || rhs == sol) return ctx_msg(ctx, B200LA_ERR_ARG, "gmg_residual: invalid argument");
+    SpmvOp op;
+    op.epi = EPI_RESID;
+    op.fin = FIN_NONE;
+    op.x = sol;
+    op.y = res;
+    op.b = rhs;
+    rc = spmv_run(ctx, A_diag, A_diag->all, op);
+    if (rc || !A_offdiag) return rc;
+    op.x = sol_ghost;
+    op.b = res;   // res -= A_offdiag sol_ghost, row by row in place
+    return spmv_run(ctx, A_offdiag, A_offdiag->all, op);
+}
+
+// res = R_diag tmp + R_offdiag res_ghost   (kernel_gmg_compute_restriction)
+extern "C" int b200la_gmg_restriction(b200la_ctx *ctx, const b200la_csr *R_diag, const b200la_csr *R_offdiag,
+                                      const void *tmp, const void *res_ghost, void *res)
+{
+    int rc = gmg_args(ctx, R_diag, R_offdiag, tmp, res_ghost, res, "gmg_restriction");
+    if (rc) return rc;
+    SpmvOp op;
+    op.epi = EPI_SET;
+    op.x = tmp;
+    op.y = res;
+    rc = spmv_run(ctx, R_diag, R_diag->all, op);
+    if (rc || !R_offdiag) return rc;
+    op.epi = EPI_ADD;
+    op.x = res_ghost;
+    return spmv_run(ctx, R_offdiag, R_offdiag->all, op);
+}
+
+// sol += P_diag res + P_offdiag res_ghost   (kernel_gmg_compute_updated_solution)
+extern "C" int b200la_gmg_prolongation_add(b200la_ctx *ctx, const b200la_csr *P_diag, const b200la_csr *P_offdiag,
+                                           const void *res, const void *res_ghost, void *sol)
+{
+    int rc = gmg_args(ctx, P_diag, P_offdiag, res, res_ghost, sol, "gmg_prolongation_add");
+    if (rc) return rc;
+    SpmvOp op;
+    op.epi = EPI_ADD;
+    op.x = res;
+    op.y = sol;
+    rc = spmv_run(ctx, P_diag, P_diag->all, op);
+    if (rc || !P_offdiag) return rc;
+    op.x = res_ghost;
+    return spmv_run(ctx, P_offdiag, P_offdiag->all, op);
+}
+
 // ------------------------------------------------------------------ BLAS1
 
 static bool dt_ok(int dtype) { return dtype == B200LA_F64 || dtype == B200LA_F32; }

@@ -153,6 +153,24 @@ int b200la_spmv_dot(b200la_ctx *ctx, const b200la_csr *A, const void *x, void *y
 int b200la_residual(b200la_ctx *ctx, const b200la_csr *A, const void *b, const void *x, void *r,
                     double *nrm2sq_dev);
 
+/* ------------------------------------------------------- GMG level steps */
+/* Geometric-multigrid grid transfers on operators split into a diagonal block
+ * (columns of this rank's vectors) and an optional off-diagonal block (columns
+ * of the ghost vector; pass NULL on one rank).  Replace the GPU kernels of
+ * lmp/cuda/cuda_gmg.h (kernel_gmg_compute_residual / _restriction /
+ * _updated_solution, lmp/cuda/cuda_gmg_kernel.h), with and without the
+ * off-diagonal block.  Device pointers; the blocks share the dtype and the
+ * row count; outputs must not alias inputs (rhs may not be sol). */
+/* res = rhs - A_diag sol - A_offdiag sol_ghost */
+int b200la_gmg_residual(b200la_ctx *ctx, const b200la_csr *A_diag, const b200la_csr *A_offdiag, const void *sol,
+                        const void *rhs, const void *sol_ghost, void *res);
+/* res = R_diag tmp + R_offdiag res_ghost (restriction to the coarse level) */
+int b200la_gmg_restriction(b200la_ctx *ctx, const b200la_csr *R_diag, const b200la_csr *R_offdiag,
+                           const void *tmp, const void *res_ghost, void *res);
+/* sol += P_diag res + P_offdiag res_ghost (prolongation of a coarse correction) */
+int b200la_gmg_prolongation_add(b200la_ctx *ctx, const b200la_csr *P_diag, const b200la_csr *P_offdiag,
+                                const void *res, const void *res_ghost, void *sol);
+
 /* ------------------------------------------------------------------- BLAS1 */
 
 /* lVector::Dot / Norm2 (src/linear_algebra/lmp/lvector.h:266,274; GPU
