@@ -167,12 +167,15 @@ def lib():
         "b200la_levelscheduling": ([_I, _P, _P, C.POINTER(_I), _P, _P], _I),
         "b200la_reorder_csr": ([_I, _P, _P, _P, _P, _P, _P, _P], _I),
         "b200la_ilu0": ([_I, _P, _P, _P], _I),
+        "b200la_matrix_power_pattern": ([_I, _P, _P, _I, _P, _P, _P], _I),
+        "b200la_ilup": ([_I, _P, _P, _P, _I, _P, _P, _P, _P], _I),
         "b200la_q1_sizes": ([_I, _I, C.POINTER(_I), C.POINTER(C.c_int64)], _I),
         "b200la_q1_assemble": ([_I, _I, _I, _P, _D, _P, _P, _P, _P], _I),
         "b200la_q1_rhs": ([C.c_uint64, _I, _I, _P], _I),
         "b200la_precond_jacobi": ([_P, _P, C.POINTER(_P)], _I),
         "b200la_precond_mcsgs": ([_P, _I, _P, _P, _P, _D, _I, C.POINTER(_P), C.POINTER(_P)], _I),
         "b200la_precond_ilu0": ([_P, _I, _P, _P, _P, _I, _I, C.POINTER(_P), C.POINTER(_P)], _I),
+        "b200la_precond_ilup": ([_P, _I, _P, _P, _P, _I, _I, _I, _I, C.POINTER(_P), C.POINTER(_P)], _I),
         "b200la_precond_info": ([_P, C.POINTER(_I), C.POINTER(_I), C.POINTER(_I), _P, _P], _I),
         "b200la_precond_apply": ([_P, _P, _P, _P], _I),
         "b200la_precond_destroy": ([_P], _I),
@@ -353,6 +356,29 @@ def ilu0(row, col, val):
     row, col, v = _i32(row), _i32(col), _f64(val).copy()
     _check(lib().b200la_ilu0(row.size - 1, _np_ptr(row), _np_ptr(col), _np_ptr(v)), "ilu0")
     return v
+
+
+def matrix_power_pattern(row, col, p):
+    """(row, col) of the pattern of A^p (MatrixSupSPower)."""
+    row, col = _i32(row), _i32(col)
+    n, nnz = row.size - 1, C.c_int()
+    _check(lib().b200la_matrix_power_pattern(n, _np_ptr(row), _np_ptr(col), p, C.byref(nnz), None, None),
+           "matrix_power_pattern")
+    ro, co = np.empty(n + 1, np.int32), np.empty(nnz.value, np.int32)
+    _check(lib().b200la_matrix_power_pattern(n, _np_ptr(row), _np_ptr(col), p, C.byref(nnz), _np_ptr(ro),
+                                             _np_ptr(co)), "matrix_power_pattern")
+    return ro, co
+
+
+def ilup(row, col, val, p):
+    """ILU(p) factors (row, col, val) on the level-of-fill pattern (ilup)."""
+    row, col, val = _i32(row), _i32(col), _f64(val)
+    n, nnz = row.size - 1, C.c_int()
+    _check(lib().b200la_ilup(n, _np_ptr(row), _np_ptr(col), _np_ptr(val), p, C.byref(nnz), None, None, None), "ilup")
+    ro, co, vo = np.empty(n + 1, np.int32), np.empty(nnz.value, np.int32), np.empty(nnz.value)
+    _check(lib().b200la_ilup(n, _np_ptr(row), _np_ptr(col), _np_ptr(val), p, C.byref(nnz), _np_ptr(ro), _np_ptr(co),
+                             _np_ptr(vo)), "ilup")
+    return ro, co, vo
 
 
 # ----------------------------------------------------------------- device side
@@ -684,6 +710,18 @@ class Preconditioner:
         h, Ap = C.c_void_p(), C.c_void_p()
         platform.check(lib().b200la_precond_ilu0(platform.h, n, _np_ptr(row), _np_ptr(col), _np_ptr(val), mode,
                                                  dtype, C.byref(h), C.byref(Ap)), "precond_ilu0")
+        A = CSR_lMatrix(platform, Ap, n, n, col.size, dtype)
+        return cls(platform, h, mode, n, A)
+
+    @classmethod
+    def ILUp(cls, platform, row, col, val, ilu_p, mat_power=1, mode=PRECOND_ILU0_MC, dtype=F64):
+        """lPreconditioner_MultiColoring_ILUp with ILU(ilu_p) factors and the
+        colouring on the pattern of A^mat_power (level scheduling: mat_power 1)."""
+        row, col, val = _i32(row), _i32(col), _f64(val)
+        n = row.size - 1
+        h, Ap = C.c_void_p(), C.c_void_p()
+        platform.check(lib().b200la_precond_ilup(platform.h, n, _np_ptr(row), _np_ptr(col), _np_ptr(val), mode,
+                                                 ilu_p, mat_power, dtype, C.byref(h), C.byref(Ap)), "precond_ilup")
         A = CSR_lMatrix(platform, Ap, n, n, col.size, dtype)
         return cls(platform, h, mode, n, A)
 

@@ -1070,6 +1070,58 @@ extern "C" int b200la_ilu0(int n, const int *row, const int *col, double *val)
     return B200LA_OK;
 }
 
+static int host_csr_in(int n, const int *row, const int *col, const double *val, host::Csr &A)
+{
+    if (n < 0 || !row || !col) return B200LA_ERR_ARG;
+    long long bad = -1;
+    if (host::validate_csr(n, n, row[n], row, col, &bad)) return B200LA_ERR_CSR;
+    A.n = A.m = n;
+    A.row.assign(row, row + n + 1);
+    A.col.assign(col, col + row[n]);
+    if (val) A.val.assign(val, val + row[n]);
+    else A.val.assign(row[n], 1.0);
+    return B200LA_OK;
+}
+
+// Copy out a host CSR in the two-call convention: always *nnz; the arrays
+// when row_out is given (then col_out and val_out, if given, hold *nnz).
+static int host_csr_out(const host::Csr &B, int *nnz, int *row_out, int *col_out, double *val_out)
+{
+    *nnz = B.nnz();
+    if (!row_out) return B200LA_OK;
+    std::copy(B.row.begin(), B.row.end(), row_out);
+    if (col_out) std::copy(B.col.begin(), B.col.end(), col_out);
+    if (val_out) std::copy(B.val.begin(), B.val.end(), val_out);
+    return B200LA_OK;
+}
+
+extern "C" int b200la_matrix_power_pattern(int n, const int *row, const int *col, int p, int *nnz, int *row_out,
+                                           int *col_out)
+{
+    if (p < 1 || !nnz) return B200LA_ERR_ARG;
+    host::Csr A, P;
+    int rc = host_csr_in(n, row, col, nullptr, A);
+    if (rc) return rc;
+    host::matrix_sup_power(A, p, P);
+    return host_csr_out(P, nnz, row_out, col_out, nullptr);
+}
+
+extern "C" int b200la_ilup(int n, const int *row, const int *col, const double *val, int p, int *nnz, int *row_out,
+                           int *col_out, double *val_out)
+{
+    if (p < 0 || !val || !nnz) return B200LA_ERR_ARG;
+    host::Csr A, LU;
+    int rc = host_csr_in(n, row, col, val, A);
+    if (rc) return rc;
+    for (int i = 0; i < n; ++i) {
+        bool diag = false;
+        for (int j = row[i]; j < row[i + 1]; ++j) diag |= (col[j] == i);
+        if (!diag) return B200LA_ERR_CSR;   // the factorisation walks each row up to its diagonal
+    }
+    host::ilup(A, p, LU);
+    return host_csr_out(LU, nnz, row_out, col_out, val_out);
+}
+
 extern "C" int b200la_q1_sizes(int dim, int N, int *n, int64_t *nnz)
 {
     if (!n || !nnz) return B200LA_ERR_ARG;

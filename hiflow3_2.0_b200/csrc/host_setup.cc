@@ -364,6 +364,104 @@ void ilu0(int n, const int *row, const int *col, double *val)
     }
 }
 
+void matrix_sup_power(const Csr &A, int p, Csr &P)
+{
+    // row i of the product with A: the union of the rows of A named by the
+    // columns of row i (the symbolic product of Bank & Douglas); columns in
+    // ascending order, as the reference's COO round trip leaves them
+    const int n = A.n;
+    P = A;
+    std::vector<int> mark(A.m > n ? A.m : n, -1), cols;
+    for (int it = 1; it < p; ++it) {
+        Csr Q;
+        Q.n = n;
+        Q.m = A.m;
+        Q.row.assign(n + 1, 0);
+        for (int i = 0; i < n; ++i) {
+            cols.clear();
+            for (int a = P.row[i]; a < P.row[i + 1]; ++a) {
+                const int k = P.col[a];
+                for (int b = A.row[k]; b < A.row[k + 1]; ++b) {
+                    const int j = A.col[b];
+                    if (mark[j] != i) {
+                        mark[j] = i;
+                        cols.push_back(j);
+                    }
+                }
+            }
+            std::sort(cols.begin(), cols.end());
+            Q.col.insert(Q.col.end(), cols.begin(), cols.end());
+            Q.row[i + 1] = (int)Q.col.size();
+        }
+        Q.val.assign(Q.col.size(), 1.0);
+        std::fill(mark.begin(), mark.end(), -1);
+        P = std::move(Q);
+    }
+}
+
+void ilup(const Csr &A, int p, Csr &LU)
+{
+    const int n = A.n;
+    // the pattern of A^(p+1) carrying A's values (zeros elsewhere)
+    Csr F;
+    matrix_sup_power(A, p + 1, F);
+    for (int i = 0; i < n; ++i)
+        for (int j = F.row[i]; j < F.row[i + 1]; ++j) {
+            double v = 0.0;
+            for (int k = A.row[i]; k < A.row[i + 1]; ++k)
+                if (F.col[j] == A.col[k]) v += A.val[k];
+            F.val[j] = v;
+        }
+    // level of fill: 0 for nonzero entries of A, 9999 for the rest
+    std::vector<double> lev(F.col.size());
+    for (size_t j = 0; j < lev.size(); ++j) lev[j] = F.val[j] * F.val[j] > 0.0 ? 0.0 : 9999.0;
+    const double pp = (double)p;
+    int kk = 0;
+    for (int i = 1; i < n; ++i) {
+        for (int ik = F.row[i]; F.col[ik] < i; ++ik) {
+            if (!(lev[ik] <= pp)) continue;
+            const int k = F.col[ik];
+            for (int h = F.row[k]; h < F.row[k + 1]; ++h)
+                if (F.col[h] == k) {
+                    kk = h;
+                    break;
+                }
+            F.val[ik] = F.val[ik] / (1.0 * F.val[kk]);
+            for (int ij = ik + 1; ij < F.row[i + 1]; ++ij) {
+                double vkj = 0.0, lkj = 9999;
+                for (int h = F.row[k]; h < F.row[k + 1]; ++h)
+                    if (F.col[h] == F.col[ij]) {
+                        vkj = F.val[h];
+                        lkj = lev[h];
+                        break;
+                    }
+                const double lt = 1 + lkj + lev[ik];
+                F.val[ij] = F.val[ij] - vkj * F.val[ik];
+                if (lev[ij] > lt) lev[ij] = lt;
+            }
+        }
+        for (int h = F.row[i]; h < F.row[i + 1]; ++h)
+            if (lev[h] > pp) {
+                F.val[h] = 0.0;
+                lev[h] = 9999.0;
+            }
+    }
+    // keep the entries of level <= p
+    LU.n = n;
+    LU.m = A.m;
+    LU.row.assign(n + 1, 0);
+    LU.col.clear();
+    LU.val.clear();
+    for (int i = 0; i < n; ++i) {
+        for (int h = F.row[i]; h < F.row[i + 1]; ++h)
+            if (lev[h] <= pp) {
+                LU.col.push_back(F.col[h]);
+                LU.val.push_back(F.val[h]);
+            }
+        LU.row[i + 1] = (int)LU.col.size();
+    }
+}
+
 void dropoffs(Csr &A, const std::vector<int> &block_off)
 {
     const int n = A.n;

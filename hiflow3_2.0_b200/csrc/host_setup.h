@@ -62,6 +62,13 @@ int levelscheduling(int n, const int *row, const int *col, int *nlevels, std::ve
 void reorder(const Csr &A, const std::vector<int> &perm, Csr &B);
 // lmp/lmatrix_csr_cpu.cc:1880-1930 (in place)
 void ilu0(int n, const int *row, const int *col, double *val);
+// lmp/lmatrix_csr_cpu.cc:1641-1664 (MatrixSupSPower) over :1520-1636
+// (MatrixMultSupStructure): the pattern of A^p (p >= 1; p = 1 copies A);
+// values are 1 for p > 1.
+void matrix_sup_power(const Csr &A, int p, Csr &P);
+// lmp/lmatrix_csr_cpu.cc:1933-2104 (ilup): ILU(p) by levels of fill on the
+// pattern of A^(p+1), compressed to the entries of level <= p.
+void ilup(const Csr &A, int p, Csr &LU);
 // lmp/lpreconditioner_mc.cc:647-693 + lmp/lmatrix_csr_cpu.cc:2436-2495
 void dropoffs(Csr &A, const std::vector<int> &block_off);
 

@@ -76,7 +76,8 @@ static int upload_csr(b200la_ctx *ctx, const host::Csr &M, int dtype, const std:
 }
 
 static int build_block(b200la_ctx *ctx, int kind, int n, const int *row, const int *col, const double *val,
-                       double omega, int dtype, b200la_precond **out, b200la_csr **A_perm)
+                       double omega, int dtype, b200la_precond **out, b200la_csr **A_perm, int ilu_p = 0,
+                       int mat_power = 1)
 {
     if (!ctx || n < 1 || !row || !col || !val || !out || (dtype != B200LA_F64 && dtype != B200LA_F32))
         return pfail(ctx, B200LA_ERR_ARG, "precond: invalid argument");
@@ -100,17 +101,26 @@ static int build_block(b200la_ctx *ctx, int kind, int n, const int *row, const i
         // ilu0 in natural order, level scheduling of the factor, permute_all
         // (lpreconditioner_mc.cc:176-192, 310-351)
         host::Csr F = A;
-        host::ilu0(n, F.row.data(), F.col.data(), F.val.data());
+        if (ilu_p > 0) host::ilup(A, ilu_p, F);
+        else host::ilu0(n, F.row.data(), F.col.data(), F.val.data());
         if (host::levelscheduling(n, F.row.data(), F.col.data(), &nb, sizes, perm))
             return pfail(ctx, B200LA_ERR_SETUP, "precond: level scheduling did not complete");
         host::reorder(A, perm, Ap);
         host::reorder(F, perm, LU);
     } else {
-        if (host::multicoloring(n, row, col, &nb, sizes, perm))
+        // colours of the analysis matrix: the operator, or the pattern of its
+        // mat_power-th power (build_aux_matrix, lpreconditioner_mc_ilup.cc:107-140)
+        host::Csr aux;
+        if (mat_power > 1) host::matrix_sup_power(A, mat_power, aux);
+        const host::Csr &an = mat_power > 1 ? aux : A;
+        if (host::multicoloring(n, an.row.data(), an.col.data(), &nb, sizes, perm))
             return pfail(ctx, B200LA_ERR_SETUP, "precond: multicolouring found no colours");
         host::reorder(A, perm, Ap);
         LU = Ap;
-        if (kind == B200LA_PRECOND_ILU0_MC) host::ilu0(n, LU.row.data(), LU.col.data(), LU.val.data());
+        if (kind == B200LA_PRECOND_ILU0_MC) {
+            if (ilu_p > 0) host::ilup(Ap, ilu_p, LU);
+            else host::ilu0(n, LU.row.data(), LU.col.data(), LU.val.data());
+        }
     }
     std::vector<int> off(nb + 1, 0);
     for (int b = 0; b < nb; ++b) off[b + 1] = off[b] + sizes[b];
@@ -202,6 +212,17 @@ extern "C" int b200la_precond_ilu0(b200la_ctx *ctx, int n, const int *row, const
     if (mode != B200LA_PRECOND_ILU0_LS && mode != B200LA_PRECOND_ILU0_MC)
         return pfail(ctx, B200LA_ERR_ARG, "precond_ilu0: mode must be ILU0_LS or ILU0_MC");
     return build_block(ctx, mode, n, row, col, val, 1.0, dtype, out, A_perm);
+}
+
+extern "C" int b200la_precond_ilup(b200la_ctx *ctx, int n, const int *row, const int *col, const double *val,
+                                   int mode, int ilu_p, int mat_power, int dtype, b200la_precond **out,
+                                   b200la_csr **A_perm)
+{
+    if (mode != B200LA_PRECOND_ILU0_LS && mode != B200LA_PRECOND_ILU0_MC)
+        return pfail(ctx, B200LA_ERR_ARG, "precond_ilup: mode must be ILU0_LS or ILU0_MC");
+    if (ilu_p < 0 || mat_power < 1 || (mode == B200LA_PRECOND_ILU0_LS && mat_power != 1))
+        return pfail(ctx, B200LA_ERR_ARG, "precond_ilup: ilu_p >= 0, mat_power >= 1 (1 with level scheduling)");
+    return build_block(ctx, mode, n, row, col, val, 1.0, dtype, out, A_perm, ilu_p, mat_power);
 }
 
 extern "C" int b200la_precond_info(const b200la_precond *P, int *kind, int *n, int *nblocks, int *block_sizes,

@@ -229,6 +229,16 @@ int b200la_reorder_csr(int n, const int *row, const int *col, const double *val,
                        int *col_out, double *val_out);
 /* ilu0 (lmatrix_csr_cpu.cc:1880-1930), in place on val. */
 int b200la_ilu0(int n, const int *row, const int *col, double *val);
+/* Two-call convention for a CSR result: *nnz always; the arrays too when
+ * row_out is given (row_out n+1, col_out / val_out *nnz entries).
+ * MatrixSupSPower (lmatrix_csr_cpu.cc:1641-1664 over MatrixMultSupStructure
+ * :1520-1636): the pattern of A^p, p >= 1, columns ascending. */
+int b200la_matrix_power_pattern(int n, const int *row, const int *col, int p, int *nnz, int *row_out, int *col_out);
+/* ilup (lmatrix_csr_cpu.cc:1933-2104): ILU(p) by levels of fill on the pattern
+ * of A^(p+1), keeping the entries of level <= p (unit-lower L strictly below,
+ * U with the diagonal, in one CSR).  p = 0 uses the pattern of A itself. */
+int b200la_ilup(int n, const int *row, const int *col, const double *val, int p, int *nnz, int *row_out,
+                int *col_out, double *val_out);
 /* Structured Q1 workloads (lexicographic DoFs; weak forms of
  * examples/poisson/poisson_tutorial.h:152-176 and examples/convection_diffusion/convdiff.cc:75-117):
  * kind 0 Poisson (kcell per cell or NULL), kind 1 convection-diffusion (nu, beta). */
@@ -264,6 +274,13 @@ int b200la_precond_mcsgs(b200la_ctx *ctx, int n, const int *row, const int *col,
  * (mc = false, ls = true); B200LA_PRECOND_ILU0_MC colours first (mc = true). */
 int b200la_precond_ilu0(b200la_ctx *ctx, int n, const int *row, const int *col, const double *val, int mode,
                         int dtype, b200la_precond **out, b200la_csr **A_perm);
+/* The same with ILU(p) factors (lpreconditioner_mc_ilup.cc:84-194): ilu_p levels
+ * of fill; with B200LA_PRECOND_ILU0_MC the colouring runs on the pattern of
+ * A^mat_power (build_aux_matrix), with B200LA_PRECOND_ILU0_LS mat_power is 1
+ * and the levels come from the factor's pattern.  ilu_p = 0, mat_power = 1 is
+ * b200la_precond_ilu0. */
+int b200la_precond_ilup(b200la_ctx *ctx, int n, const int *row, const int *col, const double *val, int mode,
+                        int ilu_p, int mat_power, int dtype, b200la_precond **out, b200la_csr **A_perm);
 /* Permutation (perm[new] = old, host array of n) and block structure
  * (colours or levels; sizes holds n entries). */
 int b200la_precond_info(const b200la_precond *P, int *kind, int *n, int *nblocks, int *block_sizes, int *perm);

@@ -674,6 +674,165 @@ int orc_ilu0_build(int n, const int *row, const int *col, const double *val, int
     return 0;
 }
 
+/* Pattern of A^p: rows of the symbolic product by A, p - 1 times, columns
+ * ascending (MatrixSupSPower / MatrixMultSupStructure, lmatrix_csr_cpu.cc:
+ * 1520-1664, whose COO round trip sorts every row).  p = 1 copies A's
+ * pattern.  Outputs allocated here (free with orc_free); returns nnz. */
+int orc_power_pattern(int n, const int *row, const int *col, int p, int **row_out, int **col_out)
+{
+    int nnz = row[n];
+    int *r = (int *)malloc(sizeof(int) * (n + 1));
+    int *c = (int *)malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+    memcpy(r, row, sizeof(int) * (n + 1));
+    memcpy(c, col, sizeof(int) * nnz);
+    int *seen = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+    int *buf = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+    for (int it = 1; it < p; ++it) {
+        for (int j = 0; j < n; ++j) seen[j] = -1;
+        int cap = nnz * 2 + n, m = 0;
+        int *r2 = (int *)malloc(sizeof(int) * (n + 1));
+        int *c2 = (int *)malloc(sizeof(int) * cap);
+        r2[0] = 0;
+        for (int i = 0; i < n; ++i) {
+            int len = 0;
+            for (int a = r[i]; a < r[i + 1]; ++a) {
+                const int k = c[a];
+                for (int b = row[k]; b < row[k + 1]; ++b)
+                    if (seen[col[b]] != i) { seen[col[b]] = i; buf[len++] = col[b]; }
+            }
+            /* insertion sort of the row's columns */
+            for (int x = 1; x < len; ++x) {
+                const int v = buf[x];
+                int y = x - 1;
+                while (y >= 0 && buf[y] > v) { buf[y + 1] = buf[y]; --y; }
+                buf[y + 1] = v;
+            }
+            if (m + len > cap) { cap = 2 * (m + len); c2 = (int *)realloc(c2, sizeof(int) * cap); }
+            memcpy(c2 + m, buf, sizeof(int) * len);
+            m += len;
+            r2[i + 1] = m;
+        }
+        free(r); free(c);
+        r = r2; c = c2; nnz = m;
+    }
+    free(seen); free(buf);
+    *row_out = r;
+    *col_out = c;
+    return nnz;
+}
+
+void orc_free(void *p) { free(p); }
+
+/* ILU(p) (lmatrix_csr_cpu.cc:1933-2104): A's values on the pattern of
+ * A^(p+1), level 0 for nonzero entries and 9999 for the rest; IKJ
+ * elimination over the lower entries of level <= p with
+ * lev_ij = min(lev_ij, 1 + lev_kj + lev_ik); entries above level p are zeroed
+ * after each row; the result keeps the entries of level <= p.  Outputs
+ * allocated here; returns nnz. */
+int orc_ilup(int n, const int *row, const int *col, const double *val, int p, int **row_out, int **col_out,
+             double **val_out)
+{
+    int *fr, *fc;
+    const int fn = orc_power_pattern(n, row, col, p + 1, &fr, &fc);
+    double *fv = (double *)malloc(sizeof(double) * (fn > 0 ? fn : 1));
+    double *lev = (double *)malloc(sizeof(double) * (fn > 0 ? fn : 1));
+    for (int i = 0; i < n; ++i)
+        for (int j = fr[i]; j < fr[i + 1]; ++j) {
+            double v = 0.0;   /* MatrixAdd onto the zeroed pattern */
+            for (int k = row[i]; k < row[i + 1]; ++k)
+                if (fc[j] == col[k]) v += val[k];
+            fv[j] = v;
+            lev[j] = v * v > 0.0 ? 0.0 : 9999.0;
+        }
+    const double pp = (double)p;
+    int kk = 0;
+    for (int i = 1; i < n; ++i) {
+        for (int ik = fr[i]; fc[ik] < i; ++ik) {
+            if (!(lev[ik] <= pp)) continue;
+            const int k = fc[ik];
+            for (int h = fr[k]; h < fr[k + 1]; ++h)
+                if (fc[h] == k) { kk = h; break; }
+            fv[ik] = fv[ik] / (1.0 * fv[kk]);
+            for (int ij = ik + 1; ij < fr[i + 1]; ++ij) {
+                double vkj = 0.0, lkj = 9999.0;
+                for (int h = fr[k]; h < fr[k + 1]; ++h)
+                    if (fc[h] == fc[ij]) { vkj = fv[h]; lkj = lev[h]; break; }
+                const double lt = 1 + lkj + lev[ik];
+                fv[ij] = fv[ij] - vkj * fv[ik];
+                if (lev[ij] > lt) lev[ij] = lt;
+            }
+        }
+        for (int h = fr[i]; h < fr[i + 1]; ++h)
+            if (lev[h] > pp) { fv[h] = 0.0; lev[h] = 9999.0; }
+    }
+    int m = 0;
+    for (int j = 0; j < fn; ++j) m += lev[j] <= pp;
+    int *r = (int *)malloc(sizeof(int) * (n + 1));
+    int *c = (int *)malloc(sizeof(int) * (m > 0 ? m : 1));
+    double *v = (double *)malloc(sizeof(double) * (m > 0 ? m : 1));
+    int t = 0;
+    r[0] = 0;
+    for (int i = 0; i < n; ++i) {
+        for (int h = fr[i]; h < fr[i + 1]; ++h)
+            if (lev[h] <= pp) { c[t] = fc[h]; v[t] = fv[h]; ++t; }
+        r[i + 1] = t;
+    }
+    free(fr); free(fc); free(fv); free(lev);
+    *row_out = r; *col_out = c; *val_out = v;
+    return m;
+}
+
+int orc_ilup_build(int n, const int *row, const int *col, const double *val, int mode, int ilu_p, int mat_power,
+                   orc_block_precond *P, int *Ap_row, int *Ap_col, double *Ap_val)
+{
+    /* lpreconditioner_mc.cc:157-195 with lpreconditioner_mc_ilup.cc:107-194:
+     * mode 0 ILU(p) in natural order, levels of the factors, permute_all;
+     * mode 1 colouring of the pattern of A^mat_power, permute, ILU(p) of the
+     * permuted operator. */
+    if (ilu_p == 0 && mat_power == 1) return orc_ilu0_build(n, row, col, val, mode, P, Ap_row, Ap_col, Ap_val);
+    memset(P, 0, sizeof(*P));
+    int *sizes = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+    P->perm = (int *)malloc(sizeof(int) * (n > 0 ? n : 1));
+    P->n = n;
+    int nb, *fr, *fc;
+    double *fv;
+    if (mode == 0) {
+        const int fn = orc_ilup(n, row, col, val, ilu_p, &fr, &fc, &fv);
+        if (orc_levelscheduling(n, fr, fc, &nb, sizes, P->perm)) { free(sizes); return -1; }
+        P->row = (int *)malloc(sizeof(int) * (n + 1));
+        P->col = (int *)malloc(sizeof(int) * (fn > 0 ? fn : 1));
+        P->val = (double *)malloc(sizeof(double) * (fn > 0 ? fn : 1));
+        orc_reorder_csr(n, fr, fc, fv, P->perm, P->row, P->col, P->val);
+        free(fr); free(fc); free(fv);
+        orc_reorder_csr(n, row, col, val, P->perm, Ap_row, Ap_col, Ap_val);
+    } else {
+        int *ar = (int *)row, *ac = (int *)col;
+        if (mat_power > 1) orc_power_pattern(n, row, col, mat_power, &ar, &ac);
+        const int bad = orc_multicoloring(n, ar, ac, &nb, sizes, P->perm);
+        if (mat_power > 1) { free(ar); free(ac); }
+        if (bad) { free(sizes); return -1; }
+        orc_reorder_csr(n, row, col, val, P->perm, Ap_row, Ap_col, Ap_val);
+        if (ilu_p > 0) {
+            orc_ilup(n, Ap_row, Ap_col, Ap_val, ilu_p, &P->row, &P->col, &P->val);
+        } else {
+            const int nnz = row[n];
+            P->row = (int *)malloc(sizeof(int) * (n + 1));
+            P->col = (int *)malloc(sizeof(int) * (nnz > 0 ? nnz : 1));
+            P->val = (double *)malloc(sizeof(double) * (nnz > 0 ? nnz : 1));
+            memcpy(P->row, Ap_row, sizeof(int) * (n + 1));
+            memcpy(P->col, Ap_col, sizeof(int) * nnz);
+            memcpy(P->val, Ap_val, sizeof(double) * nnz);
+            orc_ilu0(n, P->row, P->col, P->val);
+        }
+    }
+    P->nblocks = nb;
+    P->block_off = sizes_to_offsets(nb, sizes);
+    free(sizes);
+    dropoffs(n, nb, P->block_off, &P->row, &P->col, &P->val);
+    block_finish(P, 1, 1.0);
+    return 0;
+}
+
 void orc_block_apply(const orc_block_precond *P, const double *r, double *z)
 {
     /* ApplylPreconditioner (lpreconditioner_mc.cc:716-728): the per-block

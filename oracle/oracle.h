@@ -167,6 +167,18 @@ int orc_mcsgs_build(int n, const int *row, const int *col, const double *val, do
 int orc_ilu0_build(int n, const int *row, const int *col, const double *val, int mode,
                    orc_block_precond *P, int *Ap_row, int *Ap_col, double *Ap_val);
 
+/* Pattern of A^p (MatrixSupSPower, lmatrix_csr_cpu.cc:1520-1664) and ILU(p)
+ * (ilup, lmatrix_csr_cpu.cc:1933-2104); outputs allocated, free with orc_free;
+ * both return nnz. */
+int orc_power_pattern(int n, const int *row, const int *col, int p, int **row_out, int **col_out);
+int orc_ilup(int n, const int *row, const int *col, const double *val, int p, int **row_out, int **col_out,
+             double **val_out);
+void orc_free(void *p);
+/* ILU(p) block build (lpreconditioner_mc_ilup.cc:84-194): mode as orc_ilu0_build;
+ * the colouring (mode 1) runs on the pattern of A^mat_power. */
+int orc_ilup_build(int n, const int *row, const int *col, const double *val, int mode, int ilu_p, int mat_power,
+                   orc_block_precond *P, int *Ap_row, int *Ap_col, double *Ap_val);
+
 /* z = M^{-1} r in the permuted numbering (ApplylPreconditioner,
  * lpreconditioner_mc.cc:716-728 with the variant's forward/diagonal/backward). */
 void orc_block_apply(const orc_block_precond *P, const double *r, double *z);

@@ -130,6 +130,13 @@ class Oracle:
                                       _i32p, _i32p, _f64p]
         L.orc_ilu0_build.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int, C.POINTER(_Block),
                                      _i32p, _i32p, _f64p]
+        L.orc_ilup_build.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_int, C.c_int, C.POINTER(_Block),
+                                     _i32p, _i32p, _f64p]
+        _pp, _dp = C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.POINTER(C.c_double))
+        L.orc_power_pattern.argtypes = [C.c_int, _i32p, _i32p, C.c_int, _pp, _pp]
+        L.orc_ilup.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int, _pp, _pp, _dp]
+        L.orc_free.argtypes = [C.c_void_p]
+        L.orc_free.restype = None
         L.orc_block_apply.argtypes = [C.POINTER(_Block), _f64p, _f64p]
         L.orc_block_apply.restype = None
         L.orc_block_free.argtypes = [C.POINTER(_Block)]
@@ -292,6 +299,34 @@ class Oracle:
             raise RuntimeError("ilu0 build failed")
         return BlockPrecond(self.lib, st), (Ar, Ac, Av)
 
+    def power_pattern(self, row, col, p):
+        n = len(row) - 1
+        r, c = C.POINTER(C.c_int)(), C.POINTER(C.c_int)()
+        m = self.lib.orc_power_pattern(n, _i32(row), _i32(col), p, C.byref(r), C.byref(c))
+        out = (np.ctypeslib.as_array(r, (n + 1,)).copy(), np.ctypeslib.as_array(c, (max(m, 1),))[:m].copy())
+        self.lib.orc_free(C.cast(r, C.c_void_p))
+        self.lib.orc_free(C.cast(c, C.c_void_p))
+        return out
+
+    def ilup(self, row, col, val, p):
+        n = len(row) - 1
+        r, c, v = C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()
+        m = self.lib.orc_ilup(n, _i32(row), _i32(col), _f64(val), p, C.byref(r), C.byref(c), C.byref(v))
+        out = (np.ctypeslib.as_array(r, (n + 1,)).copy(), np.ctypeslib.as_array(c, (max(m, 1),))[:m].copy(),
+               np.ctypeslib.as_array(v, (max(m, 1),))[:m].copy())
+        for q in (r, c, v):
+            self.lib.orc_free(C.cast(q, C.c_void_p))
+        return out
+
+    def ilup_build(self, row, col, val, mode, ilu_p, mat_power=1):
+        n = len(row) - 1
+        st = _Block()
+        Ar, Ac, Av = np.empty(n + 1, np.int32), np.empty(len(col), np.int32), np.empty(len(col))
+        if self.lib.orc_ilup_build(n, _i32(row), _i32(col), _f64(val), mode, ilu_p, mat_power, C.byref(st),
+                                   Ar, Ac, Av):
+            raise RuntimeError("ilup build failed")
+        return BlockPrecond(self.lib, st), (Ar, Ac, Av)
+
     # ---- solvers ----
     def _precond_args(self, precond):
         if precond is None:
@@ -372,6 +407,12 @@ class Ref:
         L.ref_ilu_solve.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
         L.ref_block_precond.argtypes = [C.c_int, C.c_double, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p,
                                         _f64p, _i32p, C.POINTER(C.c_int), _i32p, _i32p, _i32p, _f64p]
+        L.ref_block_precond_ilup.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p,
+                                             _f64p, _f64p, _i32p, C.POINTER(C.c_int), _i32p, _i32p, _i32p, _f64p]
+        L.ref_ilup.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_int, _i32p, _i32p, _f64p]
+        L.ref_set_ilup.argtypes = [C.c_int, C.c_int]
+        L.ref_set_ilup.restype = None
+        L.ref_power_pattern.argtypes = [C.c_int, C.c_int, _i32p, _i32p, C.c_int, C.c_int, _i32p, _i32p]
         L.ref_pcg.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p,
                               _f64p, C.c_int, C.c_double, C.c_double, C.c_double, C.POINTER(C.c_int),
                               C.POINTER(C.c_double), C.c_void_p]
@@ -460,6 +501,32 @@ class Ref:
                                    perm, C.byref(nb), sizes, Ar, Ac, Av)
         return dict(z=z, perm=perm, nblocks=nb.value, sizes=sizes[:nb.value].copy(), A=(Ar, Ac, Av))
 
+    def block_precond_ilup(self, mode, ilu_p, mat_power, row, col, val, r_perm):
+        """lPreconditioner_MultiColoring_ILUp with ILU(ilu_p); mode 3 levels, 4 colours."""
+        n, nnz = len(row) - 1, len(col)
+        z, perm, sizes = np.empty(n), np.empty(n, np.int32), np.empty(n, np.int32)
+        nb = C.c_int()
+        Ar, Ac, Av = np.empty(n + 1, np.int32), np.empty(nnz, np.int32), np.empty(nnz)
+        self.lib.ref_block_precond_ilup(mode, ilu_p, mat_power, n, nnz, _i32(row), _i32(col), _f64(val),
+                                        _f64(r_perm), z, perm, C.byref(nb), sizes, Ar, Ac, Av)
+        return dict(z=z, perm=perm, nblocks=nb.value, sizes=sizes[:nb.value].copy(), A=(Ar, Ac, Av))
+
+    def ilup(self, row, col, val, p, cap=None):
+        n, nnz = len(row) - 1, len(col)
+        cap = cap or 40 * nnz + 16
+        r, c, v = np.empty(n + 1, np.int32), np.empty(cap, np.int32), np.empty(cap)
+        m = self.lib.ref_ilup(n, nnz, _i32(row), _i32(col), _f64(val), p, cap, r, c, v)
+        assert m >= 0
+        return r, c[:m].copy(), v[:m].copy()
+
+    def power_pattern(self, row, col, p, cap=None):
+        n, nnz = len(row) - 1, len(col)
+        cap = cap or 60 * nnz + 16
+        r, c = np.empty(n + 1, np.int32), np.empty(cap, np.int32)
+        m = self.lib.ref_power_pattern(n, nnz, _i32(row), _i32(col), p, cap, r, c)
+        assert m >= 0
+        return r, c[:m].copy()
+
     def pcg(self, row, col, val, b, precond=0, impl=0, nthreads=1, maxits=1000, abstol=0.0,
             reltol=1e-10, divtol=1e6, history=False):
         n = len(row) - 1
@@ -475,12 +542,14 @@ class Ref:
         return out
 
     def gmres(self, row, col, val, b, precond=0, m=30, impl=0, nthreads=1, maxits=1000, abstol=0.0,
-              reltol=1e-9, divtol=1e6):
+              reltol=1e-9, divtol=1e6, ilu_p=0, mat_power=1):
         n = len(row) - 1
         x = np.zeros(n)
         it, res = C.c_int(), C.c_double()
+        self.lib.ref_set_ilup(ilu_p, mat_power)
         conv = self.lib.ref_gmres(precond, impl, nthreads, m, n, len(col), _i32(row), _i32(col), _f64(val),
                                   _f64(b), x, maxits, abstol, reltol, divtol, C.byref(it), C.byref(res))
+        self.lib.ref_set_ilup(0, 1)
         return dict(x=x, iters=it.value, res=res.value, status=conv)
 
     def lmp_cg(self, row, col, val, b, rel_eps=0.0, abs_eps=0.0, max_iter=100):

@@ -245,6 +245,10 @@ int ref_ilu_solve(int n, int nnz, const int *row, const int *col, const double *
 // Build a block preconditioner with the reference class and apply it once.
 // kind 2: MC symmetric Gauss-Seidel; 3: ILU(0) with level scheduling;
 // 4: ILU(0) multicoloured.  r_perm is given in the permuted numbering.
+// ILU(p) parameters of the kind 3 / 4 block preconditioners built below
+// (ref_set_ilup; 0 and 1 give ILU(0) on the operator's own colouring).
+static int g_ilu_p = 0, g_mat_power = 1;
+
 static lPreconditioner_MultiColoring<double> *build_block(int kind, double omega, lMatrix<double> &A,
                                                           lMatrix<double> &Aperm, lVector<double> &x,
                                                           lVector<double> &rhs)
@@ -254,8 +258,8 @@ static lPreconditioner_MultiColoring<double> *build_block(int kind, double omega
         p = new Open<lPreconditioner_MultiColoring_SymmetricGaussSeidel<double>>();
     } else {
         Open<lPreconditioner_MultiColoring_ILUp<double>> *q = new Open<lPreconditioner_MultiColoring_ILUp<double>>();
-        if (kind == 3) q->Init(0, 1, false, false, true);
-        else q->Init(0, 1, true, true, false);
+        if (kind == 3) q->Init(g_ilu_p, 1, false, false, true);
+        else q->Init(g_ilu_p, g_mat_power, true, true, false);
         p = q;
     }
     p->SetupOperator(A);
@@ -297,6 +301,74 @@ int ref_block_precond(int kind, double omega, int n, int nnz, const int *row, co
     copy_out(*vz, z_perm);
     delete p; delete A; delete Ap; delete x; delete rhs; delete vr; delete vz;
     return 0;
+}
+
+// lPreconditioner_MultiColoring_ILUp with ILU(ilu_p) and the colouring on the
+// pattern of A^mat_power; mode 3 level scheduling, mode 4 multicolouring.
+int ref_block_precond_ilup(int mode, int ilu_p, int mat_power, int n, int nnz, const int *row, const int *col,
+                           const double *val, const double *r_perm, double *z_perm, int *perm, int *nblocks,
+                           int *sizes, int *Ap_row, int *Ap_col, double *Ap_val)
+{
+    lMatrix<double> *A = make_matrix(0, n, nnz, row, col, val, 1);
+    lMatrix<double> *Ap = make_matrix(0, n, nnz, row, col, val, 1);
+    lVector<double> *x = make_vector(0, n, nullptr, 1), *rhs = make_vector(0, n, nullptr, 1);
+    Open<lPreconditioner_MultiColoring_ILUp<double>> *q = new Open<lPreconditioner_MultiColoring_ILUp<double>>();
+    if (mode == 3) q->Init(ilu_p, mat_power, false, false, true);
+    else q->Init(ilu_p, mat_power, true, true, false);
+    q->SetupOperator(*A);
+    q->SetupPermOperator(*Ap);
+    q->SetupPermVectors(x, rhs);
+    q->Build();
+    std::memcpy(perm, q->get_permut(), sizeof(int) * n);
+    block_info(4, q, nblocks, sizes);
+    csr_out(*Ap, Ap_row, Ap_col, Ap_val);
+    lVector<double> *vr = make_vector(0, n, r_perm, 1), *vz = make_vector(0, n, nullptr, 1);
+    q->ApplylPreconditioner(*vr, vz);
+    copy_out(*vz, z_perm);
+    delete q; delete A; delete Ap; delete x; delete rhs; delete vr; delete vz;
+    return 0;
+}
+
+void ref_set_ilup(int ilu_p, int mat_power)
+{
+    g_ilu_p = ilu_p;
+    g_mat_power = mat_power;
+}
+
+// CPU_CSR_lMatrix::ilup (lmatrix_csr_cpu.cc:1933-1952); returns nnz of the
+// factors, -1 if cap is too small.
+int ref_ilup(int n, int nnz, const int *row, const int *col, const double *val, int p, int cap, int *row_out,
+             int *col_out, double *val_out)
+{
+    CPUsimple_CSR_lMatrix<double> A(nnz, n, n, "A");
+    std::memcpy(A.matrix.row, row, sizeof(int) * (n + 1));
+    std::memcpy(A.matrix.col, col, sizeof(int) * nnz);
+    std::memcpy(A.matrix.val, val, sizeof(double) * nnz);
+    A.ilup(p);
+    const int m = A.get_nnz();
+    if (m > cap) return -1;
+    std::memcpy(row_out, A.matrix.row, sizeof(int) * (n + 1));
+    std::memcpy(col_out, A.matrix.col, sizeof(int) * m);
+    std::memcpy(val_out, A.matrix.val, sizeof(double) * m);
+    return m;
+}
+
+// CPU_CSR_lMatrix::MatrixSupSPower (lmatrix_csr_cpu.cc:1641-1664).
+int ref_power_pattern(int n, int nnz, const int *row, const int *col, int p, int cap, int *row_out, int *col_out)
+{
+    CPUsimple_CSR_lMatrix<double> A(nnz, n, n, "A");
+    std::memcpy(A.matrix.row, row, sizeof(int) * (n + 1));
+    std::memcpy(A.matrix.col, col, sizeof(int) * nnz);
+    for (int j = 0; j < nnz; ++j) A.matrix.val[j] = 1.0;
+    lMatrix<double> *P = A.MatrixSupSPower(p);
+    CPU_CSR_lMatrix<double> *c = dynamic_cast<CPU_CSR_lMatrix<double> *>(P);
+    const int m = c->get_nnz();
+    if (m <= cap) {
+        std::memcpy(row_out, c->matrix.row, sizeof(int) * (n + 1));
+        std::memcpy(col_out, c->matrix.col, sizeof(int) * m);
+    }
+    delete P;
+    return m <= cap ? m : -1;
 }
 
 // CG<LAD>::SolvePrecond / SolveNoPrecond restated over lmp objects
