@@ -152,6 +152,8 @@ def lib():
         "b200la_scatter": ([_P, _I, _I, _P, _P, _P], _I),
         "b200la_permute": ([_P, _I, _I, _P, _P, _P], _I),
         "b200la_coo_to_csr": ([_I, _I, _P, _P, _P, _P, _P, _P], _I),
+        "b200la_async_jacobi": ([_P, _P, _P, _P, _P, _P, _I, _I, C.c_double, C.POINTER(Control), C.POINTER(Result)],
+                                _I),
         "b200la_gmg_residual": ([_P, _P, _P, _P, _P, _P, _P], _I),
         "b200la_gmg_restriction": ([_P, _P, _P, _P, _P, _P], _I),
         "b200la_gmg_prolongation_add": ([_P, _P, _P, _P, _P, _P], _I),
@@ -671,6 +673,16 @@ def gmg_prolongation_add(pf, P_diag, res, sol, P_offdiag=None, res_ghost=None):
     """sol += P_diag res + P_offdiag res_ghost."""
     pf.check(lib().b200la_gmg_prolongation_add(pf.h, P_diag.h, _h(P_offdiag), res.ptr, _vp(res_ghost), sol.ptr),
              "gmg_prolongation_add")
+
+
+def async_jacobi(pf, A, b, x, n_inner=10, n_block=10, w=1.0, maxits=100000, abstol=0.0, reltol=1e-8, divtol=1e6,
+                 A_offdiag=None, x_ghost=None):
+    """Asynchronous block-Jacobi solve (AsynchronousIterationGPU); returns a dict
+    with iters (sweeps), status, res0, res."""
+    ctl, res = Control(maxits, abstol, reltol, divtol), Result()
+    pf.check(lib().b200la_async_jacobi(pf.h, A.h, _h(A_offdiag), b.ptr, x.ptr, _vp(x_ghost), n_inner, n_block, w,
+                                       C.byref(ctl), C.byref(res)), "async_jacobi")
+    return dict(iters=res.iters, status=res.status, res0=res.res0, res=res.res, launches=res.launches)
 
 
 class Preconditioner:

@@ -316,6 +316,20 @@ int b200la_mpir_gmres(b200la_ctx *ctx, const b200la_csr *A64, const b200la_csr *
                       int m, const double *b, double *x, const b200la_control *outer, const b200la_control *inner,
                       int max_outer, b200la_result *res);
 
+/* Asynchronous block-Jacobi iteration (src/linear_solver/gpu-based/async_iter_gpu.cc:538-943,
+ * kernels lmp/cuda/cuda_async_iter_kernels.h): batches of n_block launches,
+ * each updating every row n_inner times,
+ *   x_i <- D_ii^-1 (b_i - sum_{j != i} A_ij x_j - sum_g O_ig x_ghost_g)
+ * (w != 1: x_i <- w * that + (1 - w) x_i), rows reading their neighbours'
+ * current values with no barrier, then ||b - A x - O x_ghost|| and
+ * IterateControl::Check (iterations counted in sweeps).  A square with a
+ * nonzero diagonal; A_offdiag and x_ghost optional (NULL on one rank; the
+ * ghost values stay fixed during the call).  The iterates are not reproducible
+ * bit for bit (asynchronous by design); the stop decision is. */
+int b200la_async_jacobi(b200la_ctx *ctx, const b200la_csr *A, const b200la_csr *A_offdiag, const void *b, void *x,
+                        const void *x_ghost, int n_inner, int n_block, double w, const b200la_control *ctl,
+                        b200la_result *res);
+
 /* ---------------------------------------------------------------- file I/O */
 /* Host arrays.  MatrixMarket matrices: replaces CPU_CSR_lMatrix::ReadFile / WriteFile
  * (lmp/lmatrix_csr_cpu.cc:1733-1765) over CPU_COO_lMatrix::ReadFile /
