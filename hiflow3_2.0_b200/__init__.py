@@ -157,6 +157,7 @@ def lib():
         "b200la_gmg_residual": ([_P, _P, _P, _P, _P, _P, _P], _I),
         "b200la_gmg_restriction": ([_P, _P, _P, _P, _P, _P], _I),
         "b200la_gmg_prolongation_add": ([_P, _P, _P, _P, _P, _P], _I),
+        "b200la_rowblock_split": ([_I, _I, _P, _P, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P, _P], _I),
         "b200la_mm_read_info": ([C.c_char_p, _P, _P, _P], _I),
         "b200la_mm_read_csr": ([C.c_char_p, _I, _I, _P, _P, _P], _I),
         "b200la_mm_write_csr": ([C.c_char_p, _I, _I, _I, _P, _P, _P], _I),
@@ -358,6 +359,23 @@ def ilu0(row, col, val):
     row, col, v = _i32(row), _i32(col), _f64(val).copy()
     _check(lib().b200la_ilu0(row.size - 1, _np_ptr(row), _np_ptr(col), _np_ptr(v)), "ilu0")
     return v
+
+
+def rowblock_split(row, col, val, n_global, col_begin, col_end):
+    """The rows of one rank split into (diag CSR, offdiag CSR, ghost global
+    numbers): CoupledMatrix::InitStructure with LaCouplings' ghost numbering."""
+    row, col, val = _i32(row), _i32(col), _f64(val)
+    n = row.size - 1
+    nd, no, ng = C.c_int(), C.c_int(), C.c_int()
+    args = (n, n_global, _np_ptr(row), _np_ptr(col), _np_ptr(val), col_begin, col_end)
+    _check(lib().b200la_rowblock_split(*args, C.byref(nd), C.byref(no), C.byref(ng), *([None] * 7)), "rowblock_split")
+    rd, cd, vd = np.empty(n + 1, np.int32), np.empty(nd.value, np.int32), np.empty(nd.value)
+    ro, co, vo = np.empty(n + 1, np.int32), np.empty(no.value, np.int32), np.empty(no.value)
+    g = np.empty(ng.value, np.int32)
+    _check(lib().b200la_rowblock_split(*args, C.byref(nd), C.byref(no), C.byref(ng), _np_ptr(rd), _np_ptr(cd),
+                                       _np_ptr(vd), _np_ptr(ro), _np_ptr(co), _np_ptr(vo), _np_ptr(g)),
+           "rowblock_split")
+    return (rd, cd, vd), (ro, co, vo), g
 
 
 def matrix_power_pattern(row, col, p):

@@ -1,0 +1,328 @@
+"""Row-block distributed vectors and matrices over several GPUs (one rank per GPU).
+
+The B200 counterpart of HiFlow3's CoupledVector / CoupledMatrix / LaCouplings
+(src/linear_algebra/coupled_vector.cc, coupled_matrix.cc, la_couplings.cc):
+- every rank owns a contiguous block of rows (``offsets``);
+- its matrix rows are split into the diagonal block (owned columns) and the
+  off-diagonal block (ghost columns), b200la_rowblock_split;
+- a vector holds its owned values (interior) and a ghost buffer; UpdateGhost
+  packs the border values every peer needs with the gather kernel and moves
+  them peer to peer (the reference's Isend/Irecv pair, coupled_vector.cc:975-1128);
+- dot products and norms reduce the local value across ranks (the reference's
+  MPI_Allreduce, coupled_vector.cc:331-436).
+
+Transports: ``DistTransport`` over torch.distributed (NCCL for device tensors
+between GPUs, gloo for host tensors) and ``LocalTransport``, several ranks in
+one process (threads, one per rank, sharing a mailbox), which lets ranks share
+a GPU.  No collective here waits inside a kernel: exchanges are host-ordered
+stream operations, so ranks on one GPU cannot deadlock one another.
+
+Only host logic (partition, couplings set-up, exchange protocol) runs without
+a GPU; vectors and matrices live on the device and compute with the
+platform's kernels, with no host fallback.
+"""
+import ctypes as C
+import threading
+
+import numpy as np
+
+from . import CSR_lMatrix, F64, Control, lib, rowblock_split
+
+__all__ = ["RowPartition", "LaCouplings", "DistTransport", "LocalTransport", "CoupledVector", "CoupledMatrix",
+           "CoupledCG", "exchange"]
+
+
+class RowPartition:
+    """Owner ranges: rank r owns global rows [offsets[r], offsets[r+1])."""
+
+    def __init__(self, offsets):
+        self.offsets = np.asarray(offsets, np.int64)
+        assert self.offsets[0] == 0 and np.all(np.diff(self.offsets) >= 0)
+
+    @classmethod
+    def even(cls, n, size):
+        return cls([n * r // size for r in range(size + 1)])
+
+    def owner(self, g):
+        return np.searchsorted(self.offsets, np.asarray(g), side="right") - 1
+
+    def range(self, rank):
+        return int(self.offsets[rank]), int(self.offsets[rank + 1])
+
+
+# ---------------------------------------------------------------- transports
+
+class DistTransport:
+    """torch.distributed (initialised process group) as the transport."""
+
+    def __init__(self, group=None):
+        import torch.distributed as dist
+        self.dist, self.group = dist, group
+        self.rank, self.size = dist.get_rank(group), dist.get_world_size(group)
+
+    def alltoall_lists(self, lists):
+        """lists[q] -> peer q; returns what every peer sent to this rank."""
+        allv = [None] * self.size
+        self.dist.all_gather_object(allv, [list(map(int, x)) for x in lists], group=self.group)
+        return [np.asarray(allv[q][self.rank], np.int64) for q in range(self.size)]
+
+    def exchange(self, sends, recvs):
+        """sends / recvs: {peer: tensor}; point-to-point, all posted together."""
+        ops = [self.dist.P2POp(self.dist.irecv, t, q, self.group) for q, t in recvs.items() if t.numel()]
+        ops += [self.dist.P2POp(self.dist.isend, t, q, self.group) for q, t in sends.items() if t.numel()]
+        if ops:
+            for w in self.dist.batch_isend_irecv(ops):
+                w.wait()
+        # the platform's kernels run on their own stream: finish the transfers first
+        if any(t.is_cuda for t in list(sends.values()) + list(recvs.values())):
+            import torch
+            torch.cuda.current_stream().synchronize()
+
+    def allreduce_sum(self, value, device):
+        import torch
+        t = torch.tensor([value], dtype=torch.float64, device=device)
+        self.dist.all_reduce(t, group=self.group)
+        return float(t.item())
+
+
+class _Fabric:
+    """Mailboxes and a barrier shared by the ranks of one LocalTransport."""
+
+    def __init__(self, size):
+        self.size = size
+        self.barrier = threading.Barrier(size)
+        self.box = {}
+
+
+class LocalTransport:
+    """Ranks of one process (one thread per rank).  Create all ranks' transports
+    from one ``LocalTransport.group(size)`` call."""
+
+    def __init__(self, fabric, rank):
+        self.f, self.rank, self.size = fabric, rank, fabric.size
+
+    @classmethod
+    def group(cls, size):
+        fab = _Fabric(size)
+        return [cls(fab, r) for r in range(size)]
+
+    def alltoall_lists(self, lists):
+        for q in range(self.size):
+            self.f.box[("a2a", self.rank, q)] = np.asarray(lists[q], np.int64)
+        self.f.barrier.wait()
+        out = [self.f.box[("a2a", q, self.rank)] for q in range(self.size)]
+        self.f.barrier.wait()
+        return out
+
+    def exchange(self, sends, recvs):
+        import torch
+        for q, t in sends.items():
+            self.f.box[("p2p", self.rank, q)] = t
+        # the senders' streams must have produced their buffers before anyone copies
+        torch.cuda.synchronize() if any(t.is_cuda for t in sends.values()) else None
+        self.f.barrier.wait()
+        for q, t in recvs.items():
+            if t.numel():
+                t.copy_(self.f.box[("p2p", q, self.rank)])
+        if any(t.is_cuda for t in recvs.values()):
+            torch.cuda.synchronize()
+        self.f.barrier.wait()
+
+    def allreduce_sum(self, value, device=None):
+        self.f.box[("sum", self.rank)] = float(value)
+        self.f.barrier.wait()
+        tot = 0.0
+        for q in range(self.size):   # every rank adds in the same order
+            tot += self.f.box[("sum", q)]
+        self.f.barrier.wait()
+        return tot
+
+
+def exchange(transport, couplings, border_values, ghost_values):
+    """Move border values (ordered by peer, couplings.border_offsets) into the
+    peers' ghost buffers (ordered by owner, couplings.ghost_offsets)."""
+    sends, recvs = {}, {}
+    for q in range(transport.size):
+        b0, b1 = couplings.border_offsets[q], couplings.border_offsets[q + 1]
+        g0, g1 = couplings.ghost_offsets[q], couplings.ghost_offsets[q + 1]
+        if b1 > b0:
+            sends[q] = border_values[b0:b1]
+        if g1 > g0:
+            recvs[q] = ghost_values[g0:g1]
+    transport.exchange(sends, recvs)
+
+
+class LaCouplings:
+    """Ghost and border index sets of one rank (la_couplings.cc:62-230).
+
+    ghost_global: ascending global numbers of the ghost columns; grouped by
+    owner (owners hold contiguous ranges), ghost_offsets[q] marks owner q's
+    part.  border_indices: local numbers of owned values that peers need,
+    grouped by peer (border_offsets), in the order the peer lists its ghosts.
+    """
+
+    def __init__(self, partition, rank, ghost_global):
+        self.part, self.rank = partition, rank
+        self.ghost_global = np.asarray(ghost_global, np.int64)
+        owners = partition.owner(self.ghost_global) if self.ghost_global.size else np.zeros(0, np.int64)
+        if np.any(owners == rank):
+            raise ValueError("a ghost column is owned by this rank")
+        size = len(partition.offsets) - 1
+        self.ghost_offsets = np.searchsorted(owners, np.arange(size + 1), side="left").astype(np.int64)
+        self.border_indices = None
+        self.border_offsets = None
+
+    def setup(self, transport):
+        """Exchange the ghost lists: what this rank needs from every owner, and
+        what every peer needs from this rank (its border)."""
+        size = transport.size
+        need = [self.ghost_global[self.ghost_offsets[q]:self.ghost_offsets[q + 1]] for q in range(size)]
+        got = transport.alltoall_lists(need)
+        r0, _ = self.part.range(self.rank)
+        self.border_offsets = np.zeros(size + 1, np.int64)
+        for q in range(size):
+            self.border_offsets[q + 1] = self.border_offsets[q] + len(got[q])
+        self.border_indices = (np.concatenate(got) - r0).astype(np.int32) if size else np.zeros(0, np.int32)
+        return self
+
+
+# ------------------------------------------------------------ device objects
+
+class CoupledVector:
+    """Owned values (an lVector on this rank's GPU) plus a ghost buffer."""
+
+    def __init__(self, platform, couplings, transport, data_or_n, dtype=F64):
+        import torch
+        self.pf, self.cp, self.tr, self.dtype = platform, couplings, transport, dtype
+        self.interior = platform.vector(data_or_n, dtype)
+        td = torch.float64 if dtype == F64 else torch.float32
+        dev = f"cuda:{platform.device}"
+        self.ghost = torch.zeros(len(couplings.ghost_global), dtype=td, device=dev)
+        self.border = torch.zeros(len(couplings.border_indices), dtype=td, device=dev)
+        self._bidx = torch.from_numpy(couplings.border_indices.astype(np.int32)).to(dev)
+
+    def clone_without_content(self):
+        return CoupledVector(self.pf, self.cp, self.tr, self.interior.get_size(), self.dtype)
+
+    def UpdateGhost(self):
+        """Pack the border with the gather kernel, then the peer exchange."""
+        nb = self.border.numel()
+        if nb:
+            self.pf.check(lib().b200la_gather(self.pf.h, self.dtype, nb, C.c_void_p(self._bidx.data_ptr()),
+                                              self.interior.ptr, C.c_void_p(self.border.data_ptr())), "gather")
+        self.pf.sync()
+        exchange(self.tr, self.cp, self.border, self.ghost)
+
+    # global reductions (local kernel, then the sum across ranks)
+    def Dot(self, other):
+        return self.tr.allreduce_sum(self.interior.Dot(other.interior), f"cuda:{self.pf.device}")
+
+    def Norm2(self):
+        return float(np.sqrt(self.Dot(self)))
+
+    # local BLAS1 (coupled_vector.cc:331-436 forward to the interior)
+    def Axpy(self, v, a):
+        self.interior.Axpy(v.interior, a)
+
+    def ScaleAdd(self, a, v):
+        self.interior.ScaleAdd(a, v.interior)
+
+    def Scale(self, a):
+        self.interior.Scale(a)
+
+    def CopyFrom(self, v):
+        self.interior.CopyFrom(v.interior)
+
+    def Zeros(self):
+        self.interior.Zeros()
+
+    def numpy(self):
+        return self.interior.numpy()
+
+
+class CoupledMatrix:
+    """Diagonal and off-diagonal blocks of this rank's rows on its GPU."""
+
+    def __init__(self, platform, partition, rank, transport, row, col, val, dtype=F64):
+        """row/col/val: this rank's rows (CSR) with global column numbers."""
+        n_global = int(partition.offsets[-1])
+        r0, r1 = partition.range(rank)
+        (rd, cd, vd), (ro, co, vo), ghosts = rowblock_split(row, col, val, n_global, r0, r1)
+        self.pf, self.part, self.rank, self.tr = platform, partition, rank, transport
+        self.couplings = LaCouplings(partition, rank, ghosts).setup(transport)
+        self.n_local = r1 - r0
+        self.diag = CSR_lMatrix.from_csr(platform, rd, cd, vd, n_cols=self.n_local, dtype=dtype)
+        self.offdiag = (CSR_lMatrix.from_csr(platform, ro, co, vo, n_cols=len(ghosts), dtype=dtype)
+                        if len(co) else None)
+        self.dtype = dtype
+
+    def vector(self, data_or_n=None):
+        return CoupledVector(self.pf, self.couplings, self.tr,
+                             self.n_local if data_or_n is None else data_or_n, self.dtype)
+
+    def VectorMult(self, x, y):
+        """y = A x: the ghost update, the diagonal block, the off-diagonal block
+        (coupled_matrix.cc:433-467)."""
+        x.UpdateGhost()
+        self.diag.VectorMult(x.interior, y.interior)
+        if self.offdiag is not None:
+            lib().b200la_spmv_add(self.pf.h, self.offdiag.h, C.c_void_p(x.ghost.data_ptr()), y.interior.ptr)
+
+
+class CoupledCG:
+    """CG<LAD>::Solve (src/linear_solver/cg.cc:84-248) on coupled objects, with
+    the block-Jacobi (diagonal) preconditioner of the local block or none."""
+
+    def __init__(self, A, jacobi=True):
+        self.A, self.jacobi = A, jacobi
+        self.iter, self.res, self.res0 = 0, 0.0, 0.0
+        if jacobi:
+            self.invd = A.vector()
+            A.pf.check(lib().b200la_csr_invdiag(A.pf.h, A.diag.h, self.invd.interior.ptr), "invdiag")
+
+    def Solve(self, b, x, maxits=10000, abstol=0.0, reltol=1e-10, divtol=1e6):
+        A = self.A
+        r, p, z, Ap = (A.vector() for _ in range(4))
+        A.VectorMult(x, r)                       # r = b - A x
+        r.ScaleAdd(-1.0, b)
+        res = r.Norm2()
+        self.res0 = res
+        ctl = Control(maxits, abstol, reltol, divtol)
+
+        def check(it, v):
+            # IterateControl::Check (src/common/iterate_control.cc:84-110)
+            if v < ctl.abstol:
+                return 1
+            if v < ctl.reltol * self.res0:
+                return 2
+            if v > ctl.divtol * self.res0:
+                return 3
+            if it >= ctl.maxits:
+                return 4
+            return 0
+
+        def precond(src, dst):
+            dst.CopyFrom(src)
+            if self.jacobi:
+                dst.interior.ElementWiseMult(self.invd.interior)
+
+        status, it = check(0, res), 0
+        precond(r, z)
+        p.CopyFrom(z)
+        rho = r.Dot(z)
+        while status == 0:
+            it += 1
+            A.VectorMult(p, Ap)
+            alpha = rho / Ap.Dot(p)
+            x.Axpy(p, alpha)
+            r.Axpy(Ap, -alpha)
+            res = r.Norm2()
+            status = check(it, res)
+            if status:
+                break
+            precond(r, z)
+            rho_new = r.Dot(z)
+            p.ScaleAdd(rho_new / rho, z)         # p = beta p + z
+            rho = rho_new
+        self.iter, self.res = it, res
+        return status

@@ -1122,6 +1122,58 @@ extern "C" int b200la_ilup(int n, const int *row, const int *col, const double *
     return host_csr_out(LU, nnz, row_out, col_out, val_out);
 }
 
+extern "C" int b200la_rowblock_split(int n_rows, int n_global, const int *row, const int *col, const double *val,
+                                     int col_begin, int col_end, int *nnz_diag, int *nnz_offdiag, int *n_ghost,
+                                     int *row_d, int *col_d, double *val_d, int *row_o, int *col_o, double *val_o,
+                                     int *ghost_global)
+{
+    // CoupledMatrix::InitStructure (coupled_matrix.cc:253-340) with the ghost
+    // numbering of LaCouplings::InitializeCouplings (la_couplings.cc:62-130):
+    // owned columns shifted to local numbering, the others numbered by their
+    // rank among the distinct ghost columns in ascending order (per owner in
+    // ascending order, owners being contiguous ranges)
+    if (n_rows < 0 || !row || !nnz_diag || !nnz_offdiag || !n_ghost || col_begin < 0 || col_end < col_begin ||
+        col_end > n_global)
+        return B200LA_ERR_ARG;
+    long long bad = -1;
+    if (host::validate_csr(n_rows, n_global, row[n_rows], row, col, &bad)) return B200LA_ERR_CSR;
+    std::vector<int> ghosts;
+    int nd = 0, no = 0;
+    for (int j = 0; j < row[n_rows]; ++j) {
+        if (col[j] >= col_begin && col[j] < col_end) ++nd;
+        else {
+            ++no;
+            ghosts.push_back(col[j]);
+        }
+    }
+    std::sort(ghosts.begin(), ghosts.end());
+    ghosts.erase(std::unique(ghosts.begin(), ghosts.end()), ghosts.end());
+    *nnz_diag = nd;
+    *nnz_offdiag = no;
+    *n_ghost = (int)ghosts.size();
+    if (!row_d) return B200LA_OK;
+    if (!row_o || (nd && (!col_d || !val_d || !val)) || (no && (!col_o || !val_o)) || (!ghosts.empty() && !ghost_global))
+        return B200LA_ERR_ARG;
+    int td = 0, to = 0;
+    row_d[0] = row_o[0] = 0;
+    for (int i = 0; i < n_rows; ++i) {
+        for (int j = row[i]; j < row[i + 1]; ++j) {
+            const int c = col[j];
+            if (c >= col_begin && c < col_end) {
+                col_d[td] = c - col_begin;
+                val_d[td++] = val[j];
+            } else {
+                col_o[to] = (int)(std::lower_bound(ghosts.begin(), ghosts.end(), c) - ghosts.begin());
+                val_o[to++] = val[j];
+            }
+        }
+        row_d[i + 1] = td;
+        row_o[i + 1] = to;
+    }
+    std::copy(ghosts.begin(), ghosts.end(), ghost_global);
+    return B200LA_OK;
+}
+
 extern "C" int b200la_q1_sizes(int dim, int N, int *n, int64_t *nnz)
 {
     if (!n || !nnz) return B200LA_ERR_ARG;

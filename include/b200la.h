@@ -330,6 +330,19 @@ int b200la_async_jacobi(b200la_ctx *ctx, const b200la_csr *A, const b200la_csr *
                         const void *x_ghost, int n_inner, int n_block, double w, const b200la_control *ctl,
                         b200la_result *res);
 
+/* ------------------------------------------------------ row-block coupling */
+/* The rows of one rank (n_rows, global column numbers) split into the
+ * diagonal block (columns in [col_begin, col_end), shifted to local numbers)
+ * and the off-diagonal block (columns numbered by their rank among the distinct
+ * ghost columns, ascending), with the ghosts' global numbers: replaces
+ * CoupledMatrix::InitStructure (coupled_matrix.cc:253-340) with the ghost
+ * numbering of LaCouplings::InitializeCouplings (la_couplings.cc:62-130).
+ * Entry order within a row is kept.  Two-call: sizes first (row_d NULL),
+ * then row_d/row_o (n_rows + 1), col/val of each block, ghost_global. */
+int b200la_rowblock_split(int n_rows, int n_global, const int *row, const int *col, const double *val, int col_begin,
+                          int col_end, int *nnz_diag, int *nnz_offdiag, int *n_ghost, int *row_d, int *col_d,
+                          double *val_d, int *row_o, int *col_o, double *val_o, int *ghost_global);
+
 /* ---------------------------------------------------------------- file I/O */
 /* Host arrays.  MatrixMarket matrices: replaces CPU_CSR_lMatrix::ReadFile / WriteFile
  * (lmp/lmatrix_csr_cpu.cc:1733-1765) over CPU_COO_lMatrix::ReadFile /

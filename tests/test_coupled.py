@@ -1,0 +1,166 @@
+"""Row-block distributed objects (hiflow3_2.0_b200/coupled.py).
+
+CPU (gloo, world sizes 2 and 3, spawned processes): the host logic of the
+multi-GPU layer -- the row-block split, the couplings set-up (which values
+every peer needs) and the peer exchange over torch.distributed -- checked
+with host tensors and a numpy product of the local blocks against the global
+product.  GPU: the device objects (gather kernel, block SpMVs, coupled CG)
+with several ranks as threads sharing one GPU (LocalTransport), against the
+single-rank solve.
+"""
+import os
+import sys
+import threading
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+
+def _spmv_np(row, col, val, x):
+    y = np.zeros(len(row) - 1)
+    for i in range(len(row) - 1):
+        y[i] = val[row[i]:row[i + 1]] @ x[col[row[i]:row[i + 1]]]
+    return y
+
+
+def _system():
+    from conftest import load_platform
+    b200 = load_platform()
+    row, col, val = b200.q1_assemble(2, 9, 1, None, 1e-2, (1.0, 0.5))
+    return b200, row, col, val
+
+
+def _gloo_worker(rank, world, port, q):
+    import torch
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import importlib
+        b200, row, col, val = _system()
+        cp = importlib.import_module("hiflow3_b200.coupled")
+        n = len(row) - 1
+        part = cp.RowPartition.even(n, world)
+        r0, r1 = part.range(rank)
+        lr = row[r0:r1 + 1] - row[r0]
+        lc, lv = col[row[r0]:row[r1]], val[row[r0]:row[r1]]
+        (rd, cd, vd), (ro, co, vo), ghosts = b200.rowblock_split(lr, lc, lv, n, r0, r1)
+        tr = cp.DistTransport()
+        cpl = cp.LaCouplings(part, rank, ghosts).setup(tr)
+        x = np.cos(np.arange(n) * 0.37)              # the global x, each rank keeps its own part
+        xi = torch.from_numpy(x[r0:r1].copy())
+        border = xi[torch.from_numpy(cpl.border_indices.astype(np.int64))]
+        ghost = torch.zeros(len(ghosts), dtype=torch.float64)
+        cp.exchange(tr, cpl, border, ghost)
+        y = _spmv_np(rd, cd, vd, x[r0:r1]) + (_spmv_np(ro, co, vo, ghost.numpy()) if len(co) else 0.0)
+        dot = tr.allreduce_sum(float(xi @ xi), "cpu")
+        q.put((rank, r0, y, ghost.numpy().copy(), ghosts.copy(), dot))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_rowblock_spmv_over_gloo(world):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29500 + os.getpid() % 400 + world
+    procs = [ctx.Process(target=_gloo_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = [q.get(timeout=180) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    b200, row, col, val = _system()
+    n = len(row) - 1
+    x = np.cos(np.arange(n) * 0.37)
+    y_global = _spmv_np(row, col, val, x)
+    for rank, r0, y, ghost, ghosts, dot in got:
+        assert np.array_equal(ghost, x[ghosts])                       # every ghost holds the owner's value
+        assert np.allclose(y, y_global[r0:r0 + len(y)], rtol=0, atol=1e-13 * np.abs(val).max())
+        assert abs(dot - x @ x) <= 1e-12 * (x @ x)
+
+
+def test_rowblock_split_blocks(b200):
+    row, col, val = b200.q1_assemble(2, 6, 0)
+    n = len(row) - 1
+    r0, r1 = 10, 30
+    lr = row[r0:r1 + 1] - row[r0]
+    lc, lv = col[row[r0]:row[r1]], val[row[r0]:row[r1]]
+    (rd, cd, vd), (ro, co, vo), g = b200.rowblock_split(lr, lc, lv, n, r0, r1)
+    assert np.all(np.diff(g) > 0) and not np.any((g >= r0) & (g < r1))
+    for i in range(r1 - r0):
+        full = dict(zip(lc[lr[i]:lr[i + 1]], lv[lr[i]:lr[i + 1]]))
+        got = {c + r0: v for c, v in zip(cd[rd[i]:rd[i + 1]], vd[rd[i]:rd[i + 1]])}
+        got.update({g[c]: v for c, v in zip(co[ro[i]:ro[i + 1]], vo[ro[i]:ro[i + 1]])})
+        assert got == full
+
+
+def _run_ranks(world, fn):
+    out, errs = [None] * world, []
+
+    def body(r):
+        try:
+            out[r] = fn(r)
+        except BaseException as e:   # surfaced below
+            errs.append(e)
+
+    th = [threading.Thread(target=body, args=(r,)) for r in range(world)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=300)
+    if errs:
+        raise errs[0]
+    return out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [2, 3])
+def test_coupled_cg_ranks_on_one_gpu(b200, world):
+    import importlib
+    cp = importlib.import_module("hiflow3_b200.coupled")
+    row, col, val = b200.q1_assemble(2, 40, 0, np.exp(np.random.default_rng(1).standard_normal(1600)))
+    n = len(row) - 1
+    b = b200.q1_rhs(4, 2, 40)
+    # the single-rank Jacobi-PCG
+    pf0 = b200.Platform(0)
+    A = b200.CSR_lMatrix.from_csr(pf0, row, col, val)
+    cg = b200.CG(pf0)
+    cg.SetupOperator(A)
+    cg.SetupPreconditioner(b200.Preconditioner.Jacobi(pf0, A))
+    cg.InitControl(5000, 0.0, 1e-10, 1e6)
+    x0 = pf0.vector(n)
+    assert cg.Solve(pf0.vector(b), x0) == b200.SUCCESS_REL
+    it0, xs = cg.iter(), x0.numpy()
+    part = cp.RowPartition.even(n, world)
+    trs = cp.LocalTransport.group(world)
+
+    def rank_fn(r):
+        pf = b200.Platform(0)
+        r0, r1 = part.range(r)
+        lr = row[r0:r1 + 1] - row[r0]
+        M = cp.CoupledMatrix(pf, part, r, trs[r], lr, col[row[r0]:row[r1]], val[row[r0]:row[r1]])
+        xv = np.sin(np.arange(n) * 0.11)
+        # the coupled product equals the global one on this rank's rows
+        xc, yc = M.vector(xv[r0:r1]), M.vector()
+        M.VectorMult(xc, yc)
+        y_rows = yc.numpy()
+        solver = cp.CoupledCG(M)
+        x = M.vector()
+        st = solver.Solve(M.vector(b[r0:r1]), x, maxits=5000, reltol=1e-10)
+        return r0, y_rows, st, solver.iter, x.numpy()
+
+    res = _run_ranks(world, rank_fn)
+    xv = np.sin(np.arange(n) * 0.11)
+    y_global = _spmv_np(row, col, val, xv)
+    for r0, y_rows, st, it, x in res:
+        assert np.allclose(y_rows, y_global[r0:r0 + len(y_rows)], rtol=0, atol=1e-12 * np.abs(y_global).max())
+        assert st == b200.SUCCESS_REL
+        assert abs(it - it0) <= max(1, 0.05 * it0), (it, it0)
+        assert np.linalg.norm(x - xs[r0:r0 + len(x)]) <= 1e-8 * np.linalg.norm(xs)
