@@ -189,6 +189,29 @@ __global__ void __launch_bounds__(kBlock, MINB) spmv_tile_kernel(CsrView A, Seg 
     }
 }
 
+
+// 16-byte streaming loads (L1 bypassed, L2 evict-first hint)
+__device__ __forceinline__ void ld_stream_vec(const double *a, uint64_t pol, double (&v)[2])
+{
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+        : "=d"(v[0]), "=d"(v[1]) : "l"(a), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream_vec(const float *a, uint64_t pol, float (&v)[4])
+{
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(a), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream_vec(const int *a, uint64_t pol, int (&v)[2])
+{
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
+        : "=r"(v[0]), "=r"(v[1]) : "l"(a), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream_vec(const int *a, uint64_t pol, int (&v)[4])
+{
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "l"(a), "l"(pol));
+}
+
 template <typename T, int EPI>
 __global__ void __launch_bounds__(kBlock) spmv_direct_kernel(CsrView A, Seg seg, SpmvOp op, Scratch sc)
 {
@@ -209,12 +232,24 @@ __global__ void __launch_bounds__(kBlock) spmv_direct_kernel(CsrView A, Seg seg,
         T s = T(0);
         if (active) {
             const int j0 = __ldg(row + r), j1 = __ldg(row + r + 1);
-            // the group's G-element windows start on a multiple of G, so each
-            // window is one aligned segment (a 32-byte sector for 4 doubles);
-            // elements outside the row are masked
-#pragma unroll 4
-            for (int j = (j0 & ~(G - 1)) + lane_g; j < j1; j += G)
-                if (j >= j0) s += ld_stream(val + j, pol_s) * ld_keep(x + ld_stream(col + j, pol_s), pol_x);
+            // 16-byte loads: E values and E column indices per lane per step,
+            // the group's windows of E * G elements aligned to their size,
+            // elements outside the row masked (the arrays are
+            // padded by 8 entries past nnz, so a window never leaves the
+            // allocation).  No unrolling: measured on B200 (128^3 Q1, FP64)
+            // 145 us against 158 us unrolled by 2 and 166 us for 8-byte loads.
+            constexpr int E = 16 / (int)sizeof(T);
+            const int W = E * G;
+#pragma unroll 1
+            for (int j = (j0 & ~(W - 1)) + E * lane_g; j < j1; j += W) {
+                T v[E];
+                int c[E];
+                ld_stream_vec(val + j, pol_s, v);
+                ld_stream_vec(col + j, pol_s, c);
+#pragma unroll
+                for (int e = 0; e < E; ++e)
+                    if (j + e >= j0 && j + e < j1) s += v[e] * ld_keep(x + c[e], pol_x);
+            }
         }
         for (int o = G >> 1; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (active && lane_g == 0) epilogue<T, EPI>(r, s, op, acc);
