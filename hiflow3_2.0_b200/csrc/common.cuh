@@ -90,6 +90,28 @@ __device__ __forceinline__ uint64_t l2_policy(int kind)
     return p;
 }
 
+// 16-byte streaming loads (L1 not allocated, the given L2 policy)
+__device__ __forceinline__ void ld_stream_vec(const double *a, uint64_t pol, double (&v)[2])
+{
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
+        : "=d"(v[0]), "=d"(v[1]) : "l"(a), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream_vec(const float *a, uint64_t pol, float (&v)[4])
+{
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(a), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream_vec(const int *a, uint64_t pol, int (&v)[2])
+{
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
+        : "=r"(v[0]), "=r"(v[1]) : "l"(a), "l"(pol));
+}
+__device__ __forceinline__ void ld_stream_vec(const int *a, uint64_t pol, int (&v)[4])
+{
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "l"(a), "l"(pol));
+}
+
 __device__ __forceinline__ double ld_stream(const double *a, uint64_t pol)
 {
     double v;

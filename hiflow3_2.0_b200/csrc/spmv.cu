@@ -190,27 +190,6 @@ __global__ void __launch_bounds__(kBlock, MINB) spmv_tile_kernel(CsrView A, Seg 
 }
 
 
-// 16-byte streaming loads (L1 bypassed, L2 evict-first hint)
-__device__ __forceinline__ void ld_stream_vec(const double *a, uint64_t pol, double (&v)[2])
-{
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.f64 {%0, %1}, [%2], %3;"
-        : "=d"(v[0]), "=d"(v[1]) : "l"(a), "l"(pol));
-}
-__device__ __forceinline__ void ld_stream_vec(const float *a, uint64_t pol, float (&v)[4])
-{
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(a), "l"(pol));
-}
-__device__ __forceinline__ void ld_stream_vec(const int *a, uint64_t pol, int (&v)[2])
-{
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.s32 {%0, %1}, [%2], %3;"
-        : "=r"(v[0]), "=r"(v[1]) : "l"(a), "l"(pol));
-}
-__device__ __forceinline__ void ld_stream_vec(const int *a, uint64_t pol, int (&v)[4])
-{
-    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]) : "l"(a), "l"(pol));
-}
 
 template <typename T, int EPI>
 __global__ void __launch_bounds__(kBlock) spmv_direct_kernel(CsrView A, Seg seg, SpmvOp op, Scratch sc)
