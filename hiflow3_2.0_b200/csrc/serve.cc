@@ -715,8 +715,9 @@ int capture_graph(b200la_server *S)
     return 0;
 }
 
-// Time the candidate kernel shapes on a calibration batch of Q1 systems and
-// keep the fastest.  No shape changes any system's arithmetic.
+// Time the candidate kernel shapes on a calibration batch of Q1 systems (one
+// captured round each, lanes concurrent) and keep the fastest.  No shape
+// changes any system's arithmetic.
 int autotune(b200la_server *S)
 {
     struct Cal {
@@ -767,16 +768,16 @@ int autotune(b200la_server *S)
             rc = -1;
             break;
         }
-        const int grid = S->num_sms * sh.cps;
-        auto iter = [&] {
-            for (int l = 0; l < S->lanes && !rc; ++l)
-                if (b200::srv::launch_round(sh.nw, grid, S->d_sys, S->d_state, S->d_tiles + (size_t)l * kTabWords, st) !=
-                    cudaSuccess)
-                    rc = -1;
-        };
-        for (int k = 0; k < 3 && !rc; ++k) iter();
+        // time the round exactly as it will run: the captured graph of this
+        // shape, with the lanes' kernel chains concurrent
+        if (capture_graph(S)) {
+            rc = -1;
+            break;
+        }
+        if (cudaGraphLaunch(S->graph, st) != cudaSuccess) rc = -1;
         cudaEventRecord(S->ev_a, st);
-        for (int k = 0; k < 12 && !rc; ++k) iter();
+        for (int k = 0; k < 2 && !rc; ++k)
+            if (cudaGraphLaunch(S->graph, st) != cudaSuccess) rc = -1;
         cudaEventRecord(S->ev_b, st);
         if (cudaStreamSynchronize(st) != cudaSuccess) rc = -1;
         float ms = 0.f;
