@@ -56,7 +56,7 @@ struct Req {
     // layout decided at submission
     int n = 0, fmt = 0, nchunks = 0;
     long long nnz = 0, slen = 0;      // stored entries (SELL: padded)
-    long long slen32 = 0;             // stored FP32 entries (mixed; stencil: groups of four)
+    long long slen32 = 0;             // stored FP32 entries (mixed; stencil: 32 L per chunk)
     std::vector<int> sell_off;        // SELL chunk offsets
     size_t bytes = 0, temp_bytes = 0; // resident / admission scratch
     double iter_bytes = 0;            // streamed by one batch iteration
@@ -153,7 +153,7 @@ int plan_request(b200la_server *S, Req *q)
         const int L = r.q1_dim == 3 ? 27 : 9;
         q->fmt = b200::srv::FMT_STENCIL;
         q->slen = (long long)q->nchunks * b200::srv::kChunk * L;
-        q->slen32 = (long long)q->nchunks * b200::srv::kChunk * 4 * ((L + 3) / 4);
+        q->slen32 = (long long)q->nchunks * b200::srv::kChunk * L;
     }
     int maxlen = 0;
     for (int v : len) maxlen = std::max(maxlen, v);

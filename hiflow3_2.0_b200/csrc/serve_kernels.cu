@@ -134,18 +134,21 @@ __device__ __forceinline__ double stencil_row(const double *__restrict__ val, in
     return s;
 }
 
-// Stencil row, FP32: the row's positions in groups of four per lane (one
-// 16-byte load each), then the bands.
+// Stencil row, FP32: the row's first 4 (L / 4) positions in groups of four
+// per lane (one 16-byte load each), the last L % 4 positions one by one
+// (position-major, 128 bytes per warp load), then the bands.  A chunk holds
+// exactly 32 L values: no padding.
 template <int NB, typename G>
 __device__ __forceinline__ float stencil_row(const float *__restrict__ val, int c, int lane, int n, int P,
                                              uint64_t pol, G gather)
 {
-    constexpr int DIM = NB == 9 ? 3 : 2, L = 3 * NB, GR = (L + 3) / 4;
+    constexpr int DIM = NB == 9 ? 3 : 2, L = 3 * NB, G4 = L / 4, TL = L % 4;
     const int r0 = c * kChunk, i = r0 + lane, he = lane == 0 ? r0 - 1 : r0 + 32;
-    const float4 *v = reinterpret_cast<const float4 *>(val + (size_t)c * kChunk * 4 * GR) + lane;
-    float a[4 * GR];
+    const float *cv = val + (size_t)c * kChunk * L;
+    const float4 *v = reinterpret_cast<const float4 *>(cv) + lane;
+    float a[L];
 #pragma unroll
-    for (int g = 0; g < GR; ++g) {
+    for (int g = 0; g < G4; ++g) {
         float4 q;
         asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
             : "=f"(q.x), "=f"(q.y), "=f"(q.z), "=f"(q.w)
@@ -155,6 +158,8 @@ __device__ __forceinline__ float stencil_row(const float *__restrict__ val, int 
         a[4 * g + 2] = q.z;
         a[4 * g + 3] = q.w;
     }
+#pragma unroll
+    for (int t = 0; t < TL; ++t) a[4 * G4 + t] = ld_stream(cv + 128 * G4 + 32 * t + lane, pol);
     float s = 0.0f;
 #pragma unroll
     for (int b = 0; b < NB; ++b)
@@ -678,9 +683,9 @@ __global__ void build_slot_kernel(SysDesc d, const int *__restrict__ row, const 
         if (d.fmt == FMT_STENCIL) {
             // values zero-filled before; each stored entry to its position
             if (i < n) {
-                const int c = i / kChunk, lane = i % kChunk, L = d.sL, GR = (L + 3) / 4;
+                const int c = i / kChunk, lane = i % kChunk, L = d.sL, G4 = L / 4;
                 const size_t base = (size_t)c * kChunk * L + lane;
-                const size_t base32 = (size_t)c * kChunk * 4 * GR + 4 * lane;
+                const size_t base32 = (size_t)c * kChunk * L;   // FP32: groups of four, then the tail
                 double *ov = const_cast<double *>(d.val64);
                 float *of = const_cast<float *>(d.val32);
                 for (int j = rb; j < re; ++j) {
@@ -688,7 +693,10 @@ __global__ void build_slot_kernel(SysDesc d, const int *__restrict__ row, const 
                     for (int k = 0; k < L; ++k)
                         if (stencil_delta(d.sdim, d.sP, k) == dl) {
                             ov[base + (size_t)kChunk * k] = val[j];
-                            if (d.mixed) of[base32 + (size_t)(k / 4) * 128 + k % 4] = (float)val[j];
+                            if (d.mixed)
+                                of[base32 + (k < 4 * G4 ? (size_t)(k / 4) * 128 + 4 * lane + k % 4
+                                                        : (size_t)G4 * 128 + (size_t)(k - 4 * G4) * 32 + lane)] =
+                                    (float)val[j];
                         }
                 }
             }
