@@ -116,6 +116,35 @@ def test_spmv_irregular_long_and_empty_rows(pf, b200, oracle):
     assert np.all(yv.numpy()[[0, 1, 2, 900, 2998]] == 0.0)
 
 
+@pytest.mark.parametrize("lanes", ["auto", "1", "4", "32"])
+def test_spmv_fp32_csr_irregular(pf, b200, lanes, monkeypatch):
+    """FP32 CSR SpMV with 16-byte value/column loads: rows that start at any
+    offset (not a multiple of four entries), long rows, empty rows (the last
+    row among them), for the automatic and forced lanes-per-row choices.
+    Tolerance: the FP32 rounding bound (row length + 16) * 2^-24 on the row's
+    magnitude sum_j |a_ij x_j|, against the product in FP64 of the same FP32
+    inputs."""
+    if lanes != "auto":
+        monkeypatch.setenv("B200LA_LANES", lanes)
+    rng = np.random.default_rng(23)
+    n, m = 2500, 4100
+    row, col, val = random_csr(rng, n, m, long_rows={3, 1200}, empty_rows={0, 7, 2499}, mean=9)
+    v32 = val.astype(np.float32)
+    x32 = rng.uniform(-1, 1, m).astype(np.float32)
+    vd, xd = v32.astype(np.float64), x32.astype(np.float64)
+    y_ref = np.array([vd[row[i]:row[i + 1]] @ xd[col[row[i]:row[i + 1]]] for i in range(n)])
+    scale = np.array([np.abs(vd[row[i]:row[i + 1]]) @ np.abs(xd[col[row[i]:row[i + 1]]]) for i in range(n)])
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, v32, n_cols=m, dtype=b200.F32)
+    if lanes != "auto":
+        assert A.info()["lanes_per_row"] == int(lanes)
+    y = pf.vector(n, b200.F32)
+    A.VectorMult(pf.vector(x32, b200.F32), y)
+    yh = y.numpy().astype(np.float64)
+    tol = (np.diff(row) + 16) * 2.0 ** -24 * np.maximum(scale, 1e-30)
+    assert np.all(np.abs(yh - y_ref) <= tol)
+    assert np.all(yh[[0, 7, 2499]] == 0.0)
+
+
 @pytest.mark.parametrize("lanes", ["1", "2", "8", "32"])
 def test_spmv_lane_layouts(pf, b200, oracle, lanes, monkeypatch):
     monkeypatch.setenv("B200LA_LANES", lanes)
