@@ -430,6 +430,12 @@ class Platform:
     def sync(self):
         self.check(lib().b200la_sync(self.h), "sync")
 
+    def stream(self):
+        """The platform's CUDA stream (every kernel of this platform runs on it)
+        as a torch stream, for ordering other work against it with events."""
+        torch = _torch()
+        return torch.cuda.ExternalStream(lib().b200la_get_stream(self.h) or 0, device=f"cuda:{self.device}")
+
     def num_sms(self):
         return lib().b200la_num_sms(self.h)
 

@@ -14,8 +14,16 @@ The B200 counterpart of HiFlow3's CoupledVector / CoupledMatrix / LaCouplings
 Transports: ``DistTransport`` over torch.distributed (NCCL for device tensors
 between GPUs, gloo for host tensors) and ``LocalTransport``, several ranks in
 one process (threads, one per rank, sharing a mailbox), which lets ranks share
-a GPU.  No collective here waits inside a kernel: exchanges are host-ordered
-stream operations, so ranks on one GPU cannot deadlock one another.
+a GPU.  No collective here waits inside a kernel, so ranks on one GPU cannot
+deadlock one another.
+
+The device exchange is stream-ordered and overlaps the diagonal-block SpMV,
+as the reference overlaps its Isend/Irecv with the local product
+(coupled_matrix.cc:433-467): the border is packed on the platform's stream,
+an event hands it to a communication stream that moves it, the diagonal
+block is multiplied meanwhile, and the platform's stream waits for the
+transfer's event only before the off-diagonal block.  The host does not wait
+for the transfer.
 
 Only host logic (partition, couplings set-up, exchange protocol) runs without
 a GPU; vectors and matrices live on the device and compute with the
@@ -26,10 +34,10 @@ import threading
 
 import numpy as np
 
-from . import CSR_lMatrix, F64, Control, lib, rowblock_split
+from . import CSR_lMatrix, F64, Control, Result, lib, rowblock_split
 
 __all__ = ["RowPartition", "LaCouplings", "DistTransport", "LocalTransport", "CoupledVector", "CoupledMatrix",
-           "CoupledCG", "exchange"]
+           "CoupledCG", "CoupledAsyncJacobi", "exchange", "exchange_async"]
 
 
 class RowPartition:
@@ -59,6 +67,7 @@ class DistTransport:
         import torch.distributed as dist
         self.dist, self.group = dist, group
         self.rank, self.size = dist.get_rank(group), dist.get_world_size(group)
+        self._comm = None
 
     def alltoall_lists(self, lists):
         """lists[q] -> peer q; returns what every peer sent to this rank."""
@@ -77,6 +86,27 @@ class DistTransport:
         if any(t.is_cuda for t in list(sends.values()) + list(recvs.values())):
             import torch
             torch.cuda.current_stream().synchronize()
+
+    def exchange_async(self, sends, recvs, ready):
+        """Device tensors: the point-to-point transfers run on a communication
+        stream once ``ready`` (recorded on this rank's platform stream after
+        the border was packed) has completed.  Returns the events the platform
+        stream waits on before it reads the ghosts or packs the border again;
+        the host does not wait."""
+        import torch
+        if self._comm is None:
+            self._comm = torch.cuda.Stream()
+        comm = self._comm
+        comm.wait_event(ready)
+        ops = [self.dist.P2POp(self.dist.irecv, t, q, self.group) for q, t in recvs.items() if t.numel()]
+        ops += [self.dist.P2POp(self.dist.isend, t, q, self.group) for q, t in sends.items() if t.numel()]
+        with torch.cuda.stream(comm):
+            if ops:
+                for w in self.dist.batch_isend_irecv(ops):
+                    w.wait()   # the communication stream waits, not the host
+        done = torch.cuda.Event()
+        done.record(comm)
+        return [done]
 
     def allreduce_sum(self, value, device):
         import torch
@@ -100,6 +130,7 @@ class LocalTransport:
 
     def __init__(self, fabric, rank):
         self.f, self.rank, self.size = fabric, rank, fabric.size
+        self._comm = None
 
     @classmethod
     def group(cls, size):
@@ -128,6 +159,36 @@ class LocalTransport:
             torch.cuda.synchronize()
         self.f.barrier.wait()
 
+    def exchange_async(self, sends, recvs, ready):
+        """Stream-ordered exchange between thread ranks: each receiver copies
+        from its senders' border buffers on its own communication stream, after
+        the senders' pack events and its own (so the copy cannot overwrite
+        ghosts its last off-diagonal product still reads).  Returns this rank's
+        copy event and the copy events of the peers that read its border: the
+        platform stream waits on all of them before it reads the ghosts or packs
+        the border again."""
+        import torch
+        if self._comm is None:
+            self._comm = torch.cuda.Stream()
+        comm = self._comm
+        for q, t in sends.items():
+            self.f.box[("p2p", self.rank, q)] = (t, ready)
+        self.f.barrier.wait()
+        comm.wait_event(ready)
+        with torch.cuda.stream(comm):
+            for q, t in recvs.items():
+                if t.numel():
+                    src, ev = self.f.box[("p2p", q, self.rank)]
+                    comm.wait_event(ev)
+                    t.copy_(src, non_blocking=True)
+        done = torch.cuda.Event()
+        done.record(comm)
+        self.f.box[("copied", self.rank)] = done
+        self.f.barrier.wait()
+        waits = [done] + [self.f.box[("copied", q)] for q, t in sends.items() if t.numel()]
+        self.f.barrier.wait()
+        return waits
+
     def allreduce_sum(self, value, device=None):
         self.f.box[("sum", self.rank)] = float(value)
         self.f.barrier.wait()
@@ -138,9 +199,7 @@ class LocalTransport:
         return tot
 
 
-def exchange(transport, couplings, border_values, ghost_values):
-    """Move border values (ordered by peer, couplings.border_offsets) into the
-    peers' ghost buffers (ordered by owner, couplings.ghost_offsets)."""
+def _pairs(transport, couplings, border_values, ghost_values):
     sends, recvs = {}, {}
     for q in range(transport.size):
         b0, b1 = couplings.border_offsets[q], couplings.border_offsets[q + 1]
@@ -149,7 +208,19 @@ def exchange(transport, couplings, border_values, ghost_values):
             sends[q] = border_values[b0:b1]
         if g1 > g0:
             recvs[q] = ghost_values[g0:g1]
-    transport.exchange(sends, recvs)
+    return sends, recvs
+
+
+def exchange(transport, couplings, border_values, ghost_values):
+    """Move border values (ordered by peer, couplings.border_offsets) into the
+    peers' ghost buffers (ordered by owner, couplings.ghost_offsets)."""
+    transport.exchange(*_pairs(transport, couplings, border_values, ghost_values))
+
+
+def exchange_async(transport, couplings, border_values, ghost_values, ready):
+    """exchange() for device buffers, ordered on streams behind the event
+    ``ready``; returns the events to wait on (transport.exchange_async)."""
+    return transport.exchange_async(*_pairs(transport, couplings, border_values, ghost_values), ready)
 
 
 class LaCouplings:
@@ -204,14 +275,29 @@ class CoupledVector:
     def clone_without_content(self):
         return CoupledVector(self.pf, self.cp, self.tr, self.interior.get_size(), self.dtype)
 
-    def UpdateGhost(self):
-        """Pack the border with the gather kernel, then the peer exchange."""
+    def begin_update(self):
+        """Pack the border with the gather kernel on the platform's stream and
+        start the exchange behind it; returns what end_update waits on."""
+        import torch
         nb = self.border.numel()
         if nb:
             self.pf.check(lib().b200la_gather(self.pf.h, self.dtype, nb, C.c_void_p(self._bidx.data_ptr()),
                                               self.interior.ptr, C.c_void_p(self.border.data_ptr())), "gather")
-        self.pf.sync()
-        exchange(self.tr, self.cp, self.border, self.ghost)
+        ready = torch.cuda.Event()
+        ready.record(self.pf.stream())
+        return exchange_async(self.tr, self.cp, self.border, self.ghost, ready)
+
+    def end_update(self, waits):
+        """The platform's stream waits for the exchange (ghosts in place, border
+        free to be packed again); the host does not."""
+        ls = self.pf.stream()
+        for ev in waits:
+            ls.wait_event(ev)
+
+    def UpdateGhost(self):
+        """Pack the border, exchange it with the peers, the ghosts ready for
+        the platform's next kernel (CoupledVector::UpdateGhost)."""
+        self.end_update(self.begin_update())
 
     # global reductions (local kernel, then the sum across ranks)
     def Dot(self, other):
@@ -261,12 +347,28 @@ class CoupledMatrix:
                              self.n_local if data_or_n is None else data_or_n, self.dtype)
 
     def VectorMult(self, x, y):
-        """y = A x: the ghost update, the diagonal block, the off-diagonal block
-        (coupled_matrix.cc:433-467)."""
-        x.UpdateGhost()
+        """y = A x (coupled_matrix.cc:433-467): the ghost exchange starts, the
+        diagonal block is multiplied while it runs, then the off-diagonal block
+        once the ghosts have arrived."""
+        waits = x.begin_update()
         self.diag.VectorMult(x.interior, y.interior)
+        x.end_update(waits)
         if self.offdiag is not None:
             lib().b200la_spmv_add(self.pf.h, self.offdiag.h, C.c_void_p(x.ghost.data_ptr()), y.interior.ptr)
+
+
+def check(ctl, it, v, res0):
+    """IterateControl::Check (src/common/iterate_control.cc:84-110): 0 iterate,
+    1 absolute, 2 relative, 3 divergence, 4 iteration limit."""
+    if v < ctl.abstol:
+        return 1
+    if v < ctl.reltol * res0:
+        return 2
+    if v > ctl.divtol * res0:
+        return 3
+    if it >= ctl.maxits:
+        return 4
+    return 0
 
 
 class CoupledCG:
@@ -289,24 +391,12 @@ class CoupledCG:
         self.res0 = res
         ctl = Control(maxits, abstol, reltol, divtol)
 
-        def check(it, v):
-            # IterateControl::Check (src/common/iterate_control.cc:84-110)
-            if v < ctl.abstol:
-                return 1
-            if v < ctl.reltol * self.res0:
-                return 2
-            if v > ctl.divtol * self.res0:
-                return 3
-            if it >= ctl.maxits:
-                return 4
-            return 0
-
         def precond(src, dst):
             dst.CopyFrom(src)
             if self.jacobi:
                 dst.interior.ElementWiseMult(self.invd.interior)
 
-        status, it = check(0, res), 0
+        status, it = check(ctl, 0, res, self.res0), 0
         precond(r, z)
         p.CopyFrom(z)
         rho = r.Dot(z)
@@ -317,12 +407,59 @@ class CoupledCG:
             x.Axpy(p, alpha)
             r.Axpy(Ap, -alpha)
             res = r.Norm2()
-            status = check(it, res)
+            status = check(ctl, it, res, self.res0)
             if status:
                 break
             precond(r, z)
             rho_new = r.Dot(z)
             p.ScaleAdd(rho_new / rho, z)         # p = beta p + z
             rho = rho_new
+        self.iter, self.res = it, res
+        return status
+
+
+class CoupledAsyncJacobi:
+    """AsynchronousIterationGPU<LAD>::SolveNormal / SolveDamped
+    (src/linear_solver/gpu-based/async_iter_gpu.cc:538-630, 780-900) on coupled
+    objects.  One check interval is n_global global iterations; each is n_block
+    launches of n_inner asynchronous sweeps over this rank's rows
+    (b200la_async_jacobi, the ghost values fixed), with the ghost update
+    (GlobalUpdate) between global iterations.  Then the global residual
+    ||b - A x|| (which updates the ghosts again) and IterateControl::Check on
+    the sweep count."""
+
+    def __init__(self, A, n_global=1, n_block=10, n_inner=10, w=1.0):
+        if min(n_global, n_block, n_inner) < 1 or not w > 0.0:
+            raise ValueError("n_global, n_block, n_inner >= 1 and w > 0 required")
+        self.A, self.n_global, self.n_block, self.n_inner, self.w = A, n_global, n_block, n_inner, float(w)
+        self.iter, self.res, self.res0 = 0, 0.0, 0.0
+
+    def _residual(self, b, x, r):
+        self.A.VectorMult(x, r)
+        r.ScaleAdd(-1.0, b)                      # r = b - A x
+        return r.Norm2()
+
+    def Solve(self, b, x, maxits=100000, abstol=0.0, reltol=1e-8, divtol=1e6):
+        A = self.A
+        ctl = Control(maxits, abstol, reltol, divtol)
+        # one batch per call: no tolerance, the limit at the batch's sweeps
+        one = Control(self.n_block * self.n_inner, 0.0, 0.0, 1e300)
+        r = A.vector()
+        res = self._residual(b, x, r)
+        self.res0, it = res, 0
+        status = check(ctl, it, res, self.res0)
+        oh = A.offdiag.h if A.offdiag is not None else None
+        while status == 0:
+            for g in range(self.n_global):
+                out = Result()
+                ghost = C.c_void_p(x.ghost.data_ptr()) if oh is not None else None
+                A.pf.check(lib().b200la_async_jacobi(A.pf.h, A.diag.h, oh, b.interior.ptr, x.interior.ptr, ghost,
+                                                     self.n_inner, self.n_block, self.w, C.byref(one),
+                                                     C.byref(out)), "async_jacobi")
+                it += self.n_block * self.n_inner
+                if g < self.n_global - 1:
+                    x.UpdateGhost()
+            res = self._residual(b, x, r)
+            status = check(ctl, it, res, self.res0)
         self.iter, self.res = it, res
         return status

@@ -164,3 +164,81 @@ def test_coupled_cg_ranks_on_one_gpu(b200, world):
         assert st == b200.SUCCESS_REL
         assert abs(it - it0) <= max(1, 0.05 * it0), (it, it0)
         assert np.linalg.norm(x - xs[r0:r0 + len(x)]) <= 1e-8 * np.linalg.norm(xs)
+
+
+@pytest.mark.gpu
+def test_coupled_products_back_to_back_without_host_waits(b200):
+    """Twelve coupled products in a row, each feeding the next (x <- 0.1 A x
+    on the platform's stream), with no host synchronisation between them: the
+    stream-ordered exchange must keep every ghost update behind the pack that
+    produced it and ahead of the off-diagonal product that reads it, and no
+    border may be repacked before its peers have copied it."""
+    import importlib
+    cp = importlib.import_module("hiflow3_b200.coupled")
+    row, col, val = b200.q1_assemble(2, 48, 1, None, 1e-2, (1.0, 0.5))
+    n = len(row) - 1
+    world, steps = 3, 12
+    part = cp.RowPartition.even(n, world)
+    trs = cp.LocalTransport.group(world)
+    x0 = np.cos(np.arange(n) * 0.23)
+
+    def rank_fn(r):
+        pf = b200.Platform(0)
+        r0, r1 = part.range(r)
+        M = cp.CoupledMatrix(pf, part, r, trs[r], row[r0:r1 + 1] - row[r0], col[row[r0]:row[r1]],
+                             val[row[r0]:row[r1]])
+        x, y = M.vector(x0[r0:r1]), M.vector()
+        for _ in range(steps):
+            M.VectorMult(x, y)
+            x.CopyFrom(y)
+            x.Scale(0.1)
+        return r0, x.numpy()
+
+    res = _run_ranks(world, rank_fn)
+    xg = x0.copy()
+    for _ in range(steps):
+        xg = 0.1 * _spmv_np(row, col, val, xg)
+    for r0, xr in res:
+        assert np.allclose(xr, xg[r0:r0 + len(xr)], rtol=0, atol=1e-11 * np.abs(xg).max())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world,n_global,w", [(2, 1, 1.0), (3, 2, 0.9)])
+def test_coupled_async_jacobi_ranks_on_one_gpu(b200, world, n_global, w):
+    """Asynchronous block-Jacobi across thread ranks with the ghost update
+    between global iterations: every rank stops on the global residual (the
+    same decision on all ranks) and the assembled solution solves the global
+    system."""
+    import importlib
+    cp = importlib.import_module("hiflow3_b200.coupled")
+    N = 14
+    row, col, val = b200.q1_assemble(2, N, 0, np.exp(np.random.default_rng(7).standard_normal(N * N)))
+    n = len(row) - 1
+    b = b200.q1_rhs(11, 2, N)
+    part = cp.RowPartition.even(n, world)
+    trs = cp.LocalTransport.group(world)
+
+    def rank_fn(r):
+        pf = b200.Platform(0)
+        r0, r1 = part.range(r)
+        M = cp.CoupledMatrix(pf, part, r, trs[r], row[r0:r1 + 1] - row[r0], col[row[r0]:row[r1]],
+                             val[row[r0]:row[r1]])
+        s = cp.CoupledAsyncJacobi(M, n_global=n_global, n_block=4, n_inner=3, w=w)
+        x = M.vector()
+        st = s.Solve(M.vector(b[r0:r1]), x, maxits=400000, reltol=1e-8)
+        return r0, st, s.iter, s.res, s.res0, x.numpy()
+
+    res = _run_ranks(world, rank_fn)
+    D = np.zeros((n, n))
+    for i in range(n):
+        D[i, col[row[i]:row[i + 1]]] += val[row[i]:row[i + 1]]
+    xe = np.linalg.solve(D, b)
+    x = np.zeros(n)
+    for r0, st, it, rn, r0n, xr in res:
+        assert st == b200.SUCCESS_REL
+        assert it % (n_global * 12) == 0
+        assert rn < 1e-8 * r0n
+        x[r0:r0 + len(xr)] = xr
+    assert len({(st, it) for _, st, it, _, _, _ in res}) == 1
+    assert np.linalg.norm(b - D @ x) <= 1e-8 * res[0][4] * 1.0001
+    assert np.linalg.norm(x - xe) <= 1e-4 * np.linalg.norm(xe)
