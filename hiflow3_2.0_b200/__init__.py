@@ -31,7 +31,7 @@ STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "allocation failed
           7: "bounded device wait gave up", 8: "preconditioner setup failed", 9: "unknown request",
           10: "request pending", 11: "file I/O failed", 12: "unsupported or malformed file"}
 PENDING = 10
-ERR_CSR, ERR_IO, ERR_FORMAT = 5, 11, 12
+ERR_ARG, ERR_CSR, ERR_IO, ERR_FORMAT = 1, 5, 11, 12
 SERVE_CG, SERVE_GMRES = 0, 1
 SERVE_F64, SERVE_MIXED = 0, 1
 
@@ -135,6 +135,10 @@ def lib():
         "b200la_csr_format": ([_P, C.POINTER(_I), C.POINTER(_I)], _I),
         "b200la_csr_set_values": ([_P, _P, _P], _I),
         "b200la_csr_invdiag": ([_P, _P, _P], _I),
+        "b200la_csr_scale": ([_P, _P, _D, _I], _I),
+        "b200la_csr_diag": ([_P, _P, _I, _I, _I, _P], _I),
+        "b200la_csr_extract_submatrix": ([_P, _P, _I, _I, _I, _I, C.POINTER(_P)], _I),
+        "b200la_csr_compress": ([_P, _P, C.POINTER(_P)], _I),
         "b200la_spmv": ([_P, _P, _P, _P], _I),
         "b200la_spmv_add": ([_P, _P, _P, _P], _I),
         "b200la_spmv_dot": ([_P, _P, _P, _P, _P], _I),
@@ -658,8 +662,48 @@ class CSR_lMatrix:
         self.pf.sync()
         return float(d.item())
 
-    def extract_invdiagelements(self, out):
-        self.pf.check(lib().b200la_csr_invdiag(self.pf.h, self.h, out.ptr), "invdiag")
+    def extract_diagelements(self, start, end, vec):
+        """vec[0 .. end - start) = a_ii of rows [start, end) (lmatrix_csr_cpu.cc:2395-2412);
+        a row without a stored diagonal leaves its entry of vec unchanged."""
+        self.pf.check(lib().b200la_csr_diag(self.pf.h, self.h, start, end, 0, vec.ptr), "extract_diagelements")
+
+    def extract_invdiagelements(self, start, end, vec):
+        """vec[0 .. end - start) = 1 / a_ii of rows [start, end) (lmatrix_csr_cpu.cc:2414-2431)."""
+        self.pf.check(lib().b200la_csr_diag(self.pf.h, self.h, start, end, 1, vec.ptr), "extract_invdiagelements")
+
+    def Scale(self, alpha):
+        """Every value times alpha (lmatrix_csr_cpu.cc:205-212)."""
+        self.pf.check(lib().b200la_csr_scale(self.pf.h, self.h, alpha, 0), "Scale")
+
+    def ScaleOffdiag(self, alpha):
+        """The values off the diagonal times alpha (lmatrix_csr_cpu.cc:215-224)."""
+        self.pf.check(lib().b200la_csr_scale(self.pf.h, self.h, alpha, 1), "ScaleOffdiag")
+
+    def Zeros(self):
+        """Every value zero, the structure kept (lmatrix_csr_cpu.cc:100-103)."""
+        self.pf.check(lib().b200la_csr_scale(self.pf.h, self.h, 0.0, 2), "Zeros")
+
+    def extract_submatrix(self, start_row, start_col, end_row, end_col):
+        """A new matrix of the block [start_row, end_row) x [start_col, end_col)
+        (lmatrix_csr_cpu.cc:1768-1843)."""
+        h = C.c_void_p()
+        self.pf.check(lib().b200la_csr_extract_submatrix(self.pf.h, self.h, start_row, start_col, end_row, end_col,
+                                                         C.byref(h)), "extract_submatrix")
+        return CSR_lMatrix._wrap(self.pf, h, self.dtype)
+
+    def Compress(self):
+        """Drop the entries whose value is zero (lmatrix_csr_cpu.cc:142-202), in place."""
+        h = C.c_void_p()
+        self.pf.check(lib().b200la_csr_compress(self.pf.h, self.h, C.byref(h)), "Compress")
+        lib().b200la_csr_destroy(self.h)
+        self.h = h
+        self.nnz = self.info()["nnz"]
+
+    @classmethod
+    def _wrap(cls, platform, h, dtype):
+        vals = [C.c_int() for _ in range(7)]
+        platform.check(lib().b200la_csr_info(h, *[C.byref(v) for v in vals]))
+        return cls(platform, h, vals[0].value, vals[1].value, vals[2].value, dtype)
 
     def close(self):
         if getattr(self, "h", None):

@@ -117,4 +117,13 @@ cudaError_t launch_invdiag(int dtype, int n, const int *row, const int *col, con
                            cudaStream_t st);
 cudaError_t launch_jacobi(int dtype, int n, const void *invd, const void *r, void *z, const int *gate,
                           cudaStream_t st);
+// matops.cu
+cudaError_t launch_csr_scale(int dtype, int n, const int *row, const int *col, void *val, double alpha, int mode,
+                             cudaStream_t st);
+cudaError_t launch_csr_diag(int dtype, int start, int end, const int *row, const int *col, const void *val,
+                            int inverse, void *out, cudaStream_t st);
+cudaError_t launch_csr_filter_count(int dtype, int r0, int r1, const int *row, const int *col, const void *val,
+                                    int mode, int sc, int ec, int *cnt, cudaStream_t st);
+cudaError_t launch_csr_filter_fill(int dtype, int r0, int r1, const int *row, const int *col, const void *val,
+                                   int mode, int sc, int ec, const int *off, int *co, void *vo, cudaStream_t st);
 }  // namespace b200

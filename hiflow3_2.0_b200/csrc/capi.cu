@@ -768,6 +768,84 @@ extern "C" int b200la_csr_set_values(b200la_ctx *ctx, b200la_csr *A, const void 
     return rc ? rc : build_stencil(ctx, A);
 }
 
+extern "C" int b200la_csr_scale(b200la_ctx *ctx, b200la_csr *A, double alpha, int mode)
+{
+    if (!ctx || !A || mode < B200LA_SCALE_ALL || mode > B200LA_SCALE_ZERO)
+        return ctx_msg(ctx, B200LA_ERR_ARG, "csr_scale: invalid argument");
+    if (A->nnz) CK(launch_csr_scale(A->dtype, A->n, A->row, A->col, A->val, alpha, mode, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    // the SpMV layouts derived from the values follow them
+    const int rc = build_sell(ctx, A);
+    return rc ? rc : build_stencil(ctx, A);
+}
+
+extern "C" int b200la_csr_diag(b200la_ctx *ctx, const b200la_csr *A, int start, int end, int inverse, void *out)
+{
+    if (!ctx || !A || start < 0 || end < start || end > A->n || end > A->m || (end > start && !out))
+        return ctx_msg(ctx, B200LA_ERR_ARG, "csr_diag: invalid argument");
+    if (end > start) CK(launch_csr_diag(A->dtype, start, end, A->row, A->col, A->val, inverse, out, ctx->stream));
+    return B200LA_OK;
+}
+
+// Rows [r0, r1) filtered on the device (mode 0: columns [sc, ec) shifted to
+// 0; mode 1: nonzero values), then a new matrix of n_cols columns from them.
+static int csr_filter(b200la_ctx *ctx, const b200la_csr *A, int mode, int r0, int r1, int sc, int ec, int n_cols,
+                      b200la_csr **out)
+{
+    const int rows = r1 - r0;
+    const size_t es = dsize(A->dtype);
+    int *d_cnt = nullptr, *d_off = nullptr, *d_col = nullptr;
+    void *d_val = nullptr;
+    std::vector<int> h_row(rows + 1, 0), h_col;
+    std::vector<char> h_val;
+    cudaError_t e = cudaMalloc(&d_cnt, sizeof(int) * std::max(rows, 1));
+    if (e == cudaSuccess && rows) e = launch_csr_filter_count(A->dtype, r0, r1, A->row, A->col, A->val, mode, sc, ec,
+                                                              d_cnt, ctx->stream);
+    if (e == cudaSuccess && rows)
+        e = cudaMemcpyAsync(h_row.data() + 1, d_cnt, sizeof(int) * rows, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    for (int i = 0; e == cudaSuccess && i < rows; ++i) h_row[i + 1] += h_row[i];
+    const int k = h_row[rows];
+    if (e == cudaSuccess && k) {
+        h_col.resize(k);
+        h_val.resize(es * k);
+        e = cudaMalloc(&d_off, sizeof(int) * (rows + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&d_col, sizeof(int) * k);
+        if (e == cudaSuccess) e = cudaMalloc(&d_val, es * k);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_off, h_row.data(), sizeof(int) * (rows + 1), cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = launch_csr_filter_fill(A->dtype, r0, r1, A->row, A->col, A->val, mode, sc, ec, d_off, d_col, d_val,
+                                       ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(h_col.data(), d_col, sizeof(int) * k, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(h_val.data(), d_val, es * k, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    }
+    cudaFree(d_cnt);
+    cudaFree(d_off);
+    cudaFree(d_col);
+    cudaFree(d_val);
+    if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_CUDA, "csr_extract", e);
+    return csr_upload(ctx, rows, n_cols, k, h_row.data(), k ? h_col.data() : nullptr,
+                      k ? static_cast<const void *>(h_val.data()) : nullptr, A->dtype, 0, nullptr, out);
+}
+
+extern "C" int b200la_csr_extract_submatrix(b200la_ctx *ctx, const b200la_csr *A, int start_row, int start_col,
+                                            int end_row, int end_col, b200la_csr **out)
+{
+    if (!ctx || !A || !out || start_row < 0 || start_col < 0 || end_row <= start_row || end_col <= start_col ||
+        end_row > A->n || end_col > A->m)
+        return ctx_msg(ctx, B200LA_ERR_ARG, "csr_extract_submatrix: invalid argument");
+    return csr_filter(ctx, A, 0, start_row, end_row, start_col, end_col, end_col - start_col, out);
+}
+
+extern "C" int b200la_csr_compress(b200la_ctx *ctx, const b200la_csr *A, b200la_csr **out)
+{
+    if (!ctx || !A || !out) return ctx_msg(ctx, B200LA_ERR_ARG, "csr_compress: invalid argument");
+    return csr_filter(ctx, A, 1, 0, A->n, 0, 0, A->m, out);
+}
+
 extern "C" int b200la_csr_invdiag(b200la_ctx *ctx, const b200la_csr *A, void *out)
 {
     if (!ctx || !A || !out || A->n != A->m) return B200LA_ERR_ARG;

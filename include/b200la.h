@@ -136,6 +136,29 @@ int b200la_csr_format(const b200la_csr *A, int *npat, int *uses_dict);
 int b200la_csr_download(b200la_ctx *ctx, const b200la_csr *A, int *row, int *col, void *val);
 /* New values, same structure (host array of the matrix dtype). */
 int b200la_csr_set_values(b200la_ctx *ctx, b200la_csr *A, const void *val);
+/* CSR_lMatrix value operations in place on the device; the SpMV layouts
+ * follow the new values.  mode B200LA_SCALE_ALL: Scale (every value times
+ * alpha, src/linear_algebra/lmp/lmatrix_csr_cpu.cc:205-212);
+ * B200LA_SCALE_OFFDIAG: ScaleOffdiag (values with col != row, :215-224);
+ * B200LA_SCALE_ZERO: Zeros (every value 0, alpha unused, :100-103). */
+enum { B200LA_SCALE_ALL = 0, B200LA_SCALE_OFFDIAG = 1, B200LA_SCALE_ZERO = 2 };
+int b200la_csr_scale(b200la_ctx *ctx, b200la_csr *A, double alpha, int mode);
+/* extract_diagelements / extract_invdiagelements (lmatrix_csr_cpu.cc:2395-2431)
+ * of rows [start, end) into out_dev[0 .. end - start) (device, matrix dtype):
+ * the row's last stored diagonal entry, or 1 over it.  A row without one
+ * leaves its output untouched (the reference writes an uninitialised value). */
+int b200la_csr_diag(b200la_ctx *ctx, const b200la_csr *A, int start, int end, int inverse, void *out_dev);
+/* extract_submatrix (lmatrix_csr_cpu.cc:1768-1843): a new matrix holding the
+ * block [start_row, end_row) x [start_col, end_col), built as the reference
+ * builds it (columns ascending per row; an entry whose column repeats is added
+ * into the first one, the repeat left as a stored zero).  Destroy with
+ * b200la_csr_destroy.  B200LA_ERR_ARG for an empty or out-of-range block. */
+int b200la_csr_extract_submatrix(b200la_ctx *ctx, const b200la_csr *A, int start_row, int start_col, int end_row,
+                                 int end_col, b200la_csr **out);
+/* Compress (lmatrix_csr_cpu.cc:142-202): a new matrix without the entries
+ * whose value is zero, the others in their order.  The reference compresses
+ * in place; the caller replaces its handle (and destroys the old one). */
+int b200la_csr_compress(b200la_ctx *ctx, const b200la_csr *A, b200la_csr **out);
 /* extract_invdiagelements (src/linear_algebra/lmp/lmatrix_csr_cpu.cc:2414-2431): out[i] = 1/a_ii, device. */
 int b200la_csr_invdiag(b200la_ctx *ctx, const b200la_csr *A, void *out_dev);
 

@@ -1164,3 +1164,70 @@ int orc_mpir(int n, const int *row, const int *col, const double *val,
     free(vl); free(dl); free(rl); free(cl); free(r); free(invd);
     return out->status == ORC_SUCCESS_REL ? 0 : 1;
 }
+
+/* ------------------------------------------------------------------ */
+/* Matrix value and structure operations                               */
+/* ------------------------------------------------------------------ */
+
+/* CPU_CSR_lMatrix::Scale / ScaleOffdiag / Zeros (lmp/lmatrix_csr_cpu.cc:100-103, 205-224). */
+void orc_csr_scale(int n, const int *row, const int *col, double *val, double alpha, int mode)
+{
+    for (int i = 0; i < n; ++i)
+        for (int j = row[i]; j < row[i + 1]; ++j) {
+            if (mode == 2) val[j] = 0.0;
+            else if (mode == 0 || col[j] != i) val[j] *= alpha;
+        }
+}
+
+/* CPU_CSR_lMatrix::extract_diagelements / extract_invdiagelements (:2395-2431):
+ * every stored diagonal entry of the row assigns, so the last one stays. */
+void orc_csr_diag(const int *row, const int *col, const double *val, int start, int end, int inverse,
+                  double *out)
+{
+    for (int i = start; i < end; ++i)
+        for (int j = row[i]; j < row[i + 1]; ++j)
+            if (col[j] == i) out[i - start] = inverse ? 1 / val[j] : val[j];
+}
+
+/* CPU_CSR_lMatrix::extract_submatrix (:1768-1843) and Compress (:142-202). */
+int orc_csr_extract(int n, const int *row, const int *col, const double *val, int mode, int sr, int sc, int er,
+                    int ec, int **row_out, int **col_out, double **val_out)
+{
+    const int r0 = mode == 0 ? sr : 0, r1 = mode == 0 ? er : n, rows = r1 - r0;
+    int *ro = (int *)calloc((size_t)rows + 1, sizeof(int));
+    int cnt = 0;
+    for (int i = r0; i < r1; ++i) {
+        for (int j = row[i]; j < row[i + 1]; ++j)
+            if (mode == 0 ? (col[j] >= sc && col[j] < ec) : (val[j] != 0.0)) ++cnt;
+        ro[i - r0 + 1] = cnt;
+    }
+    int *co = (int *)malloc(sizeof(int) * (size_t)(cnt > 0 ? cnt : 1));
+    double *vo = (double *)malloc(sizeof(double) * (size_t)(cnt > 0 ? cnt : 1));
+    for (int i = r0; i < r1; ++i) {
+        int k = ro[i - r0];
+        if (mode == 1) {
+            /* Compress keeps the nonzero entries in their order */
+            for (int j = row[i]; j < row[i + 1]; ++j)
+                if (val[j] != 0.0) { co[k] = col[j]; vo[k] = val[j]; ++k; }
+            continue;
+        }
+        /* init_structure: the row's block columns, sorted (TransformFromCOO,
+         * :951-1044); then Zeros and add_value in source order (:1127-1181),
+         * each value added to the first stored entry of its column */
+        const int b = k;
+        for (int j = row[i]; j < row[i + 1]; ++j)
+            if (col[j] >= sc && col[j] < ec) co[k++] = col[j] - sc;
+        for (int a = b; a < k; ++a)           /* ascending columns */
+            for (int c = a + 1; c < k; ++c)
+                if (co[c] < co[a]) { int t = co[a]; co[a] = co[c]; co[c] = t; }
+        for (int a = b; a < k; ++a) vo[a] = 0.0;
+        for (int j = row[i]; j < row[i + 1]; ++j)
+            if (col[j] >= sc && col[j] < ec)
+                for (int a = b; a < k; ++a)
+                    if (co[a] == col[j] - sc) { vo[a] += val[j]; break; }
+    }
+    *row_out = ro;
+    *col_out = co;
+    *val_out = vo;
+    return cnt;
+}

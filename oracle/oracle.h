@@ -185,6 +185,26 @@ void orc_block_apply(const orc_block_precond *P, const double *r, double *z);
 void orc_block_free(orc_block_precond *P);
 
 /* ------------------------------------------------------------------ */
+/* Matrix value and structure operations (lmp/lmatrix_csr_cpu.cc)       */
+/* ------------------------------------------------------------------ */
+
+/* Scale (:205-212), ScaleOffdiag (:215-224), Zeros (:100-103) of an
+ * n-row CSR, values in place: mode 0, 1, 2. */
+void orc_csr_scale(int n, const int *row, const int *col, double *val, double alpha, int mode);
+/* extract_diagelements / extract_invdiagelements (:2395-2431) of rows
+ * [start, end): the last stored diagonal entry of each row (or 1 / it).  A
+ * row without one leaves its output untouched, as in the reference. */
+void orc_csr_diag(const int *row, const int *col, const double *val, int start, int end, int inverse,
+                  double *out);
+/* extract_submatrix (:1768-1843): the block [sr, er) x [sc, ec) through
+ * init_structure (TransformFromCOO, columns sorted per row) and add_value
+ * (each entry added to the first stored entry of its column); mode 0.
+ * Compress (:142-202): the entries whose value is not zero, in place order;
+ * mode 1.  Outputs allocated (free with orc_free); returns nnz. */
+int orc_csr_extract(int n, const int *row, const int *col, const double *val, int mode, int sr, int sc, int er,
+                    int ec, int **row_out, int **col_out, double **val_out);
+
+/* ------------------------------------------------------------------ */
 /* Krylov solvers (src/linear_solver/*.cc) and IterateControl          */
 /* ------------------------------------------------------------------ */
 

@@ -136,6 +136,12 @@ class Oracle:
         L.orc_power_pattern.argtypes = [C.c_int, _i32p, _i32p, C.c_int, _pp, _pp]
         L.orc_ilup.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int, _pp, _pp, _dp]
         L.orc_free.argtypes = [C.c_void_p]
+        L.orc_csr_scale.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_double, C.c_int]
+        L.orc_csr_scale.restype = None
+        L.orc_csr_diag.argtypes = [_i32p, _i32p, _f64p, C.c_int, C.c_int, C.c_int, _f64p]
+        L.orc_csr_diag.restype = None
+        L.orc_csr_extract.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                      _pp, _pp, _dp]
         L.orc_free.restype = None
         L.orc_block_apply.argtypes = [C.POINTER(_Block), _f64p, _f64p]
         L.orc_block_apply.restype = None
@@ -318,6 +324,32 @@ class Oracle:
             self.lib.orc_free(C.cast(q, C.c_void_p))
         return out
 
+    def csr_scale(self, row, col, val, alpha, mode):
+        """Scale (mode 0), ScaleOffdiag (1), Zeros (2): the new values."""
+        v = _f64(val).copy()
+        self.lib.orc_csr_scale(len(row) - 1, _i32(row), _i32(col), v, alpha, mode)
+        return v
+
+    def csr_diag(self, row, col, val, start, end, inverse=False, fill=0.0):
+        """extract_diagelements / extract_invdiagelements of rows [start, end);
+        rows without a diagonal entry keep `fill`."""
+        out = np.full(end - start, fill)
+        self.lib.orc_csr_diag(_i32(row), _i32(col), _f64(val), start, end, int(inverse), out)
+        return out
+
+    def csr_extract(self, row, col, val, mode, sr=0, sc=0, er=0, ec=0):
+        """extract_submatrix (mode 0, block [sr, er) x [sc, ec)) or Compress (mode 1)."""
+        n = len(row) - 1
+        r, c, v = C.POINTER(C.c_int)(), C.POINTER(C.c_int)(), C.POINTER(C.c_double)()
+        m = self.lib.orc_csr_extract(n, _i32(row), _i32(col), _f64(val), mode, sr, sc, er, ec, C.byref(r),
+                                     C.byref(c), C.byref(v))
+        rows = (er - sr if mode == 0 else n) + 1
+        out = (np.ctypeslib.as_array(r, (rows,)).copy(), np.ctypeslib.as_array(c, (max(m, 1),))[:m].copy(),
+               np.ctypeslib.as_array(v, (max(m, 1),))[:m].copy())
+        for q in (r, c, v):
+            self.lib.orc_free(C.cast(q, C.c_void_p))
+        return out
+
     def ilup_build(self, row, col, val, mode, ilu_p, mat_power=1):
         n = len(row) - 1
         st = _Block()
@@ -424,6 +456,12 @@ class Ref:
         L.ref_time_spmv.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p]
         L.ref_time_spmv.restype = C.c_double
         L.ref_max_threads.restype = C.c_int
+        L.ref_csr_scale.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, C.c_double, C.c_int]
+        L.ref_csr_scale.restype = None
+        L.ref_csr_diag.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_int, C.c_int, _f64p]
+        L.ref_csr_diag.restype = None
+        L.ref_csr_extract.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_int, C.c_int,
+                                      C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p]
 
     def coo_to_csr(self, n, coo_row, coo_col, coo_val=None):
         coo_row, coo_col = _i32(coo_row), _i32(coo_col)
@@ -518,6 +556,27 @@ class Ref:
         m = self.lib.ref_ilup(n, nnz, _i32(row), _i32(col), _f64(val), p, cap, r, c, v)
         assert m >= 0
         return r, c[:m].copy(), v[:m].copy()
+
+    def csr_scale(self, row, col, val, alpha, mode, m=None):
+        n = len(row) - 1
+        v = _f64(val).copy()
+        self.lib.ref_csr_scale(n, m or n, len(col), _i32(row), _i32(col), v, alpha, mode)
+        return v
+
+    def csr_diag(self, row, col, val, start, end, inverse=False, m=None):
+        n = len(row) - 1
+        out = np.empty(end - start)
+        self.lib.ref_csr_diag(n, m or n, len(col), _i32(row), _i32(col), _f64(val), start, end, int(inverse), out)
+        return out
+
+    def csr_extract(self, row, col, val, mode, sr=0, sc=0, er=0, ec=0, m=None):
+        n, nnz = len(row) - 1, len(col)
+        rows = (er - sr if mode == 0 else n) + 1
+        r, c, v = np.empty(rows, np.int32), np.empty(max(nnz, 1), np.int32), np.empty(max(nnz, 1))
+        k = self.lib.ref_csr_extract(n, m or n, nnz, _i32(row), _i32(col), _f64(val), mode, sr, sc, er, ec,
+                                     max(nnz, 1), r, c, v)
+        assert k >= 0
+        return r, c[:k].copy(), v[:k].copy()
 
     def power_pattern(self, row, col, p, cap=None):
         n, nnz = len(row) - 1, len(col)

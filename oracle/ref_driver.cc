@@ -626,6 +626,69 @@ int ref_vec_read(const char *path, double *x, int cap)
     return n;
 }
 
+// CPU_CSR_lMatrix::Scale / ScaleOffdiag / Zeros (lmp/lmatrix_csr_cpu.cc:100-103,
+// 205-224) on an n x m CSR; the values in place.  mode 0 Scale, 1 ScaleOffdiag,
+// 2 Zeros.
+void ref_csr_scale(int n, int m, int nnz, const int *row, const int *col, double *val, double alpha, int mode)
+{
+    CPUsimple_CSR_lMatrix<double> A(nnz, n, m, "A");
+    std::memcpy(A.matrix.row, row, sizeof(int) * (n + 1));
+    std::memcpy(A.matrix.col, col, sizeof(int) * nnz);
+    std::memcpy(A.matrix.val, val, sizeof(double) * nnz);
+    if (mode == 0) A.Scale(alpha);
+    else if (mode == 1) A.ScaleOffdiag(alpha);
+    else A.Zeros();
+    std::memcpy(val, A.matrix.val, sizeof(double) * nnz);
+}
+
+// CPU_CSR_lMatrix::extract_diagelements / extract_invdiagelements
+// (lmp/lmatrix_csr_cpu.cc:2395-2431), rows [start, end) into out.
+void ref_csr_diag(int n, int m, int nnz, const int *row, const int *col, const double *val, int start, int end,
+                  int inverse, double *out)
+{
+    CPUsimple_CSR_lMatrix<double> A(nnz, n, m, "A");
+    std::memcpy(A.matrix.row, row, sizeof(int) * (n + 1));
+    std::memcpy(A.matrix.col, col, sizeof(int) * nnz);
+    std::memcpy(A.matrix.val, val, sizeof(double) * nnz);
+    CPUsimple_lVector<double> v(end - start, "d");
+    if (inverse) A.extract_invdiagelements(start, end, &v);
+    else A.extract_diagelements(start, end, &v);
+    copy_out(v, out);
+}
+
+// CPU_CSR_lMatrix::extract_submatrix (lmp/lmatrix_csr_cpu.cc:1768-1843) and
+// Compress (:142-202).  mode 0: the block [sr, er) x [sc, ec); mode 1: the
+// matrix without its zero entries.  Returns the result's nnz (-1 when cap is
+// too small), its row pointer (rows + 1 entries), columns and values out.
+int ref_csr_extract(int n, int m, int nnz, const int *row, const int *col, const double *val, int mode, int sr,
+                    int sc, int er, int ec, int cap, int *row_out, int *col_out, double *val_out)
+{
+    CPUsimple_CSR_lMatrix<double> A(nnz, n, m, "A");
+    std::memcpy(A.matrix.row, row, sizeof(int) * (n + 1));
+    std::memcpy(A.matrix.col, col, sizeof(int) * nnz);
+    std::memcpy(A.matrix.val, val, sizeof(double) * nnz);
+    const CPU_CSR_lMatrix<double> *c = &A;
+    lMatrix<double> *S = nullptr;
+    if (mode == 0) {
+        S = A.extract_submatrix(sr, sc, er, ec);
+        c = dynamic_cast<const CPU_CSR_lMatrix<double> *>(S);
+    } else {
+        A.Compress();
+    }
+    const int k = c->get_nnz(), rows = c->get_num_row();
+    int rc = -1;
+    if (k <= cap) {
+        std::memcpy(row_out, c->matrix.row, sizeof(int) * (rows + 1));
+        if (k) {
+            std::memcpy(col_out, c->matrix.col, sizeof(int) * k);
+            std::memcpy(val_out, c->matrix.val, sizeof(double) * k);
+        }
+        rc = k;
+    }
+    delete S;
+    return rc;
+}
+
 // CPU_lVector::WriteFile (lmp/lvector_cpu.cc:638-663).
 void ref_vec_write(const char *path, int n, const double *x)
 {

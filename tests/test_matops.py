@@ -1,0 +1,153 @@
+"""CSR_lMatrix value and structure operations: Scale, ScaleOffdiag, Zeros,
+extract_diagelements / extract_invdiagelements, extract_submatrix, Compress.
+
+Fixtures (tests/golden/matops_golden.npz, made by gen_matops_golden.py) hold
+the reference's own outputs (lmp/lmatrix_csr_cpu.cc:100-224, 1768-1843,
+2395-2431, its CPU code compiled unmodified) on random CSRs with unsorted
+rows, repeated columns and stored zeros, square and rectangular, and on a 2-D
+Q1 convection-diffusion system.  The oracle's restatement must equal them bit
+for bit (CPU), and so must the device operations (GPU).  Rows without a
+stored diagonal are left out of the diagonal comparisons: the reference
+writes an uninitialised value there.
+"""
+import os
+
+import numpy as np
+import pytest
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CASES = ["rand", "rect", "q1"]
+NBLOCKS = {"rand": 4, "rect": 3, "q1": 3}
+BLOCKS = {"rand": [(0, 0, 60, 60), (5, 7, 40, 33), (10, 0, 11, 60), (59, 59, 60, 60)],
+          "rect": [(0, 0, 50, 70), (3, 52, 47, 70), (20, 10, 30, 65)],
+          "q1": [(0, 0, 121, 121), (11, 11, 110, 110), (40, 30, 80, 95)]}
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(os.path.join(HERE, "golden", "matops_golden.npz"))
+
+
+def csr(gold, name):
+    return gold[f"{name}_row"], gold[f"{name}_col"], gold[f"{name}_val"], int(gold[f"{name}_m"])
+
+
+def bits(a):
+    return np.ascontiguousarray(a, np.float64).view(np.uint64)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_oracle_matops_match_reference(oracle, gold, name):
+    row, col, val, m = csr(gold, name)
+    alpha = float(gold["alpha"])
+    for mode in (0, 1, 2):
+        assert np.array_equal(bits(oracle.csr_scale(row, col, val, alpha, mode)), bits(gold[f"{name}_scale{mode}"]))
+    lo, hi = gold[f"{name}_diag_range"]
+    has = gold[f"{name}_has_diag"]
+    for inv in (0, 1):
+        d = oracle.csr_diag(row, col, val, int(lo), int(hi), inv)
+        assert np.array_equal(bits(d[has]), bits(gold[f"{name}_diag{inv}"][has]))
+    for k, blk in enumerate(BLOCKS[name]):
+        r, c, v = oracle.csr_extract(row, col, val, 0, *blk)
+        assert np.array_equal(r, gold[f"{name}_sub{k}_row"]) and np.array_equal(c, gold[f"{name}_sub{k}_col"])
+        assert np.array_equal(bits(v), bits(gold[f"{name}_sub{k}_val"]))
+    r, c, v = oracle.csr_extract(row, col, val, 1)
+    assert np.array_equal(r, gold[f"{name}_comp_row"]) and np.array_equal(c, gold[f"{name}_comp_col"])
+    assert np.array_equal(bits(v), bits(gold[f"{name}_comp_val"]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", CASES)
+def test_device_matops_match_reference(b200, gold, name):
+    pf = b200.Platform(0)
+    row, col, val, m = csr(gold, name)
+    n = len(row) - 1
+    alpha = float(gold["alpha"])
+    for mode, op in enumerate(("Scale", "ScaleOffdiag", "Zeros")):
+        A = b200.CSR_lMatrix.from_csr(pf, row, col, val, n_cols=m)
+        getattr(A, op)(*(() if op == "Zeros" else (alpha,)))
+        r, c, v = A.download()
+        assert np.array_equal(r, row) and np.array_equal(c, col)
+        assert np.array_equal(bits(v), bits(gold[f"{name}_scale{mode}"])), op
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val, n_cols=m)
+    lo, hi = (int(x) for x in gold[f"{name}_diag_range"])
+    has = gold[f"{name}_has_diag"]
+    for inv, op in enumerate(("extract_diagelements", "extract_invdiagelements")):
+        vec = pf.vector(np.full(hi - lo, -7.0))
+        getattr(A, op)(lo, hi, vec)
+        d = vec.numpy()
+        assert np.array_equal(bits(d[has]), bits(gold[f"{name}_diag{inv}"][has]))
+        assert np.all(d[~has] == -7.0)        # rows without a diagonal: untouched
+    for k, blk in enumerate(BLOCKS[name]):
+        S = A.extract_submatrix(*blk)
+        assert (S.n, S.m) == (blk[2] - blk[0], blk[3] - blk[1])
+        r, c, v = S.download()
+        assert np.array_equal(r, gold[f"{name}_sub{k}_row"]) and np.array_equal(c, gold[f"{name}_sub{k}_col"])
+        assert np.array_equal(bits(v), bits(gold[f"{name}_sub{k}_val"]))
+    A.Compress()
+    r, c, v = A.download()
+    assert np.array_equal(r, gold[f"{name}_comp_row"]) and np.array_equal(c, gold[f"{name}_comp_col"])
+    assert np.array_equal(bits(v), bits(gold[f"{name}_comp_val"]))
+
+
+@pytest.mark.gpu
+def test_device_scale_feeds_the_spmv_layouts(b200, oracle, gold):
+    """After ScaleOffdiag the SpMV (stencil layout for the Q1 operator, SELL
+    or CSR otherwise) multiplies with the new values: 1e-13 of the row's
+    magnitude sum against the oracle's SpMV of the reference's scaled values."""
+    pf = b200.Platform(0)
+    for name in ("q1", "rand"):
+        row, col, val, m = csr(gold, name)
+        if m != len(row) - 1:
+            continue
+        A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+        A.ScaleOffdiag(float(gold["alpha"]))
+        x = np.random.default_rng(3).uniform(-1, 1, m)
+        y = pf.vector(len(row) - 1)
+        A.VectorMult(pf.vector(x), y)
+        vs = gold[f"{name}_scale1"]
+        ref = oracle.spmv(row, col, vs, x)
+        scale = np.array([np.abs(vs[row[i]:row[i + 1]]) @ np.abs(x[col[row[i]:row[i + 1]]])
+                          for i in range(len(row) - 1)])
+        assert np.all(np.abs(y.numpy() - ref) <= 1e-13 * np.maximum(scale, 1e-300))
+
+
+@pytest.mark.gpu
+def test_device_matops_fp32(b200, gold):
+    """FP32 matrices: the same operations in float arithmetic (Scale and
+    ScaleOffdiag products, 1 / a_ii in float) and the same submatrix
+    structure; the Q1 operator has no repeated columns, so its block values
+    are the float copies of the FP64 ones."""
+    pf = b200.Platform(0)
+    row, col, val, m = csr(gold, "q1")
+    v32 = val.astype(np.float32)
+    a32 = np.float32(gold["alpha"])
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, v32, dtype=b200.F32)
+    A.ScaleOffdiag(float(gold["alpha"]))
+    exp = v32.copy()
+    off = col != np.repeat(np.arange(len(row) - 1), np.diff(row))
+    exp[off] = exp[off] * a32
+    assert np.array_equal(A.download()[2].view(np.uint32), exp.view(np.uint32))
+    B = b200.CSR_lMatrix.from_csr(pf, row, col, v32, dtype=b200.F32)
+    lo, hi = (int(x) for x in gold["q1_diag_range"])
+    vec = pf.vector(hi - lo, b200.F32)
+    B.extract_invdiagelements(lo, hi, vec)
+    dg = np.array([v32[row[i]:row[i + 1]][col[row[i]:row[i + 1]] == i][-1] for i in range(lo, hi)])
+    assert np.array_equal(vec.numpy().view(np.uint32), (np.float32(1) / dg).view(np.uint32))
+    S = B.extract_submatrix(*BLOCKS["q1"][2])
+    r, c, v = S.download()
+    assert np.array_equal(r, gold["q1_sub2_row"]) and np.array_equal(c, gold["q1_sub2_col"])
+    assert np.array_equal(v.view(np.uint32), gold["q1_sub2_val"].astype(np.float32).view(np.uint32))
+
+
+@pytest.mark.gpu
+def test_device_matops_reject_bad_ranges(b200, gold):
+    pf = b200.Platform(0)
+    row, col, val, m = csr(gold, "rect")
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val, n_cols=m)
+    for blk in [(5, 5, 5, 10), (0, 0, 51, 10), (0, 60, 10, 71), (-1, 0, 3, 3), (3, 9, 2, 12)]:
+        with pytest.raises(b200.B200Error) as e:
+            A.extract_submatrix(*blk)
+        assert e.value.code == b200.ERR_ARG
+    with pytest.raises(b200.B200Error):
+        A.extract_diagelements(10, 51, pf.vector(41))
