@@ -136,6 +136,13 @@ def lib():
         "b200la_csr_set_values": ([_P, _P, _P], _I),
         "b200la_csr_invdiag": ([_P, _P, _P], _I),
         "b200la_csr_scale": ([_P, _P, _D, _I], _I),
+        "b200la_iamin": ([_P, _I, _I, _P, C.POINTER(_I)], _I),
+        "b200la_iamax": ([_P, _I, _I, _P, C.POINTER(_I)], _I),
+        "b200la_normmax": ([_P, _I, _I, _P, C.POINTER(_D)], _I),
+        "b200la_asum": ([_P, _I, _I, _P, C.POINTER(_D)], _I),
+        "b200la_rot": ([_P, _I, _I, _P, _P, _D, _D], _I),
+        "b200la_rotm": ([_P, _I, _I, _P, _P, C.POINTER(_D)], _I),
+        "b200la_rotg": ([_I, _P, _P, _P, _P], _I),
         "b200la_csr_diag": ([_P, _P, _I, _I, _I, _P], _I),
         "b200la_csr_extract_submatrix": ([_P, _P, _I, _I, _I, _I, C.POINTER(_P)], _I),
         "b200la_csr_compress": ([_P, _P, C.POINTER(_P)], _I),
@@ -535,6 +542,45 @@ class lVector:
         out = C.c_double()
         self.pf.check(lib().b200la_nrm2(self.pf.h, self.dtype, self.get_size(), self.ptr, C.byref(out)), "Norm2")
         return out.value
+
+    def ArgMin(self):
+        """First index of the smallest |x_i| (CPUsimple_lvector.cc:51-70)."""
+        out = C.c_int()
+        self.pf.check(lib().b200la_iamin(self.pf.h, self.dtype, self.get_size(), self.ptr, C.byref(out)), "ArgMin")
+        return out.value
+
+    def ArgMax(self):
+        """First index of the largest |x_i| (CPUsimple_lvector.cc:73-92)."""
+        out = C.c_int()
+        self.pf.check(lib().b200la_iamax(self.pf.h, self.dtype, self.get_size(), self.ptr, C.byref(out)), "ArgMax")
+        return out.value
+
+    def NormMax(self):
+        out = C.c_double()
+        self.pf.check(lib().b200la_normmax(self.pf.h, self.dtype, self.get_size(), self.ptr, C.byref(out)),
+                      "NormMax")
+        return out.value
+
+    def Norm1(self):
+        out = C.c_double()
+        self.pf.check(lib().b200la_asum(self.pf.h, self.dtype, self.get_size(), self.ptr, C.byref(out)), "Norm1")
+        return out.value
+
+    def Rot(self, vec, sc, ss):
+        """self, vec <- sc self + ss vec, sc vec - ss self (CPUsimple_lvector.cc:448-466)."""
+        self.pf.check(lib().b200la_rot(self.pf.h, self.dtype, self.get_size(), self.ptr, vec.ptr, sc, ss), "Rot")
+
+    def Rotm(self, vec, sparam):
+        """The modified Givens rotation sparam = (flag, h11, h21, h12, h22) (CPUsimple_lvector.cc:540-600)."""
+        p = (C.c_double * 5)(*[float(v) for v in sparam])
+        self.pf.check(lib().b200la_rotm(self.pf.h, self.dtype, self.get_size(), self.ptr, vec.ptr, p), "Rotm")
+
+    def Rotg(self, sa, sb):
+        """Givens rotation of (sa, sb) (CPUsimple_lvector.cc:492-535): returns (r, z, c, s)."""
+        T = C.c_double if self.dtype == F64 else C.c_float
+        v = [T(sa), T(sb), T(), T()]
+        _check(lib().b200la_rotg(self.dtype, *[C.cast(C.byref(q), C.c_void_p) for q in v]), "Rotg")
+        return tuple(q.value for q in v)
 
     def Axpy(self, vec, scalar):
         self.pf.check(lib().b200la_axpy(self.pf.h, self.dtype, self.get_size(), scalar, vec.ptr, self.ptr), "Axpy")

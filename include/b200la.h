@@ -200,6 +200,24 @@ int b200la_gmg_prolongation_add(b200la_ctx *ctx, const b200la_csr *P_diag, const
  * cuda/GPUblas_lvector.cu:204-220).  Result to a HOST double (synchronises). */
 int b200la_dot(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, double *result);
 int b200la_nrm2(b200la_ctx *ctx, int dtype, int n, const void *x, double *result);
+/* lVector::ArgMin / ArgMax (src/linear_algebra/lmp/CPUsimple_lvector.cc:51-92):
+ * the first index of the smallest / largest |x_i| (a NaN is never chosen,
+ * except at index 0, as in the reference's scan); NormMax (:154-158): that
+ * largest |x_i|; Norm1 (:95-151): sum |x_i| (FP64 tree order).  n >= 1 for
+ * the first three.  Results to HOST memory (synchronises). */
+int b200la_iamin(b200la_ctx *ctx, int dtype, int n, const void *x, int *result);
+int b200la_iamax(b200la_ctx *ctx, int dtype, int n, const void *x, int *result);
+int b200la_normmax(b200la_ctx *ctx, int dtype, int n, const void *x, double *result);
+int b200la_asum(b200la_ctx *ctx, int dtype, int n, const void *x, double *result);
+/* lVector::Rot (:448-466): x_i, y_i <- c x_i + s y_i, c y_i - s x_i, with x
+ * the vector the method is called on.  Rotm (:540-600): the modified Givens
+ * rotation param[0..4] = (flag, h11, h21, h12, h22) (HOST array) applied to
+ * the pairs (y_i, x_i); flag -2 (or any value but -1, 0, 1) changes nothing.
+ * Each product and sum rounded on its own, as in the reference. */
+int b200la_rot(b200la_ctx *ctx, int dtype, int n, void *x, void *y, double c, double s);
+int b200la_rotm(b200la_ctx *ctx, int dtype, int n, void *x, void *y, const double *param);
+/* lVector::Rotg (:492-535) on HOST scalars of the dtype. */
+int b200la_rotg(int dtype, void *a, void *b, void *c, void *s);
 /* Same, result to a DEVICE double, no synchronisation. */
 int b200la_dot_dev(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, double *result_dev);
 /* Dot product x . y written to *result_dev (a DEVICE double) without a

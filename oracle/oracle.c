@@ -1231,3 +1231,98 @@ int orc_csr_extract(int n, const int *row, const int *col, const double *val, in
     *val_out = vo;
     return cnt;
 }
+
+/* ------------------------------------------------------------------ */
+/* lVector BLAS1 members beyond the Krylov hot path                    */
+/* ------------------------------------------------------------------ */
+
+/* CPUsimple_lVector::ArgMin (lmp/CPUsimple_lvector.cc:51-70). */
+int orc_iamin(int n, const double *x)
+{
+    int k = 0;
+    double v = fabs(x[0]);
+    for (int i = 1; i < n; ++i)
+        if (fabs(x[i]) < v) { k = i; v = fabs(x[i]); }
+    return k;
+}
+
+/* CPUsimple_lVector::ArgMax (:73-92). */
+int orc_iamax(int n, const double *x)
+{
+    int k = 0;
+    double v = fabs(x[0]);
+    for (int i = 1; i < n; ++i)
+        if (fabs(x[i]) > v) { k = i; v = fabs(x[i]); }
+    return k;
+}
+
+/* CPUsimple_lVector::Norm1 (:95-151): the n % 5 leading terms one by one,
+ * then groups of five summed left to right and added. */
+double orc_asum(int n, const double *x)
+{
+    const int m = n % 5;
+    double t = 0.0;
+    if (m == 0) {
+        for (int i = 0; i < n; i += 5)
+            t += fabs(x[i]) + fabs(x[i + 1]) + fabs(x[i + 2]) + fabs(x[i + 3]) + fabs(x[i + 4]);
+    } else {
+        for (int i = 0; i < m; ++i) t += fabs(x[i]);
+        if (n > 5)
+            for (int i = m; i < n; i += 5)
+                t += fabs(x[i]) + fabs(x[i + 1]) + fabs(x[i + 2]) + fabs(x[i + 3]) + fabs(x[i + 4]);
+    }
+    return t;
+}
+
+/* CPUsimple_lVector::Rot (:448-466). */
+void orc_rot(int n, double *x, double *y, double c, double s)
+{
+    for (int i = 0; i < n; ++i) {
+        const double t = c * x[i] + s * y[i];
+        y[i] = c * y[i] - s * x[i];
+        x[i] = t;
+    }
+}
+
+/* CPUsimple_lVector::Rotm (:540-600): flag -2 leaves both vectors. */
+void orc_rotm(int n, double *x, double *y, const double *param)
+{
+    const double flag = param[0];
+    for (int i = 0; i < n; ++i) {
+        const double t1 = y[i], t2 = x[i];
+        if (flag == -1) {
+            y[i] = t1 * param[1] + t2 * param[3];
+            x[i] = t1 * param[2] + t2 * param[4];
+        } else if (flag == 0) {
+            y[i] = t1 + t2 * param[3];
+            x[i] = t1 * param[2] + t2;
+        } else if (flag == 1) {
+            y[i] = t1 * param[1] + t2;
+            x[i] = t2 * param[4] - t1;
+        }
+    }
+}
+
+/* CPUsimple_lVector::Rotg (:492-535). */
+void orc_rotg(double *a, double *b, double *c, double *s)
+{
+    const double ta = fabs(*a), tb = fabs(*b);
+    const double roe = ta > tb ? *a : *b;
+    const double scal = ta + tb;
+    if (scal == 0) {
+        *c = 1;
+        *s = *a = *b = 0;
+        return;
+    }
+    const double t0 = ta / scal, t1 = tb / scal;
+    double r = scal * sqrt(t0 * t0 + t1 * t1);
+    if (roe < 0) r = -r;
+    *c = *a / r;
+    *s = *b / r;
+    double z;
+    if (ta > tb) z = *s;
+    else if (*c != 0) z = 1 / *c;
+    else z = 1;
+    *a = r;
+    *b = z;
+}

@@ -185,6 +185,24 @@ void orc_block_apply(const orc_block_precond *P, const double *r, double *z);
 void orc_block_free(orc_block_precond *P);
 
 /* ------------------------------------------------------------------ */
+/* lVector BLAS1 members beyond the Krylov hot path                    */
+/* (lmp/CPUsimple_lvector.cc)                                          */
+/* ------------------------------------------------------------------ */
+
+/* ArgMin / ArgMax (:51-92): first index of the smallest / largest |x_i|. */
+int orc_iamin(int n, const double *x);
+int orc_iamax(int n, const double *x);
+/* Norm1 (:95-151): sum |x_i| in the reference's unroll-by-5 order. */
+double orc_asum(int n, const double *x);
+/* Rot (:448-466): x_i, y_i <- c x_i + s y_i, c y_i - s x_i. */
+void orc_rot(int n, double *x, double *y, double c, double s);
+/* Rotm (:540-600): the modified Givens rotation param[0..4] (flag, h11, h21,
+ * h12, h22) applied to the pairs (y_i, x_i). */
+void orc_rotm(int n, double *x, double *y, const double *param);
+/* Rotg (:492-535). */
+void orc_rotg(double *a, double *b, double *c, double *s);
+
+/* ------------------------------------------------------------------ */
 /* Matrix value and structure operations (lmp/lmatrix_csr_cpu.cc)       */
 /* ------------------------------------------------------------------ */
 

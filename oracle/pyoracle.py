@@ -137,6 +137,15 @@ class Oracle:
         L.orc_ilup.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_int, _pp, _pp, _dp]
         L.orc_free.argtypes = [C.c_void_p]
         L.orc_csr_scale.argtypes = [C.c_int, _i32p, _i32p, _f64p, C.c_double, C.c_int]
+        L.orc_iamin.argtypes = L.orc_iamax.argtypes = [C.c_int, _f64p]
+        L.orc_asum.argtypes = [C.c_int, _f64p]
+        L.orc_asum.restype = C.c_double
+        L.orc_rot.argtypes = [C.c_int, _f64p, _f64p, C.c_double, C.c_double]
+        L.orc_rot.restype = None
+        L.orc_rotm.argtypes = [C.c_int, _f64p, _f64p, _f64p]
+        L.orc_rotm.restype = None
+        L.orc_rotg.argtypes = [C.POINTER(C.c_double)] * 4
+        L.orc_rotg.restype = None
         L.orc_csr_scale.restype = None
         L.orc_csr_diag.argtypes = [_i32p, _i32p, _f64p, C.c_int, C.c_int, C.c_int, _f64p]
         L.orc_csr_diag.restype = None
@@ -324,6 +333,27 @@ class Oracle:
             self.lib.orc_free(C.cast(q, C.c_void_p))
         return out
 
+    def vec_reduce(self, x):
+        """ArgMin, ArgMax, Norm1, NormMax of x."""
+        x = _f64(x)
+        n = x.size
+        k = self.lib.orc_iamax(n, x)
+        return self.lib.orc_iamin(n, x), k, self.lib.orc_asum(n, x), abs(x[k])
+
+    def rot(self, x, y, c=None, s=None, param=None):
+        """Rot (c, s) or Rotm (param); returns the new (x, y)."""
+        x, y = _f64(x).copy(), _f64(y).copy()
+        if param is None:
+            self.lib.orc_rot(x.size, x, y, c, s)
+        else:
+            self.lib.orc_rotm(x.size, x, y, _f64(param))
+        return x, y
+
+    def rotg(self, a, b):
+        v = [C.c_double(a), C.c_double(b), C.c_double(), C.c_double()]
+        self.lib.orc_rotg(*[C.byref(q) for q in v])
+        return tuple(q.value for q in v)
+
     def csr_scale(self, row, col, val, alpha, mode):
         """Scale (mode 0), ScaleOffdiag (1), Zeros (2): the new values."""
         v = _f64(val).copy()
@@ -457,6 +487,13 @@ class Ref:
         L.ref_time_spmv.restype = C.c_double
         L.ref_max_threads.restype = C.c_int
         L.ref_csr_scale.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, C.c_double, C.c_int]
+        L.ref_vec_reduce.argtypes = [C.c_int, _f64p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                     C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.ref_vec_reduce.restype = None
+        L.ref_vec_rot.argtypes = [C.c_int, _f64p, _f64p, C.c_double, C.c_double, C.c_void_p]
+        L.ref_vec_rot.restype = None
+        L.ref_rotg.argtypes = [C.POINTER(C.c_double)] * 4
+        L.ref_rotg.restype = None
         L.ref_csr_scale.restype = None
         L.ref_csr_diag.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, C.c_int, C.c_int, C.c_int, _f64p]
         L.ref_csr_diag.restype = None
@@ -556,6 +593,22 @@ class Ref:
         m = self.lib.ref_ilup(n, nnz, _i32(row), _i32(col), _f64(val), p, cap, r, c, v)
         assert m >= 0
         return r, c[:m].copy(), v[:m].copy()
+
+    def vec_reduce(self, x):
+        a, b, c, d = C.c_int(), C.c_int(), C.c_double(), C.c_double()
+        self.lib.ref_vec_reduce(len(x), _f64(x), C.byref(a), C.byref(b), C.byref(c), C.byref(d))
+        return a.value, b.value, c.value, d.value
+
+    def rot(self, x, y, c=0.0, s=0.0, param=None):
+        x, y = _f64(x).copy(), _f64(y).copy()
+        p = None if param is None else _f64(param)
+        self.lib.ref_vec_rot(x.size, x, y, c, s, None if p is None else p.ctypes.data)
+        return x, y
+
+    def rotg(self, a, b):
+        v = [C.c_double(a), C.c_double(b), C.c_double(), C.c_double()]
+        self.lib.ref_rotg(*[C.byref(q) for q in v])
+        return tuple(q.value for q in v)
 
     def csr_scale(self, row, col, val, alpha, mode, m=None):
         n = len(row) - 1

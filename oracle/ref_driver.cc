@@ -626,6 +626,41 @@ int ref_vec_read(const char *path, double *x, int cap)
     return n;
 }
 
+// CPUsimple_lVector::ArgMin / ArgMax / Norm1 / NormMax (lmp/CPUsimple_lvector.cc:51-158).
+void ref_vec_reduce(int n, const double *x, int *argmin, int *argmax, double *norm1, double *normmax)
+{
+    CPUsimple_lVector<double> v(n, "x");
+    for (int i = 0; i < n; ++i) v.buffer[i] = x[i];
+    *argmin = v.ArgMin();
+    *argmax = v.ArgMax();
+    *norm1 = v.Norm1();
+    *normmax = v.NormMax();
+}
+
+// CPUsimple_lVector::Rot (:448-466) and Rotm (:540-600) with x the vector the
+// method is called on and y its argument; both in place.
+void ref_vec_rot(int n, double *x, double *y, double c, double s, const double *param)
+{
+    CPUsimple_lVector<double> vx(n, "x"), vy(n, "y");
+    for (int i = 0; i < n; ++i) {
+        vx.buffer[i] = x[i];
+        vy.buffer[i] = y[i];
+    }
+    if (param) vx.Rotm(&vy, param[0]);
+    else vx.Rot(&vy, c, s);
+    for (int i = 0; i < n; ++i) {
+        x[i] = vx.buffer[i];
+        y[i] = vy.buffer[i];
+    }
+}
+
+// CPUsimple_lVector::Rotg (:492-535) on host scalars.
+void ref_rotg(double *a, double *b, double *c, double *s)
+{
+    CPUsimple_lVector<double> v(1, "x");
+    v.Rotg(a, b, c, s);
+}
+
 // CPU_CSR_lMatrix::Scale / ScaleOffdiag / Zeros (lmp/lmatrix_csr_cpu.cc:100-103,
 // 205-224) on an n x m CSR; the values in place.  mode 0 Scale, 1 ScaleOffdiag,
 // 2 Zeros.

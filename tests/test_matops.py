@@ -1,12 +1,16 @@
-"""CSR_lMatrix value and structure operations: Scale, ScaleOffdiag, Zeros,
-extract_diagelements / extract_invdiagelements, extract_submatrix, Compress.
+"""CSR_lMatrix value and structure operations (Scale, ScaleOffdiag, Zeros,
+extract_diagelements / extract_invdiagelements, extract_submatrix, Compress)
+and the lVector BLAS1 members beyond the Krylov path (ArgMin, ArgMax, Norm1,
+NormMax, Rot, Rotm, Rotg).
 
 Fixtures (tests/golden/matops_golden.npz, made by gen_matops_golden.py) hold
 the reference's own outputs (lmp/lmatrix_csr_cpu.cc:100-224, 1768-1843,
 2395-2431, its CPU code compiled unmodified) on random CSRs with unsorted
 rows, repeated columns and stored zeros, square and rectangular, and on a 2-D
-Q1 convection-diffusion system.  The oracle's restatement must equal them bit
-for bit (CPU), and so must the device operations (GPU).  Rows without a
+Q1 convection-diffusion system, and of CPUsimple_lvector.cc:51-158, 448-600
+on seeded vectors.  The oracle's restatement must equal them bit for bit
+(CPU), and so must the device operations (GPU); Norm1 is summed in a
+different order on the device and agrees within 1e-14 relative.  Rows without a
 stored diagonal are left out of the diagonal comparisons: the reference
 writes an uninitialised value there.
 """
@@ -151,3 +155,89 @@ def test_device_matops_reject_bad_ranges(b200, gold):
         assert e.value.code == b200.ERR_ARG
     with pytest.raises(b200.B200Error):
         A.extract_diagelements(10, 51, pf.vector(41))
+
+
+NVEC = 4
+
+
+def test_oracle_vecops_match_reference(oracle, gold):
+    for k in range(NVEC):
+        x, y = gold[f"vec{k}_x"], gold[f"vec{k}_y"]
+        ref = gold[f"vec{k}_reduce"]
+        got = oracle.vec_reduce(x)
+        assert (got[0], got[1]) == (int(ref[0]), int(ref[1]))
+        assert bits(np.array(got[2:])).tolist() == bits(ref[2:]).tolist()
+        for j, (c, s) in enumerate([(0.6, 0.8), (-0.3, 0.95)]):
+            xo, yo = oracle.rot(x, y, c, s)
+            assert np.array_equal(bits(xo), bits(gold[f"vec{k}_rot{j}_x"]))
+            assert np.array_equal(bits(yo), bits(gold[f"vec{k}_rot{j}_y"]))
+    for (a, b), ref in zip(gold["rotg_in"], gold["rotg_out"]):
+        assert bits(np.array(oracle.rotg(a, b))).tolist() == bits(ref).tolist()
+
+
+ROTM = [(-1, 0.3, -0.7, 1.2, 0.9), (0, 9, 0.25, -0.5, 9), (1, 1.5, 9, 9, -0.4), (-2, 1, 2, 3, 4)]
+
+
+@pytest.mark.gpu
+def test_device_vecops_match_reference(b200, gold):
+    pf = b200.Platform(0)
+    for k in range(NVEC):
+        x, y = gold[f"vec{k}_x"], gold[f"vec{k}_y"]
+        ref = gold[f"vec{k}_reduce"]
+        xv = pf.vector(x)
+        assert xv.ArgMin() == int(ref[0]) and xv.ArgMax() == int(ref[1])
+        assert bits(np.array([xv.NormMax()])) == bits(ref[3:4])
+        assert abs(xv.Norm1() - ref[2]) <= 1e-14 * ref[2]
+        for j, (c, s) in enumerate([(0.6, 0.8), (-0.3, 0.95)]):
+            a, b = pf.vector(x), pf.vector(y)
+            a.Rot(b, c, s)
+            assert np.array_equal(bits(a.numpy()), bits(gold[f"vec{k}_rot{j}_x"]))
+            assert np.array_equal(bits(b.numpy()), bits(gold[f"vec{k}_rot{j}_y"]))
+        for j, prm in enumerate(ROTM):
+            a, b = pf.vector(x), pf.vector(y)
+            a.Rotm(b, prm)
+            assert np.array_equal(bits(a.numpy()), bits(gold[f"vec{k}_rotm{j}_x"])), prm
+            assert np.array_equal(bits(b.numpy()), bits(gold[f"vec{k}_rotm{j}_y"])), prm
+    for (a, b), ref in zip(gold["rotg_in"], gold["rotg_out"]):
+        assert bits(np.array(pf.vector(1).Rotg(a, b))).tolist() == bits(ref).tolist()
+
+
+@pytest.mark.gpu
+def test_device_argmin_argmax_ties_and_nans(b200, oracle):
+    """Large vectors (many CTAs): the first index of the extreme magnitude
+    wins across CTAs; NaNs are skipped, except a NaN at index 0, which the
+    reference's scan keeps."""
+    pf = b200.Platform(0)
+    rng = np.random.default_rng(12)
+    n = 3_000_001
+    x = rng.uniform(-1, 1, n)
+    x[[5, 2_000_000, 2_999_999]] = -7.5          # the largest magnitude three times
+    x[[17, 1_500_000]] = 1e-300                  # the smallest twice
+    x[[100, 2_500_000]] = np.nan
+    xv = pf.vector(x)
+    assert (xv.ArgMin(), xv.ArgMax()) == (oracle.vec_reduce(x)[0], oracle.vec_reduce(x)[1]) == (17, 5)
+    assert xv.NormMax() == 7.5
+    x[0] = np.nan
+    xv = pf.vector(x)
+    assert (xv.ArgMin(), xv.ArgMax()) == (0, 0) == oracle.vec_reduce(x)[:2]
+    x32 = rng.standard_normal(100_003).astype(np.float32)
+    x32[[9, 99_999]] = np.float32(-40.0)
+    v32 = pf.vector(x32, b200.F32)
+    assert v32.ArgMax() == 9 and v32.NormMax() == 40.0
+    assert v32.ArgMin() == int(np.argmin(np.abs(x32)))
+
+
+@pytest.mark.gpu
+def test_device_rot_fp32(b200):
+    """FP32 Rot and Rotm: every product and sum rounded to float on its own."""
+    pf = b200.Platform(0)
+    rng = np.random.default_rng(4)
+    x, y = rng.standard_normal(4099).astype(np.float32), rng.standard_normal(4099).astype(np.float32)
+    c, s = np.float32(0.6), np.float32(0.8)
+    a, b = pf.vector(x, b200.F32), pf.vector(y, b200.F32)
+    a.Rot(b, 0.6, 0.8)
+    assert np.array_equal(a.numpy(), c * x + s * y) and np.array_equal(b.numpy(), c * y - s * x)
+    h = np.array([-1, 0.3, -0.7, 1.2, 0.9], np.float32)
+    a, b = pf.vector(x, b200.F32), pf.vector(y, b200.F32)
+    a.Rotm(b, h)
+    assert np.array_equal(b.numpy(), y * h[1] + x * h[3]) and np.array_equal(a.numpy(), y * h[2] + x * h[4])
