@@ -176,10 +176,24 @@ def cpu_counts(N):
     return None
 
 
-def cpu_baseline(row, col, val, b, outer, inner_total, fp64_iters):
+def cpu_estimate(ref, pyoracle, row, col, val, b, threads, outer, inner_total, fp64_iters, s1=4, s2=16):
+    """The reference's MPIR timed with `threads` OpenMP threads on its first
+    correction cut at s1 and s2 inner iterations, fitted linearly and scaled to
+    the full solve's counts; its FP64 Jacobi-CG per iteration likewise."""
+    a = pyoracle.ref_mpir(ref, row, col, val, b, threads, sample_inner=s1)
+    c = pyoracle.ref_mpir(ref, row, col, val, b, threads, sample_inner=s2)
+    per_inner = max((c["seconds"] - a["seconds"]) / (s2 - s1), 1e-9)
+    per_outer = max(a["seconds"] - s1 * per_inner, 0.0)   # residuals, casts, update of one correction
+    p = pyoracle.ref_pcg_timed(ref, row, col, val, b, threads, maxits=s2)
+    return dict(per_inner=per_inner, per_outer=per_outer, est=outer * per_outer + inner_total * per_inner,
+                fp64_est=p["seconds"] / max(p["iters"], 1) * fp64_iters, fp64_iters=p["iters"])
+
+
+def cpu_baseline(row, col, val, b, outer, inner_total, fp64_iters, single_thread=False):
     """The reference's own CPU code (oracle/_ref: HiFlow3's CPUopenmp lmp
     objects driving the restated MPIR and CG loops), timed on a bounded sample
-    and scaled to the full solve's iteration counts."""
+    and scaled to the full solve's iteration counts, with every host thread
+    (and, with single_thread, also with one)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
     threads = len(os.sched_getaffinity(0))
@@ -187,19 +201,19 @@ def cpu_baseline(row, col, val, b, outer, inner_total, fp64_iters):
         return None
     ref = pyoracle.Ref()
     s1, s2 = 4, 16
-    a = pyoracle.ref_mpir(ref, row, col, val, b, threads, sample_inner=s1)
-    c = pyoracle.ref_mpir(ref, row, col, val, b, threads, sample_inner=s2)
-    per_inner = max((c["seconds"] - a["seconds"]) / (s2 - s1), 1e-9)
-    per_outer = max(a["seconds"] - s1 * per_inner, 0.0)   # residuals, casts, update of one correction
-    est = outer * per_outer + inner_total * per_inner
-    p = pyoracle.ref_pcg_timed(ref, row, col, val, b, threads, maxits=16)
-    fp64_est = p["seconds"] / max(p["iters"], 1) * fp64_iters
-    return dict(value=1.0 / est, unit=UNIT, cores=threads, kind="reference",
-                sample=(f"reference CPUopenmp lmp MPIR: first correction cut at {s1} and {s2} FP32 inner "
-                        f"iterations (linear fit: {per_inner * 1e3:.1f} ms/inner iteration, "
-                        f"{per_outer * 1e3:.1f} ms/correction overhead) scaled to {outer} corrections and "
-                        f"{inner_total} inner iterations"),
-                est_solve_s=est, fp64_cg_est_s=fp64_est, fp64_cg_sample_iters=p["iters"])
+    e = cpu_estimate(ref, pyoracle, row, col, val, b, threads, outer, inner_total, fp64_iters, s1, s2)
+    est = e["est"]
+    out = dict(value=1.0 / est, unit=UNIT, cores=threads, kind="reference",
+               sample=(f"reference CPUopenmp lmp MPIR: first correction cut at {s1} and {s2} FP32 inner "
+                       f"iterations (linear fit: {e['per_inner'] * 1e3:.1f} ms/inner iteration, "
+                       f"{e['per_outer'] * 1e3:.1f} ms/correction overhead) scaled to {outer} corrections and "
+                       f"{inner_total} inner iterations"),
+               est_solve_s=est, fp64_cg_est_s=e["fp64_est"], fp64_cg_sample_iters=e["fp64_iters"])
+    if single_thread:
+        e1 = cpu_estimate(ref, pyoracle, row, col, val, b, 1, outer, inner_total, fp64_iters, s1, s2)
+        out["one_thread"] = dict(value=1.0 / e1["est"], unit=UNIT, cores=1, est_solve_s=e1["est"],
+                                 ms_per_inner_iteration=e1["per_inner"] * 1e3, fp64_cg_est_s=e1["fp64_est"])
+    return out
 
 
 def run_reference(args):
@@ -432,7 +446,8 @@ def run_b200(args, rank, world, local_rank, dist):
         line["serving"] = serving_bench(b200, pf, args.serve_requests, rank=rank, world=world,
                                         dist=dist if world > 1 else None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(row, col, val, b, res_mixed["outer"], res_mixed["inner_total"], fp64_iters)
+        cb = cpu_baseline(row, col, val, b, res_mixed["outer"], res_mixed["inner_total"], fp64_iters,
+                          single_thread=True)
         line["cpu_baseline"] = cb if cb else {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                               "sample": "oracle/_ref missing"}
     pf.close()
