@@ -143,6 +143,8 @@ def lib():
         "b200la_rot": ([_P, _I, _I, _P, _P, _D, _D], _I),
         "b200la_rotm": ([_P, _I, _I, _P, _P, C.POINTER(_D)], _I),
         "b200la_rotg": ([_I, _P, _P, _P, _P], _I),
+        "b200la_vec_add_values": ([_P, _I, _I, _P, _I, _P, _P], _I),
+        "b200la_vec_set_values": ([_P, _I, _I, _P, _I, _P, _P], _I),
         "b200la_csr_diag": ([_P, _P, _I, _I, _I, _P], _I),
         "b200la_csr_extract_submatrix": ([_P, _P, _I, _I, _I, _I, C.POINTER(_P)], _I),
         "b200la_csr_compress": ([_P, _P, C.POINTER(_P)], _I),
@@ -616,6 +618,88 @@ class lVector:
         self.pf.check(lib().b200la_scatter(self.pf.h, self.dtype, idx_t.numel(), C.c_void_p(idx_t.data_ptr()),
                                            C.c_void_p(v.data_ptr()), self.ptr), "SetIndexedValues")
         self.pf.sync()
+
+    # index and range access (src/linear_algebra/lmp/lvector_cpu.cc:114-200, 419-550)
+    def _at(self, i):
+        return C.c_void_p(self.t.data_ptr() + i * self.t.element_size())
+
+    def _host(self, values, n):
+        a = np.ascontiguousarray(values, dtype=np.float64 if self.dtype == F64 else np.float32).reshape(-1)
+        if a.size != n:
+            raise ValueError("values has the wrong length")
+        return a
+
+    def _range(self, start, end):
+        if not 0 <= start <= end <= self.get_size():
+            raise B200Error(1, "range outside the vector")
+
+    def SetValues(self, index, values):
+        """x[index[k]] = values[k] (a repeated index keeps its last value)."""
+        idx = _i32(index)
+        v = self._host(values, idx.size)
+        self.pf.check(lib().b200la_vec_set_values(self.pf.h, self.dtype, self.get_size(), self.ptr, idx.size,
+                                                  _np_ptr(idx), _np_ptr(v)), "SetValues")
+
+    def GetValues(self, index):
+        """x[index[k]] for every k."""
+        return self.GetIndexedValues(index)
+
+    def add_values(self, indices, values):
+        """x[indices[k]] += values[k] in order (lvector_cpu.cc:123-135)."""
+        idx = _i32(indices)
+        v = self._host(values, idx.size)
+        self.pf.check(lib().b200la_vec_add_values(self.pf.h, self.dtype, self.get_size(), self.ptr, idx.size,
+                                                  _np_ptr(idx), _np_ptr(v)), "add_values")
+
+    def add_value(self, i, val):
+        self.add_values([i], [val])
+
+    def SetBlockValues(self, start, end, values):
+        """x[start:end] = values."""
+        self._range(start, end)
+        v = self._host(values, end - start)
+        if end > start:
+            self.pf.check(lib().b200la_memcpy_h2d(self.pf.h, self._at(start), _np_ptr(v), v.nbytes), "SetBlockValues")
+            self.pf.sync()
+
+    def GetBlockValues(self, start, end):
+        self._range(start, end)
+        out = np.empty(end - start, np.float64 if self.dtype == F64 else np.float32)
+        if end > start:
+            self.pf.check(lib().b200la_memcpy_d2h(self.pf.h, _np_ptr(out), self._at(start), out.nbytes),
+                          "GetBlockValues")
+        return out
+
+    def extract_subvector(self, start, end):
+        """A new vector holding x[start:end] (lvector_cpu.cc:419-457)."""
+        self._range(start, end)
+        sub = lVector(self.pf, _torch().empty(end - start, dtype=self.t.dtype, device=self.t.device))
+        if end > start:
+            self.pf.check(lib().b200la_memcpy_d2d(self.pf.h, sub.ptr, self._at(start), (end - start) *
+                                                  self.t.element_size()), "extract_subvector")
+        return sub
+
+    def partial_replace_subvector(self, start_i, start_sub, size, sub):
+        """x[start_i + k] = sub[start_sub + k], k < size (lvector_cpu.cc:460-500)."""
+        self._range(start_i, start_i + size)
+        sub._range(start_sub, start_sub + size)
+        if size:
+            self.pf.check(lib().b200la_memcpy_d2d(self.pf.h, self._at(start_i), sub._at(start_sub),
+                                                  size * self.t.element_size()), "partial_replace_subvector")
+
+    def partial_add_subvector(self, start_i, start_sub, size, weight, sub):
+        """x[start_i + k] += weight sub[start_sub + k], k < size (lvector_cpu.cc:504-545)."""
+        self._range(start_i, start_i + size)
+        sub._range(start_sub, start_sub + size)
+        if size:
+            self.pf.check(lib().b200la_axpy(self.pf.h, self.dtype, size, weight, sub._at(start_sub),
+                                            self._at(start_i)), "partial_add_subvector")
+
+    def CopyTo(self, other):
+        other.CopyFrom(self)
+
+    def CastTo(self, other):
+        other.CastFrom(self)
 
     def Reorder(self, perm):
         """out[i] = in[perm[i]] (CPU_lVector::Reorder, lvector_cpu.cc:75-94)."""

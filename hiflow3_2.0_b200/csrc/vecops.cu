@@ -14,12 +14,17 @@
 // within rounding.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
+#include <numeric>
+#include <vector>
 
 #include "b200la.h"
 #include "b200la_internal.h"
 #include "common.cuh"
+
+#include <cstring>
 
 namespace b200 {
 namespace {
@@ -160,6 +165,27 @@ __global__ void __launch_bounds__(kBlock) rotm_kernel(int n, T *x, T *y, int fla
     }
 }
 
+// Indexed writes with repeated targets in the caller's order: the entries
+// come sorted by target (a stable sort, so each target's run keeps the
+// caller's order) and one thread walks each run.  add: x_i <- ((x_i + v_1) +
+// v_2) ..., as the reference's loop adds; set: the run's last value stays.
+template <typename T>
+__global__ void __launch_bounds__(kBlock) indexed_runs_kernel(int nruns, const int *__restrict__ run_off,
+                                                              const int *__restrict__ idx, const T *__restrict__ v,
+                                                              T *x, int add_mode)
+{
+    for (int r = blockIdx.x * kBlock + threadIdx.x; r < nruns; r += gridDim.x * kBlock) {
+        const int b = run_off[r], e = run_off[r + 1], i = idx[b];
+        if (add_mode) {
+            T a = x[i];
+            for (int k = b; k < e; ++k) a = add(a, v[k]);
+            x[i] = a;
+        } else {
+            x[i] = v[e - 1];
+        }
+    }
+}
+
 template <typename T>
 void rotg_host(T *a, T *b, T *c, T *s)
 {
@@ -290,4 +316,64 @@ extern "C" int b200la_rotg(int dtype, void *a, void *b, void *c, void *s)
     if (dtype == B200LA_F64) rotg_host((double *)a, (double *)b, (double *)c, (double *)s);
     else rotg_host((float *)a, (float *)b, (float *)c, (float *)s);
     return B200LA_OK;
+}
+
+// x[indices[k]] (+)= values[k], k = 0 .. length - 1, host indices and values
+// (of the dtype), in the caller's order for repeated indices.
+static int indexed_write(b200la_ctx *ctx, int dtype, int n, void *x, int length, const int *indices,
+                         const void *values, int add_mode)
+{
+    if (!ctx || !vdt(dtype) || n < 0 || length < 0 || (length && (!x || !indices || !values)))
+        return B200LA_ERR_ARG;
+    for (int k = 0; k < length; ++k)
+        if (indices[k] < 0 || indices[k] >= n) return B200LA_ERR_ARG;
+    if (!length) return B200LA_OK;
+    const size_t es = dtype == B200LA_F64 ? 8 : 4;
+    std::vector<int> ord(length);
+    std::iota(ord.begin(), ord.end(), 0);
+    std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return indices[a] < indices[b]; });
+    std::vector<int> sidx(length), off;
+    std::vector<char> sval(es * length);
+    off.reserve(length + 1);
+    for (int k = 0; k < length; ++k) {
+        sidx[k] = indices[ord[k]];
+        std::memcpy(sval.data() + es * k, static_cast<const char *>(values) + es * ord[k], es);
+        if (k == 0 || sidx[k] != sidx[k - 1]) off.push_back(k);
+    }
+    const int nruns = (int)off.size();
+    off.push_back(length);
+    const size_t b_idx = ((size_t)4 * length + 255) & ~size_t(255), b_off = ((size_t)4 * (nruns + 1) + 255) & ~size_t(255);
+    void *work = nullptr;
+    const int rc = ctx_work(ctx, b_idx + b_off + es * length, &work);
+    if (rc) return rc;
+    int *d_idx = static_cast<int *>(work);
+    int *d_off = reinterpret_cast<int *>(static_cast<char *>(work) + b_idx);
+    void *d_val = static_cast<char *>(work) + b_idx + b_off;
+    VCK(cudaMemcpyAsync(d_idx, sidx.data(), 4 * (size_t)length, cudaMemcpyHostToDevice, ctx->stream));
+    VCK(cudaMemcpyAsync(d_off, off.data(), 4 * (size_t)(nruns + 1), cudaMemcpyHostToDevice, ctx->stream));
+    VCK(cudaMemcpyAsync(d_val, sval.data(), es * length, cudaMemcpyHostToDevice, ctx->stream));
+    const int g = std::max(1, std::min((nruns + kBlock - 1) / kBlock, ctx->num_sms * 8));
+    if (dtype == B200LA_F64)
+        indexed_runs_kernel<double><<<g, kBlock, 0, ctx->stream>>>(nruns, d_off, d_idx, (const double *)d_val,
+                                                                   (double *)x, add_mode);
+    else
+        indexed_runs_kernel<float><<<g, kBlock, 0, ctx->stream>>>(nruns, d_off, d_idx, (const float *)d_val,
+                                                                  (float *)x, add_mode);
+    VCK(cudaGetLastError());
+    // the host arrays above go out of scope: the copies from them must be done
+    VCK(cudaStreamSynchronize(ctx->stream));
+    ctx->launches += 1;
+    return B200LA_OK;
+}
+
+extern "C" int b200la_vec_add_values(b200la_ctx *ctx, int dtype, int n, void *x, int length, const int *indices,
+                                     const void *values)
+{
+    return indexed_write(ctx, dtype, n, x, length, indices, values, 1);
+}
+
+extern "C" int b200la_vec_set_values(b200la_ctx *ctx, int dtype, int n, void *x, int length, const int *indices,
+                                     const void *values)
+{
+    return indexed_write(ctx, dtype, n, x, length, indices, values, 0);
 }

@@ -218,6 +218,16 @@ int b200la_rot(b200la_ctx *ctx, int dtype, int n, void *x, void *y, double c, do
 int b200la_rotm(b200la_ctx *ctx, int dtype, int n, void *x, void *y, const double *param);
 /* lVector::Rotg (:492-535) on HOST scalars of the dtype. */
 int b200la_rotg(int dtype, void *a, void *b, void *c, void *s);
+/* lVector::add_values / add_value (src/linear_algebra/lmp/lvector_cpu.cc:114-135):
+ * x[indices[k]] += values[k]; lVector::SetValues (lvector_cpu.cc:137-150):
+ * x[indices[k]] = values[k].  HOST indices and values (of the dtype), x on the
+ * device; a repeated index is applied in the caller's order (added in turn,
+ * or the last value kept), as the reference's loops do.  An index outside
+ * [0, n) returns B200LA_ERR_ARG before anything is written. */
+int b200la_vec_add_values(b200la_ctx *ctx, int dtype, int n, void *x, int length, const int *indices,
+                          const void *values);
+int b200la_vec_set_values(b200la_ctx *ctx, int dtype, int n, void *x, int length, const int *indices,
+                          const void *values);
 /* Same, result to a DEVICE double, no synchronisation. */
 int b200la_dot_dev(b200la_ctx *ctx, int dtype, int n, const void *x, const void *y, double *result_dev);
 /* Dot product x . y written to *result_dev (a DEVICE double) without a

@@ -241,3 +241,57 @@ def test_device_rot_fp32(b200):
     a, b = pf.vector(x, b200.F32), pf.vector(y, b200.F32)
     a.Rotm(b, h)
     assert np.array_equal(b.numpy(), y * h[1] + x * h[3]) and np.array_equal(a.numpy(), y * h[2] + x * h[4])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("dt", ["F64", "F32"])
+def test_device_vector_index_and_range_access(b200, dt):
+    """SetValues / GetValues / add_values with repeated indices, block and
+    sub-vector copies, partial_add_subvector.  The expected values restate the
+    reference's loops (lvector_cpu.cc:114-200, 419-545) one entry at a time,
+    in the vector's own precision."""
+    pf = b200.Platform(0)
+    dtype = getattr(b200, dt)
+    npt = np.float64 if dt == "F64" else np.float32
+    rng = np.random.default_rng(8)
+    n = 5000
+    x0 = rng.standard_normal(n).astype(npt)
+    idx = rng.integers(0, n, 3000).astype(np.int32)
+    idx[:50] = 17                                  # one target fifty times
+    vals = rng.standard_normal(3000).astype(npt)
+    # add_values: buffer[indices[i]] += values[i], in order
+    exp = x0.copy()
+    for i, v in zip(idx, vals):
+        exp[i] = npt(exp[i] + v)
+    xv = pf.vector(x0, dtype)
+    xv.add_values(idx, vals)
+    assert np.array_equal(xv.numpy(), exp)
+    xv.add_value(3, 2.5)
+    exp[3] = npt(exp[3] + npt(2.5))
+    assert np.array_equal(xv.numpy(), exp)
+    # SetValues: buffer[index[i]] = values[i], the last write stays
+    exp2 = x0.copy()
+    for i, v in zip(idx, vals):
+        exp2[i] = v
+    xv = pf.vector(x0, dtype)
+    xv.SetValues(idx, vals)
+    assert np.array_equal(xv.numpy(), exp2)
+    assert np.array_equal(xv.GetValues(idx[::7]), exp2[idx[::7]])
+    # block and sub-vector copies
+    xv.SetBlockValues(100, 140, np.arange(40))
+    exp2[100:140] = np.arange(40)
+    assert np.array_equal(xv.GetBlockValues(90, 150), exp2[90:150])
+    sub = xv.extract_subvector(1000, 1300)
+    assert np.array_equal(sub.numpy(), exp2[1000:1300])
+    yv = pf.vector(n, dtype)
+    yv.partial_replace_subvector(10, 5, 200, sub)
+    expy = np.zeros(n, npt)
+    expy[10:210] = exp2[1005:1205]
+    assert np.array_equal(yv.numpy(), expy)
+    yv.partial_add_subvector(0, 0, 300, 0.5, sub)
+    expy[:300] += npt(0.5) * exp2[1000:1300]
+    assert np.allclose(yv.numpy(), expy, rtol=0, atol=(1e-15 if dt == "F64" else 1e-6) * 4)
+    with pytest.raises(b200.B200Error):
+        xv.add_values([n], [1.0])
+    with pytest.raises(b200.B200Error):
+        xv.GetBlockValues(10, n + 1)
