@@ -183,6 +183,30 @@ def test_serve_failures_are_per_request(b200, srv):
     assert rg["status"] == b200.SUCCESS_REL
 
 
+def test_serve_nan_request_fails_alone(b200, srv):
+    """NaN right-hand sides (an FP64 and a mixed request) inside a batch: the
+    NaN requests end with FAIL_MAXITS (FP64: at the iteration limit; mixed: no
+    outer step starts), and the other requests of the batch converge to the
+    same bits as when solved alone."""
+    reqs = _mix_requests(b200)[:6]
+    with srv.Server(budget_bytes=2e9, max_slots=32) as s:
+        alone = [s.wait(s.submit(**r)) for r in reqs]
+    bn = b200.q1_rhs(3, 2, 40)
+    bn[100] = np.nan
+    with srv.Server(budget_bytes=2e9, max_slots=32, iters_per_round=4) as s:
+        bad64 = s.submit(q1=dict(dim=2, N=40), b=bn, ctl=(30, 0.0, 1e-10, 1e6))
+        ids = [s.submit(**r) for r in reqs]
+        badmx = s.submit(q1=dict(dim=2, N=40), b=bn, precision=b200.SERVE_MIXED, max_outer=5)
+        rb64, rbmx = s.wait(bad64), s.wait(badmx)
+        mixed = [s.wait(i) for i in ids]
+    assert rb64["status"] == b200.FAIL_MAXITS and rb64["iters"] == 30
+    assert rbmx["status"] == b200.FAIL_MAXITS and rbmx["outer"] == 0
+    for a, m in zip(alone, mixed):
+        assert a["status"] in (b200.SUCCESS_ABS, b200.SUCCESS_REL)
+        assert (a["iters"], a["outer"], a["status"], a["res"]) == (m["iters"], m["outer"], m["status"], m["res"])
+        assert np.array_equal(a["x"], m["x"])
+
+
 def test_serve_long_rows_warp_per_row(b200, srv, oracle):
     # an arrow matrix: row 0 and column 0 dense, so rows are too long for the
     # sliced layout and go through the warp-per-row path

@@ -208,6 +208,40 @@ def test_stop_states(pf, b200):
     assert cg.iter() == 0
 
 
+def test_nan_rhs_runs_to_the_limit(pf, b200, oracle):
+    """A NaN in the right-hand side: every comparison of IterateControl::Check
+    (iterate_control.cc:84-110) is false, so CG and GMRES iterate to the
+    limit and report FAIL_MAXITS, as the reference and the oracle do; MPIR's
+    outer loop does not start and reports no success.  The context stays
+    usable afterwards."""
+    row, col, val = b200.q1_assemble(2, 16)
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    b = b200.q1_rhs(1, 2, 16)
+    bn = b.copy()
+    bn[37] = np.nan
+    ref = oracle.pcg(row, col, val, bn, precond=oracle.invdiag(row, col, val), ctl=control(25, 0, 1e-10, 1e6))
+    cg = b200.CG(pf)
+    cg.SetupOperator(A)
+    cg.SetupPreconditioner(b200.Preconditioner.Jacobi(pf, A))
+    cg.InitControl(25, 0.0, 1e-10, 1e6)
+    assert cg.Solve(pf.vector(bn), pf.vector(len(b))) == b200.FAIL_MAXITS == ref["status"]
+    assert cg.iter() == 25 == ref["iters"]
+    gm = b200.GMRES(pf, 10)
+    gm.SetupOperator(A)
+    gm.InitControl(40, 0.0, 1e-10, 1e6)
+    assert gm.Solve(pf.vector(bn), pf.vector(len(b))) == b200.FAIL_MAXITS
+    m = b200.MPIR(pf, max_outer=5)
+    m.SetupOperator(A)
+    m.InitControl(5, 0.0, 1e-10, 1e6)
+    m.InitInnerControl(50, 0.0, 1e-4, 1e6)
+    assert m.Solve(pf.vector(bn), pf.vector(len(b))) not in (b200.SUCCESS_ABS, b200.SUCCESS_REL)
+    # the same context then solves a clean system
+    x = pf.vector(len(b))
+    cg.InitControl(1000, 0.0, 1e-10, 1e6)
+    assert cg.Solve(pf.vector(b), x) == b200.SUCCESS_REL
+    assert np.all(np.isfinite(x.numpy()))
+
+
 def test_precond_dtype_mismatch_rejected(pf, b200):
     row, col, val = b200.q1_assemble(2, 8)
     A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
