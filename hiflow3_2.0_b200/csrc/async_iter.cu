@@ -107,6 +107,7 @@ extern "C" int b200la_async_jacobi(b200la_ctx *ctx, const b200la_csr *A, const b
                                    const void *b, void *x, const void *x_ghost, int n_inner, int n_block,
                                    double w, const b200la_control *ctl, b200la_result *res)
 {
+    NvtxScope nvtx_range("b200la_async_jacobi");
     if (!ctx || !A || !b || !x || !ctl || A->n != A->m || n_inner < 1 || n_block < 1 || !(w > 0.0) ||
         (A_offdiag && (!x_ghost || A_offdiag->n != A->n || A_offdiag->dtype != A->dtype)))
         return ctx_fail(ctx, B200LA_ERR_ARG, "async_jacobi: invalid argument", cudaSuccess);

@@ -2,9 +2,20 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <string>
 #include <vector>
+
+// An NVTX range named after a C-ABI entry point, open for the call's scope:
+// profilers group the call's kernels under it (ncu --nvtx, nsys).  Costs a
+// function-pointer check when no tool is attached.
+struct NvtxScope {
+    explicit NvtxScope(const char *name) { nvtxRangePushA(name); }
+    ~NvtxScope() { nvtxRangePop(); }
+    NvtxScope(const NvtxScope &) = delete;
+    NvtxScope &operator=(const NvtxScope &) = delete;
+};
 
 #include "common.cuh"
 #include "host_setup.h"

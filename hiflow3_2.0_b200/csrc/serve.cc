@@ -512,6 +512,7 @@ cudaError_t upload_tables(b200la_server *S, cudaStream_t st)
 
 int run_round(b200la_server *S, const std::vector<ActiveSys> &act)
 {
+    NvtxScope nvtx_range("b200la_serve_round");
     write_table(S, act);
     cudaStream_t st = S->s_comp;
     SV(upload_tables(S, st));

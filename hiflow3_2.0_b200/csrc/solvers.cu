@@ -250,12 +250,14 @@ static int cg_entry(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *
 extern "C" int b200la_cg(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P, const void *b, void *x,
                          const b200la_control *ctl, b200la_result *res)
 {
+    NvtxScope nvtx_range("b200la_cg");
     return cg_entry(ctx, A, P, b, x, ctl, res, nullptr, 0);
 }
 
 extern "C" int b200la_cg_hist(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P, const void *b,
                               void *x, const b200la_control *ctl, b200la_result *res, double *hist, int hist_len)
 {
+    NvtxScope nvtx_range("b200la_cg_hist");
     return cg_entry(ctx, A, P, b, x, ctl, res, hist, hist_len);
 }
 
@@ -265,6 +267,7 @@ extern "C" int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_
                            double *x, const b200la_control *outer, const b200la_control *inner, int max_outer,
                            b200la_result *res)
 {
+    NvtxScope nvtx_range("b200la_mpir");
     if (!ctx || !A64 || !b || !x || !outer || !inner || A64->dtype != B200LA_F64 || A64->n != A64->m ||
         max_outer < 0 || (A32in && (A32in->dtype != B200LA_F32 || A32in->n != A64->n || A32in->nnz != A64->nnz)))
         return ctx_fail(ctx, B200LA_ERR_ARG, "mpir: invalid argument", cudaSuccess);
@@ -378,6 +381,7 @@ extern "C" int b200la_mpir_gmres(b200la_ctx *ctx, const b200la_csr *A64, const b
                                  const b200la_control *outer, const b200la_control *inner, int max_outer,
                                  b200la_result *res)
 {
+    NvtxScope nvtx_range("b200la_mpir_gmres");
     if (!ctx || !A64 || !A32 || !b || !x || !outer || !inner || m < 1 || max_outer < 0 ||
         A64->dtype != B200LA_F64 || A32->dtype != B200LA_F32 || A64->n != A64->m || A32->n != A64->n ||
         (P32 && (P32->dtype != B200LA_F32 || P32->n != A64->n)))
@@ -557,6 +561,7 @@ __global__ void lincomb_kernel(int n, int k, const T *__restrict__ V, size_t ld,
 extern "C" int b200la_gmres(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P, int m, const void *b,
                             void *x, const b200la_control *ctl, b200la_result *res)
 {
+    NvtxScope nvtx_range("b200la_gmres");
     if (!ctx || !A || !b || !x || !ctl || A->n != A->m || m < 1)
         return ctx_fail(ctx, B200LA_ERR_ARG, "gmres: invalid argument", cudaSuccess);
     if (P && (P->dtype != A->dtype || P->n != A->n))
