@@ -144,6 +144,8 @@ def lib():
         "b200la_rotm": ([_P, _I, _I, _P, _P, C.POINTER(_D)], _I),
         "b200la_rotg": ([_I, _P, _P, _P, _P], _I),
         "b200la_vec_add_values": ([_P, _I, _I, _P, _I, _P, _P], _I),
+        "b200la_spmv_add_remote": ([_P, _P, _P, _P, _P, _P], _I),
+        "b200la_enable_peer_access": ([_I, _I], _I),
         "b200la_vec_set_values": ([_P, _I, _I, _P, _I, _P, _P], _I),
         "b200la_csr_diag": ([_P, _P, _I, _I, _I, _P], _I),
         "b200la_csr_extract_submatrix": ([_P, _P, _I, _I, _I, _I, C.POINTER(_P)], _I),

@@ -189,6 +189,15 @@ class LocalTransport:
         self.f.barrier.wait()
         return waits
 
+    def allgather_objects(self, obj):
+        """Every rank's obj, in rank order (pointers and events of the
+        remote-gather product)."""
+        self.f.box[("ag", self.rank)] = obj
+        self.f.barrier.wait()
+        out = [self.f.box[("ag", q)] for q in range(self.size)]
+        self.f.barrier.wait()
+        return out
+
     def allreduce_sum(self, value, device=None):
         self.f.box[("sum", self.rank)] = float(value)
         self.f.barrier.wait()
@@ -240,6 +249,10 @@ class LaCouplings:
             raise ValueError("a ghost column is owned by this rank")
         size = len(partition.offsets) - 1
         self.ghost_offsets = np.searchsorted(owners, np.arange(size + 1), side="left").astype(np.int64)
+        # where each ghost lives: its owner and its number there
+        self.ghost_owner = np.asarray(owners, np.int32)
+        self.ghost_index = (self.ghost_global - partition.offsets[owners]).astype(np.int32) if owners.size \
+            else np.zeros(0, np.int32)
         self.border_indices = None
         self.border_offsets = None
 
@@ -329,8 +342,13 @@ class CoupledVector:
 class CoupledMatrix:
     """Diagonal and off-diagonal blocks of this rank's rows on its GPU."""
 
-    def __init__(self, platform, partition, rank, transport, row, col, val, dtype=F64):
-        """row/col/val: this rank's rows (CSR) with global column numbers."""
+    def __init__(self, platform, partition, rank, transport, row, col, val, dtype=F64, remote=False):
+        """row/col/val: this rank's rows (CSR) with global column numbers.
+        remote=True: VectorMult reads the ghost values straight from the
+        owners' vectors (b200la_spmv_add_remote) instead of exchanging them;
+        the owners' memory must be addressable from this GPU (ranks of one
+        process, on one GPU or on GPUs with peer access), so the transport
+        must be a LocalTransport."""
         n_global = int(partition.offsets[-1])
         r0, r1 = partition.range(rank)
         (rd, cd, vd), (ro, co, vo), ghosts = rowblock_split(row, col, val, n_global, r0, r1)
@@ -341,15 +359,69 @@ class CoupledMatrix:
         self.offdiag = (CSR_lMatrix.from_csr(platform, ro, co, vo, n_cols=len(ghosts), dtype=dtype)
                         if len(co) else None)
         self.dtype = dtype
+        self.remote = bool(remote)
+        if self.remote:
+            if not hasattr(transport, "allgather_objects"):
+                raise NotImplementedError("remote ghost reads need the owners' memory in this process "
+                                          "(LocalTransport ranks); across processes they would need CUDA IPC")
+            import torch
+            dev = f"cuda:{platform.device}"
+            cp = self.couplings
+            self._gowner = torch.from_numpy(cp.ghost_owner.copy()).to(dev)
+            self._gindex = torch.from_numpy(cp.ghost_index.copy()).to(dev)
+            size = transport.size
+            self._reads_from = [q for q in range(size) if cp.ghost_offsets[q + 1] > cp.ghost_offsets[q]]
+            self._read_by = [q for q in range(size) if cp.border_offsets[q + 1] > cp.border_offsets[q]]
+            self._owner_tables = {}
 
     def vector(self, data_or_n=None):
         return CoupledVector(self.pf, self.couplings, self.tr,
                              self.n_local if data_or_n is None else data_or_n, self.dtype)
 
+    def _owners_table(self, ptrs):
+        """Device array of the owners' vector pointers (cached per pointer set)."""
+        t = self._owner_tables.get(ptrs)
+        if t is None:
+            import torch
+            if len(self._owner_tables) >= 64:
+                self.pf.sync()
+                self._owner_tables.clear()
+            host = torch.tensor(list(ptrs), dtype=torch.int64).pin_memory()
+            t = torch.empty(len(ptrs), dtype=torch.int64, device=f"cuda:{self.pf.device}")
+            with torch.cuda.stream(self.pf.stream()):
+                t.copy_(host, non_blocking=True)
+            self.pf.stream().synchronize()
+            self._owner_tables[ptrs] = t
+        return t
+
+    def _vector_mult_remote(self, x, y):
+        import torch
+        ls = self.pf.stream()
+        ready = torch.cuda.Event()
+        ready.record(ls)
+        peers = self.tr.allgather_objects((x.interior.t.data_ptr(), ready))
+        for q in self._reads_from:               # the owners' values are final
+            ls.wait_event(peers[q][1])
+        self.diag.VectorMult(x.interior, y.interior)
+        if self.offdiag is not None:
+            owners = self._owners_table(tuple(p for p, _ in peers))
+            self.pf.check(lib().b200la_spmv_add_remote(self.pf.h, self.offdiag.h, C.c_void_p(owners.data_ptr()),
+                                                       C.c_void_p(self._gowner.data_ptr()),
+                                                       C.c_void_p(self._gindex.data_ptr()), y.interior.ptr),
+                          "spmv_add_remote")
+        done = torch.cuda.Event()
+        done.record(ls)
+        readers = self.tr.allgather_objects(done)
+        for q in self._read_by:                  # x is not rewritten before its readers finish
+            ls.wait_event(readers[q])
+
     def VectorMult(self, x, y):
         """y = A x (coupled_matrix.cc:433-467): the ghost exchange starts, the
         diagonal block is multiplied while it runs, then the off-diagonal block
-        once the ghosts have arrived."""
+        once the ghosts have arrived.  In remote mode the off-diagonal block
+        reads the ghosts from their owners instead (no exchange)."""
+        if self.remote:
+            return self._vector_mult_remote(x, y)
         waits = x.begin_update()
         self.diag.VectorMult(x.interior, y.interior)
         x.end_update(waits)

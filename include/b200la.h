@@ -394,6 +394,22 @@ int b200la_rowblock_split(int n_rows, int n_global, const int *row, const int *c
                           int col_end, int *nnz_diag, int *nnz_offdiag, int *n_ghost, int *row_d, int *col_d,
                           double *val_d, int *row_o, int *col_o, double *val_o, int *ghost_global);
 
+/* y += A_offdiag g with every ghost value read from its owner:
+ * g[k] = owners[ghost_owner[k]][ghost_index[k]] (device arrays; owners holds
+ * device pointers of the matrix dtype, on this GPU or on peer GPUs made
+ * accessible with b200la_enable_peer_access).  Replaces the ghost exchange of
+ * CoupledVector::UpdateGhost (coupled_vector.cc:975-1128) followed by the
+ * off-diagonal product of CoupledMatrix::VectorMult (coupled_matrix.cc:433-467)
+ * when the owners' vectors are addressable: no pack, transfer or ghost
+ * buffer.  The caller orders the streams (owners' vectors final before, not
+ * rewritten until this product has finished). */
+int b200la_spmv_add_remote(b200la_ctx *ctx, const b200la_csr *A_offdiag, const void *const *owners_dev,
+                           const int *ghost_owner_dev, const int *ghost_index_dev, void *y);
+/* Let kernels running on `device` load from `peer_device`'s memory
+ * (cudaDeviceEnablePeerAccess; B200LA_ERR_DEVICE when the pair has no peer
+ * path).  Same device: nothing to do. */
+int b200la_enable_peer_access(int device, int peer_device);
+
 /* ---------------------------------------------------------------- file I/O */
 /* Host arrays.  MatrixMarket matrices: replaces CPU_CSR_lMatrix::ReadFile / WriteFile
  * (lmp/lmatrix_csr_cpu.cc:1733-1765) over CPU_COO_lMatrix::ReadFile /

@@ -121,8 +121,8 @@ def _run_ranks(world, fn):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("world", [2, 3])
-def test_coupled_cg_ranks_on_one_gpu(b200, world):
+@pytest.mark.parametrize("world,remote", [(2, False), (3, False), (2, True), (3, True)])
+def test_coupled_cg_ranks_on_one_gpu(b200, world, remote):
     import importlib
     cp = importlib.import_module("hiflow3_b200.coupled")
     row, col, val = b200.q1_assemble(2, 40, 0, np.exp(np.random.default_rng(1).standard_normal(1600)))
@@ -145,7 +145,7 @@ def test_coupled_cg_ranks_on_one_gpu(b200, world):
         pf = b200.Platform(0)
         r0, r1 = part.range(r)
         lr = row[r0:r1 + 1] - row[r0]
-        M = cp.CoupledMatrix(pf, part, r, trs[r], lr, col[row[r0]:row[r1]], val[row[r0]:row[r1]])
+        M = cp.CoupledMatrix(pf, part, r, trs[r], lr, col[row[r0]:row[r1]], val[row[r0]:row[r1]], remote=remote)
         xv = np.sin(np.arange(n) * 0.11)
         # the coupled product equals the global one on this rank's rows
         xc, yc = M.vector(xv[r0:r1]), M.vector()
@@ -167,12 +167,15 @@ def test_coupled_cg_ranks_on_one_gpu(b200, world):
 
 
 @pytest.mark.gpu
-def test_coupled_products_back_to_back_without_host_waits(b200):
+@pytest.mark.parametrize("remote", [False, True])
+def test_coupled_products_back_to_back_without_host_waits(b200, remote):
     """Twelve coupled products in a row, each feeding the next (x <- 0.1 A x
     on the platform's stream), with no host synchronisation between them: the
     stream-ordered exchange must keep every ghost update behind the pack that
     produced it and ahead of the off-diagonal product that reads it, and no
-    border may be repacked before its peers have copied it."""
+    border may be repacked before its peers have copied it.  Remote mode: the
+    off-diagonal product reads the owners' x directly, after their last write
+    and before their next."""
     import importlib
     cp = importlib.import_module("hiflow3_b200.coupled")
     row, col, val = b200.q1_assemble(2, 48, 1, None, 1e-2, (1.0, 0.5))
@@ -186,7 +189,7 @@ def test_coupled_products_back_to_back_without_host_waits(b200):
         pf = b200.Platform(0)
         r0, r1 = part.range(r)
         M = cp.CoupledMatrix(pf, part, r, trs[r], row[r0:r1 + 1] - row[r0], col[row[r0]:row[r1]],
-                             val[row[r0]:row[r1]])
+                             val[row[r0]:row[r1]], remote=remote)
         x, y = M.vector(x0[r0:r1]), M.vector()
         for _ in range(steps):
             M.VectorMult(x, y)
