@@ -34,7 +34,7 @@ import threading
 
 import numpy as np
 
-from . import CSR_lMatrix, F64, Control, Result, lib, rowblock_split
+from . import CSR_lMatrix, F64, B200Error, Control, Result, lib, rowblock_split
 
 __all__ = ["RowPartition", "LaCouplings", "DistTransport", "LocalTransport", "CoupledVector", "CoupledMatrix",
            "CoupledCG", "CoupledAsyncJacobi", "exchange", "exchange_async"]
@@ -373,6 +373,13 @@ class CoupledMatrix:
             self._reads_from = [q for q in range(size) if cp.ghost_offsets[q + 1] > cp.ghost_offsets[q]]
             self._read_by = [q for q in range(size) if cp.border_offsets[q + 1] > cp.border_offsets[q]]
             self._owner_tables = {}
+            # ranks on other GPUs of this process: their memory over NVLink
+            devices = transport.allgather_objects(platform.device)
+            for q in self._reads_from:
+                if devices[q] != platform.device:
+                    rc = lib().b200la_enable_peer_access(platform.device, devices[q])
+                    if rc:
+                        raise B200Error(rc, f"no peer access from GPU {platform.device} to GPU {devices[q]}")
 
     def vector(self, data_or_n=None):
         return CoupledVector(self.pf, self.couplings, self.tr,
