@@ -60,6 +60,7 @@ struct Req {
     std::vector<int> sell_off;        // SELL chunk offsets
     size_t bytes = 0, temp_bytes = 0; // resident / admission scratch
     double iter_bytes = 0;            // streamed by one batch iteration
+    double work = 0;                  // estimated bytes to convergence (iter_bytes x ~iterations)
     int w1 = 1, w2 = 1;               // chunk weights of the SpMV and update kernels (bytes per row)
 };
 
@@ -91,6 +92,7 @@ struct b200la_server {
     cudaStream_t s_comp = nullptr, s_copy = nullptr, s_lane[kLanes] = {};   // s_lane[0] unused (lane 0: s_comp)
     cudaEvent_t ev_a = nullptr, ev_b = nullptr, ev_fork = nullptr, ev_join[kLanes] = {};
     int lanes = 3, lane_nt[kLanes] = {};
+    bool lpt = false;                 // activate the ready system with the most estimated work first
     SysDesc *d_sys = nullptr;
     SysState *d_state = nullptr;
     unsigned *d_ticket = nullptr;
@@ -194,6 +196,8 @@ int plan_request(b200la_server *S, Req *q)
                     ((!r.row && r.q1_kcell) ? al256(8 * q1_cells(r.q1_dim, r.q1_N)) : 0);
     const double ib = stencil ? 0.0 : 4.0;   // index bytes per stored entry
     q->iter_bytes = mixed ? 4.0 * q->slen32 + ib * q->slen + 48.0 * n : (8.0 + ib) * q->slen + 96.0 * n;   // vectors: 32n (SpMV) + 64n (update)
+    // Jacobi-CG on a Q1 grid needs iterations in proportion to the nodes per line
+    q->work = q->iter_bytes * (q->r.q1_N > 0 ? (double)q->r.q1_N : std::sqrt((double)n));
     // per-row costs of the two kernels: operator + gathers and stores (k1),
     // the update's vector traffic (k2); warp-per-row CSR counts double
     const double rows = 32.0 * q->nchunks;
@@ -543,13 +547,18 @@ void round_loop(b200la_server *S)
                 wsum += (long long)sl->desc.nchunks * std::max(sl->req->w1, sl->req->w2);
             }
             while (!S->ready.empty() && (int)S->active.size() < std::min(S->max_active, kTabCap)) {
-                Slot *sl = S->ready.front();
+                auto it = S->ready.begin();
+                if (S->lpt)
+                    it = std::max_element(S->ready.begin(), S->ready.end(), [](const Slot *a, const Slot *b) {
+                        return a->req->work < b->req->work;
+                    });
+                Slot *sl = *it;
                 const bool room = S->active.empty() || wb + sl->req->iter_bytes <= S->active_cap;
                 const long long ws = (long long)sl->desc.nchunks * std::max(sl->req->w1, sl->req->w2);
                 if (!room || wsum + ws >= (1LL << 31)) break;
                 wb += sl->req->iter_bytes;
                 wsum += ws;
-                S->ready.pop_front();
+                S->ready.erase(it);
                 S->active.push_back(sl);
             }
             S->peak_active = std::max(S->peak_active, (int)S->active.size());
@@ -866,6 +875,7 @@ extern "C" int b200la_serve_start(const b200la_serve_config *cfg, b200la_server 
         ok = cudaMemPoolSetAttribute(S->pool, cudaMemPoolAttrReleaseThreshold, &keep) == cudaSuccess;
     }
     if (const char *ln = std::getenv("B200LA_SERVE_LANES")) S->lanes = std::max(1, std::min(kLanes, std::atoi(ln)));
+    if (const char *o = std::getenv("B200LA_SERVE_LPT")) S->lpt = std::atoi(o) != 0;
     ok = ok && cudaStreamCreateWithFlags(&S->s_comp, cudaStreamNonBlocking) == cudaSuccess &&
          cudaStreamCreateWithFlags(&S->s_copy, cudaStreamNonBlocking) == cudaSuccess &&
          cudaEventCreate(&S->ev_a) == cudaSuccess && cudaEventCreate(&S->ev_b) == cudaSuccess &&
