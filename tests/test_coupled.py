@@ -245,3 +245,16 @@ def test_coupled_async_jacobi_ranks_on_one_gpu(b200, world, n_global, w):
     assert len({(st, it) for _, st, it, _, _, _ in res}) == 1
     assert np.linalg.norm(b - D @ x) <= 1e-8 * res[0][4] * 1.0001
     assert np.linalg.norm(x - xe) <= 1e-4 * np.linalg.norm(xe)
+
+
+@pytest.mark.gpu
+def test_enable_peer_access_paths(b200):
+    """b200la_enable_peer_access: the same device needs nothing; a device that
+    does not exist (or has no peer path) is refused with B200LA_ERR_DEVICE,
+    and the calling thread keeps its current device."""
+    import torch
+    lib = b200.lib()
+    assert lib.b200la_enable_peer_access(0, 0) == 0
+    missing = torch.cuda.device_count() + 3
+    assert lib.b200la_enable_peer_access(0, missing) == 4
+    assert torch.cuda.current_device() == 0
