@@ -80,7 +80,10 @@ extern "C" int b200la_enable_peer_access(int device, int peer_device)
 {
     int can = 0;
     if (device == peer_device) return B200LA_OK;
-    if (cudaDeviceCanAccessPeer(&can, device, peer_device) != cudaSuccess || !can) return B200LA_ERR_DEVICE;
+    if (cudaDeviceCanAccessPeer(&can, device, peer_device) != cudaSuccess || !can) {
+        (void)cudaGetLastError();   // leave no error behind for the next launch check
+        return B200LA_ERR_DEVICE;
+    }
     int cur = 0;
     if (cudaGetDevice(&cur) != cudaSuccess) return B200LA_ERR_CUDA;
     if (cudaSetDevice(device) != cudaSuccess) return B200LA_ERR_CUDA;
