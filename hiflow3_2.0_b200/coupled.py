@@ -355,6 +355,7 @@ class CoupledMatrix:
         self.pf, self.part, self.rank, self.tr = platform, partition, rank, transport
         self.couplings = LaCouplings(partition, rank, ghosts).setup(transport)
         self.n_local = r1 - r0
+        self.diag_host = (rd, cd, vd)            # the local block, for preconditioner set-ups
         self.diag = CSR_lMatrix.from_csr(platform, rd, cd, vd, n_cols=self.n_local, dtype=dtype)
         self.offdiag = (CSR_lMatrix.from_csr(platform, ro, co, vo, n_cols=len(ghosts), dtype=dtype)
                         if len(co) else None)
@@ -451,15 +452,40 @@ def check(ctl, it, v, res0):
 
 
 class CoupledCG:
-    """CG<LAD>::Solve (src/linear_solver/cg.cc:84-248) on coupled objects, with
-    the block-Jacobi (diagonal) preconditioner of the local block or none."""
+    """CG<LAD>::Solve (src/linear_solver/cg.cc:84-248) on coupled objects.
+    Preconditioners act on the local block only (op.diagonal(), as
+    PreconditionerBlockJacobiStand and PreconditionerMultiColoring bind them,
+    preconditioner_bjacobi_standard.cc:45-156, preconditioner_mc.cc:49-273):
+    precond "jacobi" (default), "none", or "mcsgs" -- the rank's block coloured
+    and permuted, r gathered into that order, the MC-SGS sweeps, z scattered
+    back (block-Jacobi across ranks)."""
 
-    def __init__(self, A, jacobi=True):
-        self.A, self.jacobi = A, jacobi
+    def __init__(self, A, jacobi=True, precond=None):
+        self.A = A
+        self.kind = precond or ("jacobi" if jacobi else "none")
+        if self.kind not in ("jacobi", "none", "mcsgs"):
+            raise ValueError("precond: jacobi, none or mcsgs")
+        self.jacobi = self.kind == "jacobi"
         self.iter, self.res, self.res0 = 0, 0.0, 0.0
-        if jacobi:
+        if self.jacobi:
             self.invd = A.vector()
             A.pf.check(lib().b200la_csr_invdiag(A.pf.h, A.diag.h, self.invd.interior.ptr), "invdiag")
+        if self.kind == "mcsgs":
+            import torch
+            from . import Preconditioner
+            rd, cd, vd = A.diag_host
+            self.P = Preconditioner.MultiColoringSGS(A.pf, rd, cd, vd, dtype=A.dtype)
+            self._perm = torch.from_numpy(np.asarray(self.P.perm, np.int32).copy()).to(f"cuda:{A.pf.device}")
+            self._rp, self._zp = A.pf.vector(A.n_local, A.dtype), A.pf.vector(A.n_local, A.dtype)
+
+    def _apply_mcsgs(self, src, dst):
+        pf, n = self.A.pf, self.A.n_local
+        if n == 0:
+            return
+        perm = C.c_void_p(self._perm.data_ptr())
+        pf.check(lib().b200la_gather(pf.h, self.A.dtype, n, perm, src.interior.ptr, self._rp.ptr), "gather")
+        self.P.ApplyPreconditioner(self._rp, self._zp)
+        pf.check(lib().b200la_scatter(pf.h, self.A.dtype, n, perm, self._zp.ptr, dst.interior.ptr), "scatter")
 
     def Solve(self, b, x, maxits=10000, abstol=0.0, reltol=1e-10, divtol=1e6):
         A = self.A
@@ -471,6 +497,9 @@ class CoupledCG:
         ctl = Control(maxits, abstol, reltol, divtol)
 
         def precond(src, dst):
+            if self.kind == "mcsgs":
+                self._apply_mcsgs(src, dst)
+                return
             dst.CopyFrom(src)
             if self.jacobi:
                 dst.interior.ElementWiseMult(self.invd.interior)

@@ -258,3 +258,56 @@ def test_enable_peer_access_paths(b200):
     missing = torch.cuda.device_count() + 3
     assert lib.b200la_enable_peer_access(0, missing) == 4
     assert torch.cuda.current_device() == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("world", [1, 2, 3])
+def test_coupled_cg_mcsgs_block_jacobi(b200, world):
+    """Coupled CG with the multicoloured SGS of each rank's block (block-Jacobi
+    across ranks, as PreconditionerMultiColoring on op.diagonal()).  One rank:
+    the same iterations (within 5%) as the single-system MC-SGS PCG on the
+    permuted operator.  Every world size: the global solution within 1e-8, and
+    fewer iterations than the coupled Jacobi-PCG."""
+    import importlib
+    cp = importlib.import_module("hiflow3_b200.coupled")
+    N = 12
+    row, col, val = b200.q1_assemble(3, N, 0, np.exp(np.random.default_rng(2).standard_normal(N ** 3)))
+    n = len(row) - 1
+    b = b200.q1_rhs(6, 3, N)
+    D = np.zeros((n, n))
+    for i in range(n):
+        D[i, col[row[i]:row[i + 1]]] += val[row[i]:row[i + 1]]
+    xe = np.linalg.solve(D, b)
+    pf0 = b200.Platform(0)
+    P0 = b200.Preconditioner.MultiColoringSGS(pf0, row, col, val)
+    cg = b200.CG(pf0)
+    cg.SetupOperator(P0.A_perm)
+    cg.SetupPreconditioner(P0)
+    cg.InitControl(5000, 0.0, 1e-10, 1e6)
+    assert cg.Solve(pf0.vector(b[P0.perm]), pf0.vector(n)) == b200.SUCCESS_REL
+    it_single = cg.iter()
+    part = cp.RowPartition.even(n, world)
+    trs = cp.LocalTransport.group(world)
+
+    def rank_fn(r):
+        pf = b200.Platform(0)
+        r0, r1 = part.range(r)
+        M = cp.CoupledMatrix(pf, part, r, trs[r], row[r0:r1 + 1] - row[r0], col[row[r0]:row[r1]],
+                             val[row[r0]:row[r1]])
+        out = []
+        for kind in ("mcsgs", "jacobi"):
+            s = cp.CoupledCG(M, precond=kind)
+            x = M.vector()
+            st = s.Solve(M.vector(b[r0:r1]), x, maxits=5000, reltol=1e-10)
+            out.append((st, s.iter, x.numpy()))
+        return r0, out
+
+    res = _run_ranks(world, rank_fn)
+    x = np.zeros(n)
+    for r0, ((st, it, xr), (stj, itj, _)) in res:
+        assert st == b200.SUCCESS_REL and stj == b200.SUCCESS_REL
+        assert it < itj, (it, itj)
+        if world == 1:
+            assert abs(it - it_single) <= max(1, 0.05 * it_single), (it, it_single)
+        x[r0:r0 + len(xr)] = xr
+    assert np.linalg.norm(x - xe) <= 1e-8 * np.linalg.norm(xe)
