@@ -37,7 +37,7 @@ import numpy as np
 from . import CSR_lMatrix, F64, B200Error, Control, Result, lib, rowblock_split
 
 __all__ = ["RowPartition", "LaCouplings", "DistTransport", "LocalTransport", "CoupledVector", "CoupledMatrix",
-           "CoupledCG", "CoupledAsyncJacobi", "exchange", "exchange_async"]
+           "BlockPrecond", "CoupledCG", "CoupledGMRES", "CoupledAsyncJacobi", "exchange", "exchange_async"]
 
 
 class RowPartition:
@@ -451,26 +451,22 @@ def check(ctl, it, v, res0):
     return 0
 
 
-class CoupledCG:
-    """CG<LAD>::Solve (src/linear_solver/cg.cc:84-248) on coupled objects.
-    Preconditioners act on the local block only (op.diagonal(), as
-    PreconditionerBlockJacobiStand and PreconditionerMultiColoring bind them,
-    preconditioner_bjacobi_standard.cc:45-156, preconditioner_mc.cc:49-273):
-    precond "jacobi" (default), "none", or "mcsgs" -- the rank's block coloured
-    and permuted, r gathered into that order, the MC-SGS sweeps, z scattered
-    back (block-Jacobi across ranks)."""
+class BlockPrecond:
+    """A preconditioner of the local block only (op.diagonal(), as
+    PreconditionerBlockJacobiStand and PreconditionerMultiColoring bind the lmp
+    preconditioners, preconditioner_bjacobi_standard.cc:45-156,
+    preconditioner_mc.cc:49-273): "none", "jacobi", or "mcsgs" -- the rank's
+    block coloured and permuted, r gathered into that order, the MC-SGS
+    sweeps, z scattered back.  Across ranks this is block-Jacobi."""
 
-    def __init__(self, A, jacobi=True, precond=None):
-        self.A = A
-        self.kind = precond or ("jacobi" if jacobi else "none")
-        if self.kind not in ("jacobi", "none", "mcsgs"):
+    def __init__(self, A, kind="jacobi"):
+        if kind not in ("jacobi", "none", "mcsgs"):
             raise ValueError("precond: jacobi, none or mcsgs")
-        self.jacobi = self.kind == "jacobi"
-        self.iter, self.res, self.res0 = 0, 0.0, 0.0
-        if self.jacobi:
+        self.A, self.kind = A, kind
+        if kind == "jacobi":
             self.invd = A.vector()
             A.pf.check(lib().b200la_csr_invdiag(A.pf.h, A.diag.h, self.invd.interior.ptr), "invdiag")
-        if self.kind == "mcsgs":
+        if kind == "mcsgs":
             import torch
             from . import Preconditioner
             rd, cd, vd = A.diag_host
@@ -478,14 +474,33 @@ class CoupledCG:
             self._perm = torch.from_numpy(np.asarray(self.P.perm, np.int32).copy()).to(f"cuda:{A.pf.device}")
             self._rp, self._zp = A.pf.vector(A.n_local, A.dtype), A.pf.vector(A.n_local, A.dtype)
 
-    def _apply_mcsgs(self, src, dst):
-        pf, n = self.A.pf, self.A.n_local
-        if n == 0:
+    def apply(self, src, dst):
+        """dst = M^-1 src (local block; no communication)."""
+        A = self.A
+        if self.kind == "mcsgs":
+            pf, n = A.pf, A.n_local
+            if n == 0:
+                return
+            perm = C.c_void_p(self._perm.data_ptr())
+            pf.check(lib().b200la_gather(pf.h, A.dtype, n, perm, src.interior.ptr, self._rp.ptr), "gather")
+            self.P.ApplyPreconditioner(self._rp, self._zp)
+            pf.check(lib().b200la_scatter(pf.h, A.dtype, n, perm, self._zp.ptr, dst.interior.ptr), "scatter")
             return
-        perm = C.c_void_p(self._perm.data_ptr())
-        pf.check(lib().b200la_gather(pf.h, self.A.dtype, n, perm, src.interior.ptr, self._rp.ptr), "gather")
-        self.P.ApplyPreconditioner(self._rp, self._zp)
-        pf.check(lib().b200la_scatter(pf.h, self.A.dtype, n, perm, self._zp.ptr, dst.interior.ptr), "scatter")
+        dst.CopyFrom(src)
+        if self.kind == "jacobi":
+            dst.interior.ElementWiseMult(self.invd.interior)
+
+
+class CoupledCG:
+    """CG<LAD>::Solve (src/linear_solver/cg.cc:84-248) on coupled objects, with
+    a BlockPrecond of the local block: precond "jacobi" (default), "none" or
+    "mcsgs"."""
+
+    def __init__(self, A, jacobi=True, precond=None):
+        self.A = A
+        self.kind = precond or ("jacobi" if jacobi else "none")
+        self.M = BlockPrecond(A, self.kind)
+        self.iter, self.res, self.res0 = 0, 0.0, 0.0
 
     def Solve(self, b, x, maxits=10000, abstol=0.0, reltol=1e-10, divtol=1e6):
         A = self.A
@@ -496,13 +511,7 @@ class CoupledCG:
         self.res0 = res
         ctl = Control(maxits, abstol, reltol, divtol)
 
-        def precond(src, dst):
-            if self.kind == "mcsgs":
-                self._apply_mcsgs(src, dst)
-                return
-            dst.CopyFrom(src)
-            if self.jacobi:
-                dst.interior.ElementWiseMult(self.invd.interior)
+        precond = self.M.apply
 
         status, it = check(ctl, 0, res, self.res0), 0
         precond(r, z)
@@ -524,6 +533,89 @@ class CoupledCG:
             rho = rho_new
         self.iter, self.res = it, res
         return status
+
+
+class CoupledGMRES:
+    """GMRES<LAD>::SolveRight (src/linear_solver/gmres.cc:285-510) on coupled
+    objects: restarted GMRES(m), modified Gram-Schmidt with global dots, Givens
+    rotations on the host (gmres.h:77-97), right preconditioning with a
+    BlockPrecond of the local block.  As in the reference, a restart
+    normalises the new residual by the last Givens estimate |g[j+1]|, not by
+    its recomputed norm."""
+
+    def __init__(self, A, m=30, precond="none"):
+        if m < 1:
+            raise ValueError("m >= 1 required")
+        self.A, self.m = A, int(m)
+        self.M = BlockPrecond(A, precond) if precond != "none" else None
+        self.iter, self.res, self.res0 = 0, 0.0, 0.0
+
+    def _prec(self, src, dst):
+        if self.M is None:
+            dst.CopyFrom(src)
+        else:
+            self.M.apply(src, dst)
+
+    def Solve(self, b, x, maxits=10000, abstol=0.0, reltol=1e-9, divtol=1e6):
+        A = self.A
+        ctl = Control(maxits, abstol, reltol, divtol)
+        mb = min(self.m, maxits)                                    # gmres.cc:301
+        V = [A.vector() for _ in range(mb + 1)]
+        w, z = A.vector(), A.vector()
+        A.VectorMult(x, V[0])                                       # V0 = b - A x
+        V[0].ScaleAdd(-1.0, b)
+        res = V[0].Norm2()
+        self.res0, it = res, 0
+        conv = check(ctl, it, res, self.res0)
+        while conv == 0:
+            H = np.zeros((mb, mb + 1))                              # H[j, i]: column j
+            g, cs, sn = np.zeros(mb + 1), np.zeros(mb + 1), np.zeros(mb + 1)
+            V[0].Scale(1.0 / res)
+            g[0] = res
+            j_end = mb - 1
+            for j in range(mb):
+                it += 1
+                self._prec(V[j], z)
+                A.VectorMult(z, w)
+                for i in range(j + 1):                              # modified Gram-Schmidt
+                    H[j, i] = w.Dot(V[i])
+                    w.Axpy(V[i], -1.0 * H[j, i])
+                H[j, j + 1] = w.Norm2()
+                w.Scale(1.0 / H[j, j + 1])
+                V[j + 1].CopyFrom(w)
+                for k in range(j):                                  # earlier rotations
+                    t = cs[k] * H[j, k] + sn[k] * H[j, k + 1]
+                    H[j, k + 1] = -sn[k] * H[j, k] + cs[k] * H[j, k + 1]
+                    H[j, k] = t
+                beta = np.sqrt(H[j, j] * H[j, j] + H[j, j + 1] * H[j, j + 1])
+                cs[j], sn[j] = H[j, j] / beta, H[j, j + 1] / beta
+                t = cs[j] * H[j, j] + sn[j] * H[j, j + 1]
+                H[j, j + 1] = -sn[j] * H[j, j] + cs[j] * H[j, j + 1]
+                H[j, j] = t
+                t = cs[j] * g[j] + sn[j] * g[j + 1]
+                g[j + 1] = -sn[j] * g[j] + cs[j] * g[j + 1]
+                g[j] = t
+                res = abs(g[j + 1])
+                conv = check(ctl, it, res, self.res0)
+                if conv:
+                    j_end = j
+                    break
+            # UpdateSolution (gmres.cc:487-510): back substitution, x += M^-1 (V y)
+            y = g.copy()
+            for i in range(j_end, -1, -1):
+                y[i] /= H[i, i]
+                for k in range(i):
+                    y[k] -= H[i, k] * y[i]
+            z.Zeros()
+            for k in range(j_end + 1):
+                z.Axpy(V[k], y[k])
+            self._prec(z, w)
+            x.Axpy(w, 1.0)
+            if conv == 0:
+                A.VectorMult(x, V[0])
+                V[0].ScaleAdd(-1.0, b)
+        self.iter, self.res = it, res
+        return conv
 
 
 class CoupledAsyncJacobi:
