@@ -37,7 +37,8 @@ import numpy as np
 from . import CSR_lMatrix, F64, B200Error, Control, Result, lib, rowblock_split
 
 __all__ = ["RowPartition", "LaCouplings", "DistTransport", "LocalTransport", "CoupledVector", "CoupledMatrix",
-           "BlockPrecond", "CoupledCG", "CoupledGMRES", "CoupledAsyncJacobi", "exchange", "exchange_async"]
+           "BlockPrecond", "CoupledCG", "CoupledGMRES", "CoupledMPIR", "CoupledAsyncJacobi", "exchange",
+           "exchange_async"]
 
 
 class RowPartition:
@@ -312,6 +313,11 @@ class CoupledVector:
         the platform's next kernel (CoupledVector::UpdateGhost)."""
         self.end_update(self.begin_update())
 
+    def CastInteriorFrom(self, other):
+        """The owned values of other in this vector's precision
+        (CoupledVector::CastInteriorFrom, coupled_vector.cc:755-806)."""
+        self.interior.CastFrom(other.interior)
+
     # global reductions (local kernel, then the sum across ranks)
     def Dot(self, other):
         return self.tr.allreduce_sum(self.interior.Dot(other.interior), f"cuda:{self.pf.device}")
@@ -385,6 +391,18 @@ class CoupledMatrix:
     def vector(self, data_or_n=None):
         return CoupledVector(self.pf, self.couplings, self.tr,
                              self.n_local if data_or_n is None else data_or_n, self.dtype)
+
+    def cast(self, dtype):
+        """A copy of this matrix in another precision on the same couplings
+        (CoupledMatrix::CastFrom over lMatrix::CastFrom of both blocks)."""
+        M = object.__new__(CoupledMatrix)
+        M.__dict__.update(self.__dict__)
+        M.dtype = dtype
+        M.diag = self.diag.CastFrom(dtype)
+        M.offdiag = self.offdiag.CastFrom(dtype) if self.offdiag is not None else None
+        if self.remote:
+            M._owner_tables = {}
+        return M
 
     def _owners_table(self, ptrs):
         """Device array of the owners' vector pointers (cached per pointer set)."""
@@ -616,6 +634,46 @@ class CoupledGMRES:
                 V[0].ScaleAdd(-1.0, b)
         self.iter, self.res = it, res
         return conv
+
+
+class CoupledMPIR:
+    """MPIR<LAD_high, LAD_low>::Solve (src/linear_solver/mpir.cc:69-326) on
+    coupled objects: the FP64 residual r = b - A x across ranks, its FP32 copy
+    (CastInteriorFrom), an FP32 coupled Jacobi-CG correction A32 c = r32 to the
+    inner tolerance, x += (double) c; stop on the outer residual relative to
+    the first one (the benchmark's criterion, as b200la_mpir)."""
+
+    def __init__(self, A, A32=None, inner_precond="jacobi", max_outer=50):
+        from . import F32
+        self.A = A
+        self.A32 = A32 if A32 is not None else A.cast(F32)
+        self.inner_precond, self.max_outer = inner_precond, int(max_outer)
+        self.outer, self.inner_iters, self.res, self.res0 = 0, 0, 0.0, 0.0
+
+    def Solve(self, b, x, maxits=50, abstol=0.0, reltol=1e-10, divtol=1e6, inner=(10000, 0.0, 1e-4, 1e6)):
+        A, A32 = self.A, self.A32
+        r = A.vector()
+        A.VectorMult(x, r)                                  # mpir.cc:125-128
+        r.ScaleAdd(-1.0, b)
+        res = r.Norm2()
+        self.res0 = res
+        r32, c32, c64 = A32.vector(), A32.vector(), A.vector()
+        solver = CoupledCG(A32, precond=self.inner_precond)
+        outer = total = 0
+        limit = min(self.max_outer, maxits)
+        while res > abstol and res > reltol * self.res0 and res < divtol and outer < limit:
+            outer += 1
+            r32.CastInteriorFrom(r)                         # mpir.cc:169-170
+            c32.Zeros()
+            solver.Solve(r32, c32, *inner)                  # mpir.cc:193
+            total += solver.iter
+            c64.CastInteriorFrom(c32)                       # mpir.cc:223, 253
+            x.Axpy(c64, 1.0)
+            A.VectorMult(x, r)                              # mpir.cc:271-273
+            r.ScaleAdd(-1.0, b)
+            res = r.Norm2()
+        self.outer, self.inner_iters, self.res = outer, total, res
+        return 1 if res < abstol else 2 if res < reltol * self.res0 else 3 if res >= divtol else 4
 
 
 class CoupledAsyncJacobi:
