@@ -404,3 +404,23 @@ def test_coupled_mpir_ranks_on_one_gpu(b200, oracle, world):
         assert abs(outer - ref["outer"]) <= 1, (outer, ref["outer"])
         x[r0:r0 + len(xr)] = xr
     assert np.linalg.norm(x - xe) <= 1e-8 * np.linalg.norm(xe)
+
+
+def test_couplings_ghost_owner_and_index():
+    """Where every ghost lives (the remote-read tables): its owner from the
+    partition, and its number there (global minus the owner's first row); no
+    transport is needed for these."""
+    import importlib
+    from conftest import load_platform
+    load_platform()
+    cp = importlib.import_module("hiflow3_b200.coupled")
+    part = cp.RowPartition([0, 10, 25, 25, 40])          # rank 2 owns nothing
+    ghosts = np.array([3, 9, 30, 39], np.int64)         # rank 1's ghosts
+    c = cp.LaCouplings(part, 1, ghosts)
+    assert c.ghost_owner.tolist() == [0, 0, 3, 3]
+    assert c.ghost_index.tolist() == [3, 9, 5, 14]
+    assert c.ghost_offsets.tolist() == [0, 2, 2, 2, 4]
+    with pytest.raises(ValueError):
+        cp.LaCouplings(part, 1, np.array([12], np.int64))   # a ghost this rank owns
+    empty = cp.LaCouplings(part, 0, np.zeros(0, np.int64))
+    assert empty.ghost_owner.size == 0 and empty.ghost_index.size == 0
