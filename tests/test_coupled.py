@@ -316,16 +316,22 @@ def test_coupled_cg_mcsgs_block_jacobi(b200, world):
 @pytest.mark.gpu
 @pytest.mark.parametrize("world", [1, 2, 3])
 def test_coupled_gmres_ranks_on_one_gpu(b200, world):
-    """Coupled GMRES(30) on a nonsymmetric 2-D convection-diffusion system.
-    Unpreconditioned it is the global method: the iterations of the
-    single-system GMRES within 5%.  With the local blocks' Jacobi or MC-SGS
-    (block-Jacobi across ranks) it reaches the global solution."""
+    """Coupled GMRES(30) on the reference's GMRES case (2-D 32^2 convection-
+    diffusion, nu = 1e-3, its right-hand side from the golden fixtures).
+    Unpreconditioned it is the global method: the reference's iteration count
+    and the single-system GMRES's, within 5%.  With the local blocks' Jacobi
+    (block-Jacobi across ranks) it reaches the global solution; with the
+    blocks' MC-SGS it does so on a milder case (24^2, nu = 1e-2), since on
+    this strongly convective one SGS blocks make a poor right preconditioner
+    (GMRES(30) stalls)."""
     import importlib
     cp = importlib.import_module("hiflow3_b200.coupled")
-    N = 24
-    row, col, val = b200.q1_assemble(2, N, 1, None, 1e-2, (1.0, 0.5))
+    golden = np.load(os.path.join(ROOT, "tests", "golden", "lmp_golden.npz"))
+    N = 32
+    row, col, val = b200.q1_assemble(2, N, 1, None, 1e-3, (1.0, 0.5))
     n = len(row) - 1
-    b = b200.q1_rhs(8, 2, N)
+    b = golden["gmres2d32_b"]
+    it_ref = int(golden["gmres2d32_none_iters"][0])
     D = np.zeros((n, n))
     for i in range(n):
         D[i, col[row[i]:row[i + 1]]] += val[row[i]:row[i + 1]]
@@ -345,23 +351,47 @@ def test_coupled_gmres_ranks_on_one_gpu(b200, world):
         M = cp.CoupledMatrix(pf, part, r, trs[r], row[r0:r1 + 1] - row[r0], col[row[r0]:row[r1]],
                              val[row[r0]:row[r1]])
         out = []
-        for kind in ("none", "jacobi", "mcsgs"):
+        for kind in ("none", "jacobi"):
             s = cp.CoupledGMRES(M, 30, precond=kind)
             x = M.vector()
             st = s.Solve(M.vector(b[r0:r1]), x, maxits=3000, reltol=1e-9)
             out.append((kind, st, s.iter, x.numpy()))
-        return r0, out
+        # the milder case with MC-SGS blocks
+        r0m, r1m = part_m.range(r)
+        Mm = cp.CoupledMatrix(pf, part_m, r, trs_m[r], row_m[r0m:r1m + 1] - row_m[r0m], col_m[row_m[r0m]:row_m[r1m]],
+                              val_m[row_m[r0m]:row_m[r1m]])
+        s = cp.CoupledGMRES(Mm, 30, precond="mcsgs")
+        xm = Mm.vector()
+        stm = s.Solve(Mm.vector(b_m[r0m:r1m]), xm, maxits=3000, reltol=1e-9)
+        return r0, out, (r0m, stm, xm.numpy())
 
+    row_m, col_m, val_m = b200.q1_assemble(2, 24, 1, None, 1e-2, (1.0, 0.5))
+    n_m = len(row_m) - 1
+    b_m = b200.q1_rhs(8, 2, 24)
+    part_m = cp.RowPartition.even(n_m, world)
+    trs_m = cp.LocalTransport.group(world)
     res = _run_ranks(world, rank_fn)
-    for kind_i, kind in enumerate(("none", "jacobi", "mcsgs")):
+    Dm = np.zeros((n_m, n_m))
+    for i in range(n_m):
+        Dm[i, col_m[row_m[i]:row_m[i + 1]]] += val_m[row_m[i]:row_m[i + 1]]
+    xm = np.zeros(n_m)
+    for _, _, (r0m, stm, xr) in res:
+        assert stm == b200.SUCCESS_REL
+        xm[r0m:r0m + len(xr)] = xr
+    assert np.linalg.norm(b_m - Dm @ xm) <= 2e-9 * np.linalg.norm(b_m)
+    res = [(r0, out) for r0, out, _ in res]
+    for kind_i, kind in enumerate(("none", "jacobi")):
         x = np.zeros(n)
         for r0, out in res:
             k, st, it, xr = out[kind_i]
             assert st == b200.SUCCESS_REL, (kind, st)
             if kind == "none":
                 assert abs(it - it_single) <= max(1, 0.05 * it_single), (it, it_single)
+                assert abs(it - it_ref) <= max(1, 0.05 * it_ref), (it, it_ref)
             x[r0:r0 + len(xr)] = xr
-        assert np.linalg.norm(x - xe) <= 1e-6 * np.linalg.norm(xe), kind
+        # the stop test is on the Givens estimate; the true residual agrees closely
+        assert np.linalg.norm(b - D @ x) <= 2e-9 * np.linalg.norm(b), kind
+        assert np.linalg.norm(x - xe) <= 1e-4 * np.linalg.norm(xe), kind
 
 
 @pytest.mark.gpu
