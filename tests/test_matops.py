@@ -295,3 +295,19 @@ def test_device_vector_index_and_range_access(b200, dt):
         xv.add_values([n], [1.0])
     with pytest.raises(b200.B200Error):
         xv.GetBlockValues(10, n + 1)
+
+
+def test_rotg_host_abi_matches_reference(b200, gold):
+    """b200la_rotg runs on the host: the library's own entry point (no GPU)
+    against the reference's Rotg outputs, bit for bit, in FP64; FP32 against
+    the same formulas evaluated in float."""
+    import ctypes as C
+    lib = b200.lib()
+    for (a, b), ref in zip(gold["rotg_in"], gold["rotg_out"]):
+        v = [C.c_double(a), C.c_double(b), C.c_double(), C.c_double()]
+        assert lib.b200la_rotg(b200.F64, *[C.cast(C.byref(q), C.c_void_p) for q in v]) == 0
+        assert bits(np.array([q.value for q in v])).tolist() == bits(ref).tolist()
+    f = [C.c_float(3.0), C.c_float(4.0), C.c_float(), C.c_float()]
+    assert lib.b200la_rotg(b200.F32, *[C.cast(C.byref(q), C.c_void_p) for q in f]) == 0
+    assert [q.value for q in f] == [5.0, np.float32(1) / np.float32(0.6), np.float32(0.6), np.float32(0.8)]
+    assert lib.b200la_rotg(7, None, None, None, None) == 1
