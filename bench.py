@@ -168,80 +168,141 @@ def shard(items, rank, world):
 
 # --------------------------------------------------------------- CPU baseline
 
-def cpu_counts(N):
-    p = os.path.join(ROOT, "tests", "golden", "c3_counts.json" if N == 128 else f"c3_counts_{N}.json")
-    if os.path.exists(p):
-        with open(p) as f:
-            return json.load(f)
-    return None
+def load_workloads_file():
+    """workloads.py loaded by path: numpy only, so the reference arm loads no
+    library of this platform."""
+    name = "b200_workloads_file"
+    if name in sys.modules:
+        return sys.modules[name]
+    spec = importlib.util.spec_from_file_location(name, os.path.join(ROOT, "hiflow3_2.0_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
 
 
-def cpu_estimate(ref, pyoracle, row, col, val, b, threads, outer, inner_total, fp64_iters, s1=4, s2=16):
-    """The reference's MPIR timed with `threads` OpenMP threads on its first
-    correction cut at s1 and s2 inner iterations, fitted linearly and scaled to
-    the full solve's counts; its FP64 Jacobi-CG per iteration likewise."""
-    a = pyoracle.ref_mpir(ref, row, col, val, b, threads, sample_inner=s1)
-    c = pyoracle.ref_mpir(ref, row, col, val, b, threads, sample_inner=s2)
-    per_inner = max((c["seconds"] - a["seconds"]) / (s2 - s1), 1e-9)
-    per_outer = max(a["seconds"] - s1 * per_inner, 0.0)   # residuals, casts, update of one correction
-    p = pyoracle.ref_pcg_timed(ref, row, col, val, b, threads, maxits=s2)
-    return dict(per_inner=per_inner, per_outer=per_outer, est=outer * per_outer + inner_total * per_inner,
-                fp64_est=p["seconds"] / max(p["iters"], 1) * fp64_iters, fp64_iters=p["iters"])
+def host_cpu():
+    """The host's CPU model, physical cores (distinct physical id / core id
+    pairs of /proc/cpuinfo), the logical CPUs this process may run on, and
+    OMP_NUM_THREADS."""
+    model, cores = None, set()
+    try:
+        phys = None
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                k, _, v = line.partition(":")
+                k, v = k.strip(), v.strip()
+                if k == "model name" and model is None:
+                    model = v
+                elif k == "physical id":
+                    phys = v
+                elif k == "core id":
+                    cores.add((phys, v))
+    except OSError:
+        pass
+    return {"model": model, "physical_cores": len(cores) or None,
+            "logical_cpus_available": len(os.sched_getaffinity(0)),
+            "omp_num_threads": os.environ.get("OMP_NUM_THREADS")}
 
 
-def cpu_baseline(row, col, val, b, outer, inner_total, fp64_iters, single_thread=False):
-    """The reference's own CPU code (oracle/_ref: HiFlow3's CPUopenmp lmp
-    objects driving the restated MPIR and CG loops), timed on a bounded sample
-    and scaled to the full solve's iteration counts, with every host thread
-    (and, with single_thread, also with one)."""
+def repo_libraries():
+    """Shared libraries of this repository mapped into this process."""
+    libs = set()
+    try:
+        with open("/proc/self/maps") as f:
+            for line in f:
+                path = line.split()[-1]
+                if path.endswith(".so") and os.path.realpath(path).startswith(os.path.realpath(ROOT)):
+                    libs.add(os.path.relpath(os.path.realpath(path), os.path.realpath(ROOT)))
+    except OSError:
+        pass
+    return sorted(libs)
+
+
+def pyoracle_module():
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle
-    threads = len(os.sched_getaffinity(0))
+    return pyoracle
+
+
+def reference_system(N):
+    """The 3-D Q1 N^3 GRF system assembled by the reference's own code
+    (oracle/_ref: CPU_CSR_lMatrix init_structure + add_values + ZeroRows),
+    bit-identical to the platform's assembler."""
+    pyoracle = pyoracle_module()
+    ref = pyoracle.Ref()
+    wl = load_workloads_file()
+    kc = np.exp(wl.grf_cells(N, 3))
+    row, col, val = ref.q1_assemble(3, N, 0, kc)
+    b = ref.q1_rhs(42, 3, N)
+    return ref, row, col, val, b
+
+
+def cpu_baseline(row, col, val, b, single_thread=False, ref=None):
+    """The reference's own CPU code (oracle/_ref: HiFlow3's CPUopenmp lmp
+    objects driving the restated MPIR loop of mpir.cc:69-326), one full
+    mixed-precision solve to 1e-10 timed with every host thread, and (with
+    single_thread) one more with one thread."""
+    pyoracle = pyoracle_module()
     if not os.path.exists(pyoracle.REF_SO):
         return None
-    ref = pyoracle.Ref()
-    s1, s2 = 4, 16
-    e = cpu_estimate(ref, pyoracle, row, col, val, b, threads, outer, inner_total, fp64_iters, s1, s2)
-    est = e["est"]
-    out = dict(value=1.0 / est, unit=UNIT, cores=threads, kind="reference",
-               sample=(f"reference CPUopenmp lmp MPIR: first correction cut at {s1} and {s2} FP32 inner "
-                       f"iterations (linear fit: {e['per_inner'] * 1e3:.1f} ms/inner iteration, "
-                       f"{e['per_outer'] * 1e3:.1f} ms/correction overhead) scaled to {outer} corrections and "
-                       f"{inner_total} inner iterations"),
-               est_solve_s=est, fp64_cg_est_s=e["fp64_est"], fp64_cg_sample_iters=e["fp64_iters"])
+    ref = ref or pyoracle.Ref()
+    threads = len(os.sched_getaffinity(0))
+    sess = pyoracle.RefMpirSession(ref, row, col, val, threads)
+    sess.run(b, sample_inner=16)                      # warm-up: threads started, pages touched
+    m = sess.run(b)
+    out = dict(value=1.0 / m["seconds"], unit=UNIT, cores=threads, kind="reference",
+               sample=(f"one full solve to 1e-10 of the same system by the reference's CPUopenmp lmp objects "
+                       f"(MPIR: {m['outer']} corrections, {m['inner_total']} FP32 inner iterations), "
+                       f"{threads} OpenMP threads"),
+               solve_s=m["seconds"], outer=m["outer"], inner_total=m["inner_total"], cpu=host_cpu())
     if single_thread:
-        e1 = cpu_estimate(ref, pyoracle, row, col, val, b, 1, outer, inner_total, fp64_iters, s1, s2)
-        out["one_thread"] = dict(value=1.0 / e1["est"], unit=UNIT, cores=1, est_solve_s=e1["est"],
-                                 ms_per_inner_iteration=e1["per_inner"] * 1e3, fp64_cg_est_s=e1["fp64_est"])
+        sess.threads(1)
+        sess.run(b, sample_inner=4)
+        m1 = sess.run(b)
+        out["one_thread"] = dict(value=1.0 / m1["seconds"], unit=UNIT, cores=1, solve_s=m1["seconds"],
+                                 outer=m1["outer"], inner_total=m1["inner_total"])
+    sess.close()
     return out
 
 
 def run_reference(args):
-    wl = load_workloads()
-    b200 = load_platform()
-    row, col, val, b, _ = wl.system(b200, "c3", N=args.N)
-    counts = cpu_counts(args.N)
-    if counts is None:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        import pyoracle
-        ref = pyoracle.Ref()
-        m = pyoracle.ref_mpir(ref, row, col, val, b, len(os.sched_getaffinity(0)))
-        counts = dict(mpir_outer=m["outer"], mpir_inner_total=m["inner_total"], fp64_cg_iters=0)
-    ests = []
-    for k in range(args.warmup + args.steps):
-        cb = cpu_baseline(row, col, val, b, counts["mpir_outer"], counts["mpir_inner_total"],
-                          counts["fp64_cg_iters"])
-        if cb is None:
-            return {"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU lmp build) is missing"}
-        if k >= args.warmup:
-            ests.append(cb["est_solve_s"])
-    est = statistics.median(ests)
-    v = 1.0 / est
-    cb["value"] = v
+    """The reference's own CPU implementation of the path (oracle/_ref, built
+    from the reference's lmp sources), on the same system, timed per step as
+    one full solve to 1e-10; warm-up steps are untimed solves cut after 16
+    inner iterations.  Nothing of this platform is loaded."""
+    pyoracle = pyoracle_module()
+    if not os.path.exists(pyoracle.REF_SO):
+        return {"impl": "reference", "unavailable": "oracle/_ref (the reference's CPU lmp build) is missing"}
+    t0 = time.time()
+    ref, row, col, val, b = reference_system(args.N)
+    t_asm = time.time() - t0
+    threads = len(os.sched_getaffinity(0))
+    sess = pyoracle.RefMpirSession(ref, row, col, val, threads)
+    for _ in range(args.warmup):
+        sess.run(b, sample_inner=16)
+    secs = []
+    for _ in range(args.steps):
+        m = sess.run(b)
+        secs.append(m["seconds"])
+    sess.close()
+    r = b - ref.spmv(row, col, val, m["x"], impl=1, nthreads=threads)
+    relres = float(np.linalg.norm(r) / np.linalg.norm(b))
+    total = sum(secs)
+    v = args.steps / total
+    wl = load_workloads_file()
+    cb = {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+          "sample": (f"{args.steps} full solves to 1e-10 by the reference's CPUopenmp lmp objects (MPIR: "
+                     f"{m['outer']} corrections, {m['inner_total']} FP32 inner iterations), {threads} OpenMP threads"),
+          "cpu": host_cpu()}
     return {"metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": est * 1e3, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic (seeded)", "impl": "reference",
-            "config": {"workload": wl.CONFIGS["c3"]["desc"], "cells": args.N ** 3},
+            "warmup": args.warmup, "ms_per_step": total / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32-inner/f64-outer", "data": "synthetic (seeded)",
+            "impl": "reference",
+            "config": {"workload": wl.CONFIGS["c3"]["desc"], "cells": args.N ** 3, "dofs": len(b), "nnz": len(col)},
+            "solve": {"outer": m["outer"], "inner_total": m["inner_total"], "relres_true": relres,
+                      "seconds_min": min(secs), "seconds_max": max(secs)},
+            "setup_s": {"grf_and_assembly": t_asm}, "libraries_loaded": repo_libraries(),
             "cpu_baseline": cb, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
@@ -446,8 +507,7 @@ def run_b200(args, rank, world, local_rank, dist):
         line["serving"] = serving_bench(b200, pf, args.serve_requests, rank=rank, world=world,
                                         dist=dist if world > 1 else None)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb = cpu_baseline(row, col, val, b, res_mixed["outer"], res_mixed["inner_total"], fp64_iters,
-                          single_thread=True)
+        cb = cpu_baseline(row, col, val, b, single_thread=True)
         line["cpu_baseline"] = cb if cb else {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
                                               "sample": "oracle/_ref missing"}
     pf.close()
@@ -647,21 +707,20 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     dist = None
+    if args.impl == "reference":
+        # rank 0 alone times the reference's CPU code; other ranks exit at once
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
     if world > 1:
         import torch.distributed as dist
-        backend = "gloo" if args.impl == "reference" else "nccl"
-        if backend == "nccl":
-            import torch
-            torch.cuda.set_device(local_rank)
-        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+        import torch
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     try:
-        if args.impl == "reference":
-            if rank == 0:
-                print(json.dumps(run_reference(args)), flush=True)
-        else:
-            line = run_b200(args, rank, world, local_rank, dist)
-            if rank == 0:
-                print(json.dumps(line), flush=True)
+        line = run_b200(args, rank, world, local_rank, dist)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
     finally:
         if dist is not None:
             dist.destroy_process_group()

@@ -20,7 +20,15 @@
 // device address.  The first call on each device (with that device current)
 // resolves the address with cudaGetSymbolAddress, checks it and caches it;
 // later calls on that device reuse it.  Make that first call before any stream
-// capture begins.
+// capture begins.  The cached address belongs to the device's primary context:
+// after cudaDeviceReset on a device, this entry point must not be called on it
+// again in the same process.
+//
+// Errors: an error already pending in the CUDA runtime when the call starts
+// (an earlier asynchronous failure of the caller's own work) is left in place
+// for the caller and the call returns B200LA_ERR_CUDA without launching; a
+// failure of this call's own set-up or launch is cleared from the runtime and
+// reported as B200LA_ERR_CUDA.
 #include "b200la.h"
 #include "common.cuh"
 
@@ -91,14 +99,22 @@ extern "C" int b200la_dot_noalloc(int dtype, int n, const void *x, const void *y
     if ((dtype != B200LA_F64 && dtype != B200LA_F32) || n < 0 || !result_dev || (n > 0 && (!x || !y)))
         return B200LA_ERR_ARG;
     if (n > B200LA_NOALLOC_MAX_N) return B200LA_ERR_ARG;   // the scratch holds partials for at most this many
+    // an earlier, unrelated error stays with the caller: report it, clear nothing
+    if (cudaPeekAtLastError() != cudaSuccess) return B200LA_ERR_CUDA;
     int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return B200LA_ERR_DEVICE;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        cudaGetLastError();
+        return B200LA_ERR_DEVICE;
+    }
     double *scratch;
     {
         std::lock_guard<std::mutex> lock(g_mutex);
         if (!g_addr[dev]) {
             void *p = nullptr;
-            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return B200LA_ERR_CUDA;
+            if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) {
+                cudaGetLastError();   // this call's own failure, reported by the return code
+                return B200LA_ERR_CUDA;
+            }
             g_addr[dev] = static_cast<double *>(p);
         }
         scratch = g_addr[dev];

@@ -240,7 +240,12 @@ int b200la_dot_dev(b200la_ctx *ctx, int dtype, int n, const void *x, const void 
  * returns B200LA_ERR_ARG before anything is launched.  stream is a
  * cudaStream_t (NULL: the default stream).  The first call on a device sets up
  * the array's device address and should come before any stream capture; calls
- * whose kernels overlap on the GPU share the array and race. */
+ * whose kernels overlap on the GPU share the array and race.  The address is
+ * kept for the life of the process: after cudaDeviceReset on a device, do not
+ * call this again on that device.  An error already pending in the CUDA
+ * runtime when the call starts is left to the caller (the call returns
+ * B200LA_ERR_CUDA and launches nothing); this call's own CUDA failures are
+ * cleared and reported by the return code. */
 #define B200LA_NOALLOC_MAX_N 67108864
 int b200la_dot_noalloc(int dtype, int n, const void *x, const void *y, double *result_dev, void *stream);
 /* lVector::Axpy: y += alpha x (lvector.h:283) */

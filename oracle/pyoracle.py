@@ -679,6 +679,14 @@ class Ref:
     def max_threads(self):
         return self.lib.ref_max_threads()
 
+    def q1_rhs(self, seed, dim, N):
+        """The seeded right-hand side (the C restatement linked into this library)."""
+        b = np.empty((N + 1) ** dim)
+        self.lib.orc_q1_rhs.argtypes = [C.c_uint64, C.c_int, C.c_int, _f64p]
+        self.lib.orc_q1_rhs.restype = None
+        self.lib.orc_q1_rhs(seed, dim, N, b)
+        return b
+
 
 def _ref_timing_sigs(L):
     L.ref_mpir.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_int,
@@ -710,3 +718,41 @@ def ref_pcg_timed(ref, row, col, val, b, nthreads, reltol=1e-10, maxits=100000, 
     dt = ref.lib.ref_pcg_timed(impl, nthreads, n, len(col), _i32(row), _i32(col), _f64(val), _f64(b), x, reltol,
                                maxits, C.byref(it))
     return dict(seconds=dt, iters=it.value, x=x)
+
+
+class RefMpirSession:
+    """The reference's MPIR over CPUopenmp objects that persist between
+    solves (ref_mpir_create / ref_mpir_run / ref_mpir_threads), so that each
+    timed solve excludes the matrix copies and the preconditioner build."""
+
+    def __init__(self, ref, row, col, val, nthreads):
+        L = self.lib = ref.lib
+        L.ref_mpir_create.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f64p]
+        L.ref_mpir_create.restype = C.c_void_p
+        L.ref_mpir_threads.argtypes = [C.c_void_p, C.c_int]
+        L.ref_mpir_threads.restype = None
+        L.ref_mpir_run.argtypes = [C.c_void_p, _f64p, _f64p, C.c_int, C.c_double, C.c_double, C.c_int, C.c_int,
+                                   C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_double)]
+        L.ref_mpir_run.restype = C.c_double
+        L.ref_mpir_destroy.argtypes = [C.c_void_p]
+        L.ref_mpir_destroy.restype = None
+        self.n = len(row) - 1
+        self.h = L.ref_mpir_create(nthreads, self.n, len(col), _i32(row), _i32(col), _f64(val))
+
+    def threads(self, nthreads):
+        self.lib.ref_mpir_threads(self.h, nthreads)
+
+    def run(self, b, max_outer=50, reltol=1e-10, inner_reltol=1e-4, inner_maxits=100000, sample_inner=0):
+        x = np.zeros(self.n)
+        o, i, r = C.c_int(), C.c_int(), C.c_double()
+        dt = self.lib.ref_mpir_run(self.h, _f64(b), x, max_outer, reltol, inner_reltol, inner_maxits, sample_inner,
+                                   C.byref(o), C.byref(i), C.byref(r))
+        return dict(seconds=dt, outer=o.value, inner_total=i.value, res=r.value, x=x)
+
+    def close(self):
+        if self.h:
+            self.lib.ref_mpir_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

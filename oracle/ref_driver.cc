@@ -99,11 +99,15 @@ struct Control {
 
 // Preconditioner adaptor: z = M^-1 r for the types driven below.
 struct Precond {
-    int kind = 0;   // 0 none, 1 Jacobi, 2 MC-SGS, 3 ILU(0) level-scheduled, 4 ILU(0) multicoloured
+    // 0 none, 1 Jacobi, 2 MC-SGS, 3 ILU(0) level-scheduled, 4 ILU(0) multicoloured,
+    // 5 ILU(0) level-scheduled without the block split (factors applied by ilu_solve)
+    int kind = 0;
     lPreconditioner<double> *lp = nullptr;
+    lMatrix<double> *factors = nullptr;
     void apply(const lVector<double> &r, lVector<double> *z)
     {
         if (kind == 0) z->CopyFrom(r);
+        else if (kind == 5) factors->ilu_solve(r, z);
         else lp->ApplylPreconditioner(r, z);
     }
 };
@@ -461,8 +465,9 @@ int ref_pcg(int precond, int impl, int nthreads, int n, int nnz, const int *row,
 }
 
 // GMRES<LAD>::SolveRight restated (src/linear_solver/gmres.cc:285-510).
-// precond: 0 none, 3 ILU(0) level-scheduled, 4 ILU(0) multicoloured; with a
-// block preconditioner b and x are in its permuted numbering.
+// precond: 0 none, 3 ILU(0) level-scheduled, 4 ILU(0) multicoloured, 5 ILU(0)
+// level-scheduled applied by ilu_solve; with a block preconditioner b and x
+// are in its permuted numbering.
 int ref_gmres(int precond, int impl, int nthreads, int m, int n, int nnz, const int *row,
               const int *col, const double *val, const double *b, double *x, int maxits,
               double abstol, double reltol, double divtol, int *iters, double *res_out)
@@ -479,6 +484,28 @@ int ref_gmres(int precond, int impl, int nthreads, int m, int n, int nnz, const 
         CPU_CSR_lMatrix<double> *c = dynamic_cast<CPU_CSR_lMatrix<double> *>(Ap);
         A = make_matrix(impl, n, nnz, c->matrix.row, c->matrix.col, c->matrix.val, nthreads);
         delete Ap;
+    }
+    if (precond == 5) {
+        // lPreconditioner_MultiColoring_ILUp with level scheduling, Build steps
+        // (lpreconditioner_mc.cc:157-199): ilu0 of the operator in its own
+        // order, Levelscheduling of the factors, the factors and the operator
+        // reordered by that permutation.  The apply is the reference's
+        // ilu_solve on the reordered factors (the same triangular solves that
+        // the block apply performs level by level, without the per-level-pair
+        // submatrices whose extraction costs O(levels^2 nnz) at set-up).
+        lMatrix<double> *F = make_matrix(0, n, nnz, row, col, val, 1);
+        F->ilu0();
+        int nl = 0, *ls = nullptr, *pi = nullptr;
+        dynamic_cast<CPU_CSR_lMatrix<double> *>(F)->Levelscheduling(nl, &ls, &pi);
+        F->Reorder(pi);
+        lMatrix<double> *Ap = make_matrix(0, n, nnz, row, col, val, 1);
+        Ap->Reorder(pi);
+        delete A;
+        CPU_CSR_lMatrix<double> *c = dynamic_cast<CPU_CSR_lMatrix<double> *>(Ap);
+        A = make_matrix(impl, n, nnz, c->matrix.row, c->matrix.col, c->matrix.val, nthreads);
+        delete Ap;
+        delete[] ls; delete[] pi;
+        P.factors = F;
     }
     lVector<double> *vb = make_vector(impl, n, b, nthreads), *vx = make_vector(impl, n, x, nthreads);
     Control ctl{maxits, abstol, reltol, divtol, 0.0};
@@ -551,7 +578,7 @@ int ref_gmres(int precond, int impl, int nthreads, int m, int n, int nnz, const 
     *iters = iter;
     *res_out = res;
     for (auto &v : V) delete v;
-    delete w; delete z; delete vb; delete vx; delete A; delete P.lp;
+    delete w; delete z; delete vb; delete vx; delete A; delete P.lp; delete P.factors;
     return conv;
 }
 
@@ -858,6 +885,98 @@ double ref_mpir(int impl, int nthreads, int n, int nnz, const int *row, const in
     *res_out = res;
     delete Ah; delete Al; delete vb; delete vx; delete resh; delete corh; delete resl; delete corl; delete dl;
     return dt;
+}
+
+// The same MPIR over objects that persist between solves, so that repeated
+// timed solves of one system do not rebuild the matrices: ref_mpir_create
+// copies the CSR into the reference's FP64 and FP32 CPUopenmp matrices and
+// builds the FP32 Jacobi preconditioner; ref_mpir_run solves once from x
+// (seconds of the solve, as ref_mpir); ref_mpir_threads changes the OpenMP
+// thread count of every object.
+struct MpirSession {
+    int n;
+    lMatrix<double> *Ah;
+    lMatrix<float> *Al;
+    lVector<double> *vb, *vx, *resh, *corh;
+    lVector<float> *resl, *corl, *dl;
+    lPreconditioner_Jacobi<float> *J;
+};
+
+void *ref_mpir_create(int nthreads, int n, int nnz, const int *row, const int *col, const double *val)
+{
+    MpirSession *s = new MpirSession();
+    s->n = n;
+    s->Ah = make_matrix_t<double>(1, n, nnz, row, col, val, nthreads);
+    s->Al = make_matrix_t<float>(1, n, nnz, row, col, val, nthreads);
+    s->vb = make_vector_t<double>(1, n, nthreads);
+    s->vx = make_vector_t<double>(1, n, nthreads);
+    s->resh = s->vb->CloneWithoutContent();
+    s->corh = s->vb->CloneWithoutContent();
+    s->resl = make_vector_t<float>(1, n, nthreads);
+    s->corl = make_vector_t<float>(1, n, nthreads);
+    s->dl = s->resl->CloneWithoutContent();
+    s->J = new lPreconditioner_Jacobi<float>();
+    s->J->Init(*s->dl);
+    s->J->SetupOperator(*s->Al);
+    s->J->Build();
+    return s;
+}
+
+void ref_mpir_threads(void *h, int nthreads)
+{
+    MpirSession *s = static_cast<MpirSession *>(h);
+    const int t = nthreads > 0 ? nthreads : 1;
+    dynamic_cast<CPUopenmp_CSR_lMatrix<double> *>(s->Ah)->set_num_threads(t);
+    dynamic_cast<CPUopenmp_CSR_lMatrix<float> *>(s->Al)->set_num_threads(t);
+    for (lVector<double> *v : {s->vb, s->vx, s->resh, s->corh})
+        dynamic_cast<CPUopenmp_lVector<double> *>(v)->set_num_threads(t);
+    for (lVector<float> *v : {s->resl, s->corl, s->dl})
+        dynamic_cast<CPUopenmp_lVector<float> *>(v)->set_num_threads(t);
+}
+
+double ref_mpir_run(void *h, const double *b, double *x, int max_outer, double reltol, double inner_reltol,
+                    int inner_maxits, int sample_inner, int *outer_done, int *inner_done, double *res_out)
+{
+    MpirSession *s = static_cast<MpirSession *>(h);
+    const int n = s->n;
+    std::memcpy(dynamic_cast<CPU_lVector<double> *>(s->vb)->buffer, b, sizeof(double) * n);
+    std::memcpy(dynamic_cast<CPU_lVector<double> *>(s->vx)->buffer, x, sizeof(double) * n);
+    const auto t0 = std::chrono::steady_clock::now();
+    s->Ah->VectorMult(*s->vx, s->resh);
+    s->resh->ScaleAdd(-1.0, *s->vb);
+    double res = s->resh->Norm2();
+    const double res0 = res;
+    int outer = 0, inner_total = 0;
+    while (res > 0.0 && res > reltol * res0 && outer < max_outer &&
+           (sample_inner <= 0 || inner_total < sample_inner)) {
+        ++outer;
+        s->resl->CastFrom(*s->resh);
+        s->corl->Zeros();
+        Control ic{inner_maxits, 0.0, inner_reltol, 1e6, 0.0};
+        int it = 0;
+        pcg_t<float>(*s->Al, *s->J, *s->resl, *s->corl, ic, sample_inner > 0 ? sample_inner - inner_total : 0, &it);
+        inner_total += it;
+        s->corh->CastFrom(*s->corl);
+        s->vx->Axpy(*s->corh, 1.0);
+        s->Ah->VectorMult(*s->vx, s->resh);
+        s->resh->ScaleAdd(-1.0, *s->vb);
+        res = s->resh->Norm2();
+    }
+    const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    std::memcpy(x, dynamic_cast<CPU_lVector<double> *>(s->vx)->buffer, sizeof(double) * n);
+    *outer_done = outer;
+    *inner_done = inner_total;
+    *res_out = res;
+    return dt;
+}
+
+void ref_mpir_destroy(void *h)
+{
+    MpirSession *s = static_cast<MpirSession *>(h);
+    delete s->J;
+    delete s->Ah; delete s->Al; delete s->vb; delete s->vx; delete s->resh; delete s->corh;
+    delete s->resl; delete s->corl; delete s->dl;
+    delete s;
 }
 
 // FP64 Jacobi-CG over the reference's objects with an iteration cap, timed

@@ -82,3 +82,36 @@ def test_full_size_assembly_and_analysis_vs_oracle(b200, oracle, dim, N, kind):
         assert c1[0] == 8
     l1, l2 = b200.levelscheduling(row, col), oracle.levelscheduling(row, col)
     assert l1[0] == l2[0] and np.array_equal(l1[2], l2[2])
+
+
+def test_config_structure_bitexact_vs_reference_full_size(b200):
+    """The benchmark configurations at their full sizes: the platform's host
+    assembly, colouring (3-D 128^3) and level scheduling (2-D 512^2
+    convection-diffusion) equal the reference's own (SHA-256 of the arrays
+    written by tests/golden/gen_config_counts.py from oracle/_ref)."""
+    import hashlib
+    import json
+    import os
+
+    def sha(*arrays):
+        h = hashlib.sha256()
+        for a in arrays:
+            h.update(np.ascontiguousarray(a).tobytes())
+        return h.hexdigest()
+
+    with open(os.path.join(os.path.dirname(__file__), "golden", "config_counts.json")) as f:
+        cc = json.load(f)
+    row, col, val = b200.q1_assemble(2, 256)
+    assert sha(row, col, val) == cc["c1"]["csr_sha256"]
+    row, col, val = b200.q1_assemble(3, 128)
+    assert sha(row, col, val) == cc["c2"]["csr_sha256"]
+    nc, sizes, perm = b200.multicoloring(row, col)
+    assert nc == cc["c2"]["colours"] == 8
+    assert [int(v) for v in sizes[:nc]] == cc["c2"]["colour_sizes"]
+    assert sha(np.asarray(perm, np.int32)) == cc["c2"]["multicoloring_perm_sha256"]
+    row, col, val = b200.q1_assemble(2, 512, 1, None, nu=1e-3, beta=(1.0, 0.5))
+    assert sha(row, col, val) == cc["c4"]["csr_sha256"]
+    nl, lsizes, lperm = b200.levelscheduling(row, col)
+    assert nl == cc["c4"]["levels"] == 1537
+    assert sha(np.asarray(lsizes[:nl], np.int32)) == cc["c4"]["level_sizes_sha256"]
+    assert sha(np.asarray(lperm, np.int32)) == cc["c4"]["levelscheduling_perm_sha256"]

@@ -71,3 +71,6 @@ def test_reference_arm_under_torchrun():
     assert rec["impl"] == "reference" and rec["value"] > 0
     assert rec["cpu_baseline"]["kind"] == "reference" and rec["cpu_baseline"]["cores"] >= 1
     assert rec["e2e"]["h2d_bytes_per_step"] == 0
+    # the arm runs the reference's own code only: no library of this platform
+    assert rec["libraries_loaded"] == ["oracle/_ref/libhiflow_lmp_ref.so"], rec["libraries_loaded"]
+    assert rec["solve"]["relres_true"] <= 1e-10

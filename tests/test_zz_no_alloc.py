@@ -44,6 +44,34 @@ def test_dot_noalloc_matches_dot_twice_in_a_row(b200):
             assert got[0] == got[1]   # same order of summation on every call
 
 
+def test_dot_noalloc_full_scratch_and_explicit_stream(b200):
+    """n at the limit fills every partial slot (the last one included); the
+    call is also made on a caller's stream and checked against b200la_dot."""
+    import torch
+    pf = b200.Platform(0)
+    L = b200.lib()
+    n = b200.NOALLOC_MAX_N
+    x = torch.ones(n, dtype=torch.float32, device="cuda")
+    out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda")
+    assert L.b200la_dot_noalloc(b200.F32, n, _ptr(x), _ptr(x), _ptr(out), None) == 0
+    torch.cuda.synchronize()
+    assert out[0].item() == float(n)          # exact: every product is 1
+    del x
+    m = 3_000_017
+    rng = np.random.default_rng(11)
+    a = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
+    c = torch.from_numpy(rng.uniform(-1, 1, m)).cuda()
+    ref = C.c_double()
+    pf.check(L.b200la_dot(pf.h, b200.F64, m, _ptr(a), _ptr(c), C.byref(ref)))
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(s):
+        assert L.b200la_dot_noalloc(b200.F64, m, _ptr(a), _ptr(c), C.c_void_p(out.data_ptr() + 8),
+                                    C.c_void_p(s.cuda_stream)) == 0
+    s.synchronize()
+    np.testing.assert_allclose(out[1].item(), ref.value, rtol=1e-12, atol=1e-14 * m)
+
+
 def test_dot_noalloc_rejects_sizes_beyond_its_scratch(b200):
     import torch
     L = b200.lib()
