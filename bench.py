@@ -149,6 +149,19 @@ def stencil_spmv_bytes(n, nb, vbytes):
     return vbytes * slots * 32 * ((n + 31) // 32) + 2 * vbytes * n
 
 
+def half_spmv_bytes(n, nb, vbytes):
+    """Algorithmic bytes of one SpMV on the half stencil layout of a symmetric
+    stencil operator: the diagonal and upper-half values (FP64: 2 + 3 U
+    positions per row; FP32: max(U, 2) groups of four, U = (nb - 1) / 2) in
+    zero-padded chunks of 32 rows, one identity-row mask word per chunk, x
+    read once, y written once.  The lower half is the same values read a
+    second time, from L2, by the neighbouring rows."""
+    u = (nb - 1) // 2
+    slots = 4 * max(u, 2) if vbytes == 4 else 2 + 3 * u
+    nch = (n + 31) // 32
+    return vbytes * slots * 32 * nch + 4 * nch + 2 * vbytes * n
+
+
 # --------------------------------------------------------------- ranks
 
 def reduce_max(x, dist, device):
@@ -401,7 +414,7 @@ def run_b200(args, rank, world, local_rank, dist):
         t_ms = pf.timer_stop() / reps
         storage = A.info()["storage"]
         by = {"csr": spmv_bytes(n, nnz, vbytes), "dictionary": dict_spmv_bytes(n, nnz, vbytes),
-              "stencil": stencil_spmv_bytes(n, 9, vbytes)}[storage]
+              "stencil": stencil_spmv_bytes(n, 9, vbytes), "half-stencil": half_spmv_bytes(n, 9, vbytes)}[storage]
         return by, t_ms, by / (t_ms * 1e-3) / 1e9, storage
 
     by64, t64, gbs64, st64 = spmv_rate(A64, 8)

@@ -745,7 +745,7 @@ class CSR_lMatrix:
         npat, uses = C.c_int(), C.c_int()
         self.pf.check(lib().b200la_csr_format(self.h, C.byref(npat), C.byref(uses)))
         out["row_patterns"], out["uses_pattern_dictionary"] = npat.value, bool(uses.value)
-        out["storage"] = {0: "csr", 1: "dictionary", 2: "stencil"}[uses.value]
+        out["storage"] = {0: "csr", 1: "dictionary", 2: "stencil", 3: "half-stencil"}[uses.value]
         return out
 
     def CastFrom(self, dtype):

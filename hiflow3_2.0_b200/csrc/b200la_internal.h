@@ -84,6 +84,11 @@ struct b200la_csr {
     void *st_val = nullptr;
     int st_nb = 0;                    // bands (0: no stencil layout)
     int st_use = 0;                   // SpMV of the whole operator runs on it
+    // half stencil layout (stencil operators symmetric outside their identity
+    // rows): diagonal and upper half, identity-row mask; see kernels.cuh
+    void *sh_val = nullptr;
+    unsigned *sh_mask = nullptr;
+    int sh_use = 0;                   // SpMV runs on it instead of the full layout
 };
 
 struct b200la_precond {

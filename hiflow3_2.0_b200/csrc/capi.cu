@@ -107,6 +107,9 @@ CsrView csr_view(const b200la_csr *A)
     v.st_nb = A->st_nb;
     v.st_use = A->st_use && A->st_val != nullptr;
     for (int b = 0; b < kMaxBands; ++b) v.st_center[b] = b < A->st_nb ? A->st_union[3 * b + 1] : 0;
+    v.sh_val = A->sh_val;
+    v.sh_mask = A->sh_mask;
+    v.sh_use = A->sh_use && A->sh_val != nullptr;
     return v;
 }
 
@@ -453,9 +456,72 @@ static void stencil_plan(b200la_csr *A, const std::vector<int> &uni)
     A->st_nb = L / 3;
 }
 
+// Whether the half stencil layout is built for symmetric stencil operators.
+// B200LA_HALF_STENCIL = 0: never, 1 (default): whenever the operator is
+// symmetric outside its identity rows.
+static bool half_policy()
+{
+    const char *e = std::getenv("B200LA_HALF_STENCIL");
+    return !e || std::atoi(e) != 0;
+}
+
+static void free_half(b200la_csr *A)
+{
+    if (A->sh_val) cudaFree(A->sh_val);
+    if (A->sh_mask) cudaFree(A->sh_mask);
+    A->sh_val = nullptr;
+    A->sh_mask = nullptr;
+    A->sh_use = 0;
+}
+
+// The half stencil layout from the full one: built when the band centres are
+// symmetric about a centre band at offset 0 and the values are symmetric
+// bit for bit between rows that are not identity rows; dropped otherwise.
+static int build_half(b200la_ctx *ctx, b200la_csr *A)
+{
+    const int nb = A->st_nb;
+    bool ok = half_policy() && A->st_val && (nb == 3 || nb == 9);
+    for (int b = 0; ok && b < nb; ++b)
+        if (A->st_union[3 * b + 1] != -A->st_union[3 * (nb - 1 - b) + 1]) ok = false;
+    if (!ok) {
+        free_half(A);
+        return B200LA_OK;
+    }
+    const size_t es = dsize(A->dtype), len = half_len(A->n, nb, A->dtype), nch = (A->n + 31) / 32;
+    cudaError_t e;
+    if (!A->sh_val) {
+        // one word past the mask receives the symmetry check's result
+        if ((e = cudaMalloc(&A->sh_val, es * len)) || (e = cudaMalloc(&A->sh_mask, sizeof(unsigned) * (nch + 1)))) {
+            free_half(A);
+            return ctx_fail(ctx, B200LA_ERR_ALLOC, "half stencil layout", e);
+        }
+    }
+    int centers[kMaxBands];
+    for (int b = 0; b < nb; ++b) centers[b] = A->st_union[3 * b + 1];
+    int *asym = reinterpret_cast<int *>(A->sh_mask + nch);
+    int h_asym = 0;
+    if ((e = cudaMemsetAsync(asym, 0, sizeof(int), ctx->stream)) ||
+        (e = launch_stencil_to_half(A->dtype, A->n, nb, centers, A->st_val, A->sh_val, A->sh_mask, asym,
+                                    ctx->stream)) ||
+        (e = cudaMemcpyAsync(&h_asym, asym, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream)) ||
+        (e = cudaStreamSynchronize(ctx->stream))) {
+        free_half(A);
+        return ctx_fail(ctx, B200LA_ERR_CUDA, "half stencil layout", e);
+    }
+    if (h_asym) {
+        free_half(A);
+        return B200LA_OK;
+    }
+    A->sh_use = 1;
+    return B200LA_OK;
+}
+
 static int build_stencil(b200la_ctx *ctx, b200la_csr *A)
 {
-    if (!A->st_nb) return B200LA_OK;
+    if (!A->st_nb) {
+        free_half(A);
+        return B200LA_OK;
+    }
     const size_t es = dsize(A->dtype), len = stencil_len(A->n, A->st_nb, A->dtype);
     cudaError_t e;
     if (!A->st_val) {
@@ -467,7 +533,7 @@ static int build_stencil(b200la_ctx *ctx, b200la_csr *A)
                                    ctx->stream)) ||
         (e = cudaStreamSynchronize(ctx->stream)))
         return ctx_fail(ctx, B200LA_ERR_CUDA, "stencil layout", e);
-    return B200LA_OK;
+    return build_half(ctx, A);
 }
 
 static int upload_lines(b200la_ctx *ctx, b200la_csr *A, const std::vector<int> &ls, const std::vector<int> &lsp,
@@ -652,6 +718,7 @@ extern "C" int b200la_csr_destroy(b200la_csr *A)
     if (A->sell_off) cudaFree(A->sell_off);
     if (A->sell_val) cudaFree(A->sell_val);
     if (A->st_val) cudaFree(A->st_val);
+    free_half(A);
     delete A;
     return B200LA_OK;
 }
@@ -675,6 +742,9 @@ extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, 
     B->sell_len = 0;
     B->st_val = nullptr;
     B->st_use = stencil_policy(dtype);
+    B->sh_val = nullptr;
+    B->sh_mask = nullptr;
+    B->sh_use = 0;
     const size_t pad = 8, es = dsize(dtype);
     cudaError_t e;
     if (A->pid) {
@@ -744,7 +814,9 @@ extern "C" int b200la_csr_format(const b200la_csr *A, int *npat, int *uses_dict)
 {
     if (!A) return B200LA_ERR_ARG;
     if (npat) *npat = A->pid ? A->npat : 0;
-    if (uses_dict) *uses_dict = (A->st_use && A->st_val) ? 2 : (A->pid && A->use_pat) ? 1 : 0;
+    if (uses_dict)
+        *uses_dict = (A->st_use && A->sh_use && A->sh_val) ? 3 : (A->st_use && A->st_val) ? 2
+                                                                 : (A->pid && A->use_pat) ? 1 : 0;
     return B200LA_OK;
 }
 

@@ -87,6 +87,18 @@ inline size_t stencil_len(int n, int nb, int dtype)
     const int W = dtype == 1 ? 4 : 1, G = (3 * nb + W - 1) / W;
     return (size_t)((n + 31) / 32) * 32 * G * W;
 }
+// Half stencil layout of a symmetric stencil operator (see spmv.cu): U =
+// (nb - 1) / 2 bands above the centre band.  FP64 stores 2 + 3 U positions
+// per row (diagonal, +1, the upper bands); FP32 stores max(U, 2) groups of
+// four (group u: band U + 1 + u in slots 0-2; slot 3 holds the diagonal in
+// group 0 and the +1 entry in group 1).
+__host__ __device__ constexpr int half_positions(int nb) { return 2 + 3 * ((nb - 1) / 2); }
+__host__ __device__ constexpr int half_groups(int nb) { return (nb - 1) / 2 < 2 ? 2 : (nb - 1) / 2; }
+inline size_t half_len(int n, int nb, int dtype)
+{
+    const size_t rows = (size_t)((n + 31) / 32) * 32;
+    return dtype == 1 ? rows * 4 * half_groups(nb) : rows * half_positions(nb);
+}
 
 struct CsrView {
     const int *row;
@@ -125,6 +137,12 @@ struct CsrView {
     const void *st_val;
     int st_nb, st_use;
     int st_center[kMaxBands];
+    // half stencil layout (null when absent: the operator is not symmetric
+    // outside its identity rows): sh_val by half_positions / half_groups,
+    // sh_mask[c] bit l set when row 32 c + l has no nonzero off-diagonal value
+    const void *sh_val;
+    const unsigned *sh_mask;
+    int sh_use;
 };
 
 constexpr int kMaxPatterns = 1024;
@@ -160,6 +178,13 @@ cudaError_t launch_csr_to_sell(int dtype, int n, const int *row, const void *val
 // the 3 nb offsets of the bands in ascending order.
 cudaError_t launch_csr_to_stencil(int dtype, int n, const int *row, const int *col, const void *val, const int *uni,
                                   int nb, void *out, cudaStream_t st);
+// Half stencil layout from the full one (same dtype): the identity-row mask,
+// the diagonal and upper half (a row without nonzero off-diagonal values
+// keeps, in its upper slots, the transposed entries its neighbours need),
+// and *asym != 0 afterwards when some pair of non-identity rows i, j has
+// a_ij != a_ji bitwise.
+cudaError_t launch_stencil_to_half(int dtype, int n, int nb, const int *center, const void *st_val, void *sh_val,
+                                   unsigned *sh_mask, int *asym, cudaStream_t st);
 cudaError_t launch_spmv(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st);
 
 // ---- BLAS1 (dtype 0 double, 1 float; scalars in double) ----

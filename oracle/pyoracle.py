@@ -450,7 +450,7 @@ class Ref:
 
     def __init__(self, path=REF_SO):
         if not os.path.exists(path):
-            raise FileNotFoundError(f"{path} missing: build it with `make -C oracle` where the "
+            raise FileNotFoundError(f"{path} missing: build it with `make -C oracle REF=<HiFlow3 source tree>` where the "
                                     "reference sources are present")
         L = self.lib = C.CDLL(path)
         L.ref_coo_to_csr.argtypes = [C.c_int, C.c_int, _i32p, _i32p, C.c_void_p, _i32p, _i32p, C.c_void_p]
@@ -669,6 +669,18 @@ class Ref:
         rc = self.lib.ref_lmp_cg(len(row) - 1, len(col), _i32(row), _i32(col), _f64(val), _f64(b), x,
                                  rel_eps, abs_eps, max_iter)
         return rc, x
+
+    def lmp_cg_iters(self, row, col, val, b, rel_eps=0.0, abs_eps=0.0, max_iter=100, jacobi=False):
+        """CGFunctor<double, true> on CPUsimple objects, optionally with
+        lPreconditioner_Jacobi: (code, x, iterations)."""
+        L = self.lib
+        L.ref_lmp_cg_iters.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f64p, _f64p, _f64p, C.c_double, C.c_double,
+                                       C.c_int, C.c_int, C.POINTER(C.c_int)]
+        x = np.zeros(len(row) - 1)
+        it = C.c_int()
+        rc = L.ref_lmp_cg_iters(len(row) - 1, len(col), _i32(row), _i32(col), _f64(val), _f64(b), x, rel_eps,
+                                abs_eps, max_iter, int(jacobi), C.byref(it))
+        return rc, x, it.value
 
     def time_spmv(self, row, col, val, x, nthreads, reps):
         y = np.empty(len(row) - 1)

@@ -596,6 +596,30 @@ int ref_lmp_cg(int n, int nnz, const int *row, const int *col, const double *val
     return rc;
 }
 
+// The same functor (CGFunctor<double, true>, the harness of
+// benchmark_local_solver) with or without lPreconditioner_Jacobi, reporting
+// the iterations it ran (its max_iter argument on return).
+int ref_lmp_cg_iters(int n, int nnz, const int *row, const int *col, const double *val, const double *b,
+                     double *x, double rel_eps, double abs_eps, int max_iter, int jacobi, int *iters)
+{
+    lMatrix<double> *A = make_matrix(0, n, nnz, row, col, val, 1);
+    lVector<double> *vb = make_vector(0, n, b, 1), *vx = make_vector(0, n, x, 1);
+    lVector<double> *d = make_vector(0, n, nullptr, 1);
+    lPreconditioner_Jacobi<double> J;
+    if (jacobi) {
+        J.Init(*d);
+        J.SetupOperator(*A);
+        J.Build();
+    }
+    CGFunctor<double, true> f;
+    int mi = max_iter;
+    const int rc = f(vx, vb, A, rel_eps, abs_eps, mi, -1, jacobi ? &J : (lPreconditioner<double> *)nullptr);
+    *iters = mi;
+    copy_out(*vx, x);
+    delete A; delete vb; delete vx; delete d;
+    return rc;
+}
+
 // Wall time of `reps` CPUopenmp_CSR_lMatrix::VectorMult calls
 // (openmp/CPUopenmp_csr_lmatrix.cc:144-165), in seconds.
 double ref_time_spmv(int nthreads, int reps, int n, int nnz, const int *row, const int *col,

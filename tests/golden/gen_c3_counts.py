@@ -5,7 +5,7 @@ The CPU baseline times a bounded sample of the reference's mixed-precision
 solve (MPIR, FP32 Jacobi-CG inside FP64 defect correction) and of its FP64
 Jacobi-CG, and scales the per-iteration cost by these full-solve counts.
 
-Usage:  make -C oracle && python tests/golden/gen_c3_counts.py [N]
+Usage:  make -C oracle REF=<HiFlow3 source tree> && python tests/golden/gen_c3_counts.py [N]
 """
 import importlib.util
 import json

@@ -23,7 +23,7 @@ the solution (its 2-norm and its dot product with a seeded weight vector
 w = numpy default_rng(7).uniform(-1, 1, n)), plus its true relative residual.
 The solution vectors themselves (17 MB at 128^3) are not stored.
 
-Usage:  make -C oracle && python tests/golden/gen_config_counts.py [c1 c2 c4]
+Usage:  make -C oracle REF=<HiFlow3 source tree> && python tests/golden/gen_config_counts.py [c1 c2 c4]
 """
 import hashlib
 import json

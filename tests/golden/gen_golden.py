@@ -10,7 +10,7 @@ are written out beside them:
 * test-legacy/lmp_test.cc:38-89 and test-legacy/cuda_test.cc:27-100 (SpMV),
 * test/LinearAlgebra/cg.cc:35-91 and gmres.cc:35-91 (3x3 solve).
 
-Usage:  make -C oracle && python tests/golden/gen_golden.py
+Usage:  make -C oracle REF=<HiFlow3 source tree> && python tests/golden/gen_golden.py
 """
 import os
 import sys

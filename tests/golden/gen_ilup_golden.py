@@ -9,7 +9,7 @@ sources) on small Q1 operators assembled by the reference's own code path:
     sizes, permuted operator and one apply;
   - right-preconditioned GMRES(30) with ILU(1) level-scheduled: iterations and x.
 
-Usage:  make -C oracle && python tests/golden/gen_ilup_golden.py
+Usage:  make -C oracle REF=<HiFlow3 source tree> && python tests/golden/gen_ilup_golden.py
 """
 import os
 import sys

@@ -11,7 +11,7 @@ Rotg on seeded vectors with repeated magnitudes, signed zeros and lengths
 around the reference's unroll-by-5.  The inputs and the reference's outputs
 go into the fixture.
 
-Usage:  make -C oracle && python tests/golden/gen_matops_golden.py
+Usage:  make -C oracle REF=<HiFlow3 source tree> && python tests/golden/gen_matops_golden.py
 """
 import os
 import sys

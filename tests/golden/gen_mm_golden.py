@@ -7,7 +7,7 @@ unmodified CPU lmp sources), writes CSR matrices and vectors with the
 reference's WriteFile, and stores the reference's CSR arrays, values and
 written texts in ``mm/mm_golden.npz``.
 
-Usage:  make -C oracle && python tests/golden/gen_mm_golden.py
+Usage:  make -C oracle REF=<HiFlow3 source tree> && python tests/golden/gen_mm_golden.py
 """
 import ctypes as C
 import os

@@ -170,7 +170,9 @@ def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, tma, stencil, di
     monkeypatch.setenv("B200LA_SELL_TMA", tma)
     monkeypatch.setenv("B200LA_STENCIL", stencil)
     stencil_ok = N > 1     # N = 1: every row is a corner, the padding exceeds the limit
-    want = "stencil" if (stencil == "2" and stencil_ok) else "dictionary" if mode == "2" else "csr"
+    # symmetric operators (Poisson, kind 0) take the half stencil layout
+    want = (("half-stencil" if kind == 0 else "stencil") if (stencil == "2" and stencil_ok)
+            else "dictionary" if mode == "2" else "csr")
     row, col, val = oracle.q1_assemble(dim, N, kind, None, nu=1e-3, beta=(1.0, 0.5))
     n = len(row) - 1
     x = np.random.default_rng(4).uniform(-1, 1, n)
@@ -190,6 +192,60 @@ def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, tma, stencil, di
     A32.VectorMult(pf.vector(x32, b200.F32), y32)
     y32_ref = oracle.spmv(row, col, val.astype(np.float32), x32)
     assert np.all(np.abs(y32.numpy().astype(np.float64) - y32_ref) <= 2e-6 * sc + 1e-30)
+
+
+@pytest.mark.parametrize("dim,N,coef", [(2, 5, False), (2, 63, True), (3, 3, False), (3, 9, True), (3, 64, True)])
+def test_spmv_half_stencil_bitwise(pf, b200, oracle, dim, N, coef, monkeypatch):
+    """The half stencil layout (diagonal and upper half; the lower half read
+    from the rows that own it) gives y bit for bit equal to the full stencil
+    layout, in both precisions and in every fused epilogue (y = Ax, y += Ax,
+    y = Ax with x.y, r = b - Ax with ||r||^2), and within the SpMV tolerance
+    of the oracle."""
+    rng = np.random.default_rng(100 * dim + N)
+    kc = np.exp(rng.standard_normal(N ** dim)) if coef else None
+    row, col, val = oracle.q1_assemble(dim, N, 0, kc)
+    n = len(row) - 1
+    x, y0, b = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
+    outs = {}
+    for half in ("1", "0"):
+        monkeypatch.setenv("B200LA_HALF_STENCIL", half)
+        A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+        A32 = A.CastFrom(b200.F32)
+        assert A.info()["storage"] == A32.info()["storage"] == ("half-stencil" if half == "1" else "stencil")
+        res = []
+        for M, dt in ((A, b200.F64), (A32, b200.F32)):
+            cast = (lambda v: v) if dt == b200.F64 else (lambda v: v.astype(np.float32))
+            xv, yv = pf.vector(cast(x), dt), pf.vector(n, dt)
+            M.VectorMult(xv, yv)
+            res.append(yv.numpy())
+            ya = pf.vector(cast(y0), dt)
+            M.VectorMultAdd(xv, ya)
+            res.append(ya.numpy())
+            res.append(np.array([M.VectorMultDot(xv, yv)]))
+            rv = pf.vector(n, dt)
+            res.append(np.array([M.Residual(pf.vector(cast(b), dt), xv, rv)]))
+            res.append(rv.numpy())
+        outs[half] = res
+    for a, c in zip(outs["1"], outs["0"]):
+        assert np.array_equal(a.view(np.uint8), c.view(np.uint8))
+    assert spmv_ok(outs["1"][0], oracle.spmv(row, col, val, x), row_scale(row, col, val, x), 1e-13)
+
+
+def test_spmv_half_stencil_rejects_asymmetry(pf, b200, oracle):
+    """One off-diagonal entry changed between two interior rows: the operator
+    is no longer symmetric, the half layout is not used, and SpMV stays exact."""
+    row, col, val = oracle.q1_assemble(3, 6, 0, None)
+    n = len(row) - 1
+    r = (n // 2)
+    j = next(k for k in range(row[r], row[r + 1]) if col[k] != r and val[k] != 0.0)
+    val = val.copy()
+    val[j] *= 1.0 + 2.0 ** -40
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    assert A.info()["storage"] == "stencil"
+    x = np.random.default_rng(5).uniform(-1, 1, n)
+    yv = pf.vector(n)
+    A.VectorMult(pf.vector(x), yv)
+    assert spmv_ok(yv.numpy(), oracle.spmv(row, col, val, x), row_scale(row, col, val, x), 1e-13)
 
 
 def test_spmv_degenerate_shapes(pf, b200):
