@@ -162,6 +162,26 @@ def half_spmv_bytes(n, nb, vbytes):
     return vbytes * slots * 32 * nch + 4 * nch + 2 * vbytes * n
 
 
+def reference_gpu_spmv(row, col, val, x, reps=20):
+    """The reference's own GPU SpMV (kernel_spmv_csr_scalar of
+    lmp/cuda/cuda_spmv_kernel_csr_scalar.h, one thread per row, 256 per block,
+    as GPUscalar_CSR_lMatrix::VectorMult launches it), built for sm_100a into
+    baseline/_ref and timed on the same FP64 CSR matrix: mean kernel time of
+    back-to-back launches, and y for a check.  None when the library is absent."""
+    import ctypes as C
+    so = os.path.join(ROOT, "baseline", "_ref", "libref_gpu_spmv.so")
+    if not os.path.exists(so):
+        return None
+    L = C.CDLL(so)
+    n = len(row) - 1
+    y = np.empty(n)
+    ms = C.c_double()
+    rc = L.refgpu_spmv(0, n, len(col), C.c_void_p(row.ctypes.data), C.c_void_p(col.ctypes.data),
+                       C.c_void_p(val.ctypes.data), C.c_void_p(x.ctypes.data), C.c_void_p(y.ctypes.data), reps,
+                       C.byref(ms))
+    return (ms.value, y) if rc == 0 else None
+
+
 # --------------------------------------------------------------- ranks
 
 def reduce_max(x, dist, device):
@@ -440,6 +460,19 @@ def run_b200(args, rank, world, local_rank, dist):
     fp64c_iters = cgc.iter()
     del A64c, cgc, xc
     peak, peak_kind = measured_peaks()
+    # the reference's own GPU kernel on the same FP64 CSR matrix
+    xr = np.random.default_rng(1).uniform(-1, 1, n)
+    rg = reference_gpu_spmv(row, col, val, xr)
+    ref_gpu = None
+    if rg is not None:
+        import scipy.sparse as sp
+        y_host = sp.csr_matrix((val, col, row), shape=(n, n)) @ xr
+        scale = sp.csr_matrix((np.abs(val), col, row), shape=(n, n)) @ np.abs(xr)
+        by_ref = spmv_bytes(n, nnz, 8)
+        ref_gpu = {"kernel": "kernel_spmv_csr_scalar<double> (the reference's GPUscalar CSR SpMV, sm_100a build)",
+                   "us": rg[0] * 1e3, "gbs": by_ref / (rg[0] * 1e-3) / 1e9, "bytes": by_ref,
+                   "frac_of_peak": by_ref / (rg[0] * 1e-3) / 1e9 / peak,
+                   "max_rel_err": float(np.max(np.abs(rg[1] - y_host) / np.maximum(scale, 1e-300)))}
     # SURVEY units: one FP64 / FP32 SpMV of this operator (CSR algorithmic bytes)
     unit64, unit32 = spmv_bytes(n, nnz, 8), spmv_bytes(n, nnz, 4)
 
@@ -499,7 +532,8 @@ def run_b200(args, rank, world, local_rank, dist):
                  "fp64_csr": {"us": t64c * 1e3, "gbs": gbs64c, "bytes": by64c, "frac_of_peak": gbs64c / peak},
                  "fp32_inner": {"storage": st32, "us": t32 * 1e3, "gbs": gbs32, "bytes": by32,
                                 "frac_of_peak": gbs32 / peak, "csr_unit_gbs": unit32 / (t32 * 1e-3) / 1e9},
-                 "csr_unit_bytes": {"fp64": unit64, "fp32": unit32}},
+                 "csr_unit_bytes": {"fp64": unit64, "fp32": unit32},
+                 "reference_gpu_fp64_csr": ref_gpu},
         "roofline": {"bound": "hbm",
                      "kernel": f"FP32 SpMV + p.Ap of the inner CG ({st32} layout)",
                      "achieved": gbs32, "peak": peak, "unit": "GB/s", "frac": gbs32 / peak,

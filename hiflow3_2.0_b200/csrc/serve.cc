@@ -20,6 +20,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <memory>
@@ -57,6 +58,8 @@ struct Req {
     int n = 0, fmt = 0, nchunks = 0;
     long long nnz = 0, slen = 0;      // stored entries (SELL: padded)
     long long slen32 = 0;             // stored FP32 entries (mixed; stencil: 32 L per chunk)
+    int half = 0;                     // Q1 Poisson: half stencil layout (full-size storage kept for the fallback)
+    long long hlen64 = 0, hlen32 = 0; // half stencil: FP64 / FP32 values streamed per product
     std::vector<int> sell_off;        // SELL chunk offsets
     size_t bytes = 0, temp_bytes = 0; // resident / admission scratch
     double iter_bytes = 0;            // streamed by one batch iteration
@@ -156,6 +159,12 @@ int plan_request(b200la_server *S, Req *q)
         q->fmt = b200::srv::FMT_STENCIL;
         q->slen = (long long)q->nchunks * b200::srv::kChunk * L;
         q->slen32 = (long long)q->nchunks * b200::srv::kChunk * L;
+        // Poisson operators are symmetric outside their identity rows: half
+        // stencil (checked on the device at admission, full layout otherwise)
+        const char *hv = std::getenv("B200LA_SERVE_HALF");
+        q->half = r.q1_kind == 0 && !(hv && std::atoi(hv) == 0);
+        q->hlen64 = (long long)q->nchunks * b200::srv::kChunk * b200::srv::half_len64(r.q1_dim);
+        q->hlen32 = (long long)q->nchunks * b200::srv::kChunk * b200::srv::half_len32(r.q1_dim);
     }
     int maxlen = 0;
     for (int v : len) maxlen = std::max(maxlen, v);
@@ -189,19 +198,22 @@ int plan_request(b200la_server *S, Req *q)
     const size_t pst = (size_t)((q->nchunks + 1) & ~1);
     const size_t ng = (size_t)((q->nchunks + b200::srv::kGroup - 1) / b200::srv::kGroup), gst = (ng + 1) & ~size_t(1);
     size_t b = offb + colb + al256(8 * (size_t)q->slen) + al256(24 * pst) + al256(24 * gst) + al256(4 * ng);
+    if (stencil) b += al256(4 * (size_t)(q->nchunks + 1));   // identity-row mask and set-up check
     if (mixed) b += al256(4 * (size_t)q->slen32) + 2 * v8 + 7 * v4;
     else b += 8 * v8;
     q->bytes = b;
     q->temp_bytes = al256(4 * (size_t)(n + 1)) + al256(4 * (size_t)q->nnz) + al256(8 * (size_t)q->nnz) +
                     ((!r.row && r.q1_kcell) ? al256(8 * q1_cells(r.q1_dim, r.q1_N)) : 0);
     const double ib = stencil ? 0.0 : 4.0;   // index bytes per stored entry
-    q->iter_bytes = mixed ? 4.0 * q->slen32 + ib * q->slen + 48.0 * n : (8.0 + ib) * q->slen + 96.0 * n;   // vectors: 32n (SpMV) + 64n (update)
+    // values streamed per product (the half layout streams fewer than it stores)
+    const double s64 = q->half ? (double)q->hlen64 : (double)q->slen, s32 = q->half ? (double)q->hlen32 : (double)q->slen32;
+    q->iter_bytes = mixed ? 4.0 * s32 + ib * q->slen + 48.0 * n : (8.0 + ib) * s64 + 96.0 * n;   // vectors: 32n (SpMV) + 64n (update)
     // Jacobi-CG on a Q1 grid needs iterations in proportion to the nodes per line
     q->work = q->iter_bytes * (q->r.q1_N > 0 ? (double)q->r.q1_N : std::sqrt((double)n));
     // per-row costs of the two kernels: operator + gathers and stores (k1),
     // the update's vector traffic (k2); warp-per-row CSR counts double
     const double rows = 32.0 * q->nchunks;
-    const double op = mixed ? (4.0 * q->slen32 + ib * q->slen) / rows : (8.0 + ib) * q->slen / rows;
+    const double op = mixed ? (4.0 * s32 + ib * q->slen) / rows : (8.0 + ib) * s64 / rows;
     const double k1 = (op + (mixed ? 16.0 : 32.0)) * (q->fmt == b200::srv::FMT_CSRW ? 2.0 : 1.0);
     q->w1 = std::max(1, (int)std::lround(k1));
     q->w2 = mixed ? 32 : 64;
@@ -261,6 +273,8 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
         d.sdim = r.q1_dim;
         d.sP = r.q1_N + 1;
         d.sL = r.q1_dim == 3 ? 27 : 9;
+        d.half = q->half;
+        d.smask = reinterpret_cast<unsigned *>(take(4 * (size_t)(q->nchunks + 1)));
     } else {
         d.off = reinterpret_cast<int *>(take(sell ? 4 * (size_t)(q->nchunks + 1) : 4 * (size_t)(n + 1)));
         d.col = reinterpret_cast<int *>(take(4 * (size_t)q->slen));
@@ -308,6 +322,7 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
     if (stencil) {
         SV(cudaMemsetAsync(const_cast<double *>(d.val64), 0, 8 * (size_t)q->slen, st));
         if (mixed) SV(cudaMemsetAsync(const_cast<float *>(d.val32), 0, 4 * (size_t)q->slen32, st));
+        SV(cudaMemsetAsync(const_cast<unsigned *>(d.smask), 0, 4 * (size_t)(q->nchunks + 1), st));
     } else if (sell) {
         SV(cudaMemcpyAsync(const_cast<int *>(d.off), q->sell_off.data(), 4 * (size_t)(q->nchunks + 1),
                            cudaMemcpyHostToDevice, st));
@@ -317,6 +332,18 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
         SV(cudaMemcpyAsync(const_cast<double *>(d.val64), tval, 8 * (size_t)q->nnz, cudaMemcpyDeviceToDevice, st));
     }
     SV(b200::srv::launch_build_slot(d, trow, tcol, tval, st));
+    if (stencil && d.half) {
+        // the half layout needs a_ij == a_ji between rows that are not identity rows
+        unsigned asym = 0;
+        SV(cudaMemcpyAsync(&asym, d.smask + q->nchunks, sizeof asym, cudaMemcpyDeviceToHost, st));
+        SV(cudaStreamSynchronize(st));
+        if (asym) {
+            d.half = 0;
+            SV(cudaMemsetAsync(const_cast<double *>(d.val64), 0, 8 * (size_t)q->slen, st));
+            if (mixed) SV(cudaMemsetAsync(const_cast<float *>(d.val32), 0, 4 * (size_t)q->slen32, st));
+            SV(b200::srv::launch_build_slot(d, trow, tcol, tval, st));
+        }
+    }
     if (r.b) SV(cudaMemcpyAsync(const_cast<double *>(d.b), r.b, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
     else SV(b200::launch_q1_rhs(r.rhs_seed, r.q1_dim, r.q1_N, const_cast<double *>(d.b), st));
     SV(cudaMemsetAsync(vec0, 0, (size_t)(vec1 - vec0), st));

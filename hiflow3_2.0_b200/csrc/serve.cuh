@@ -39,6 +39,12 @@ enum Phase : int { PH_CG_START = 0, PH_CG = 1, PH_OUTER = 2, PH_INNER = 3, PH_CO
 // FP32 values in groups of four positions per lane at
 // val32[128 G c + 128 (k / 4) + 4 lane + k % 4], G = ceil(L / 4).  No column
 // indices or offsets are stored or loaded.
+// Half stencil (FMT_STENCIL with half = 1: Q1 Poisson requests, symmetric
+// outside their identity rows): only the diagonal and the upper half are
+// stored, and a row's lower half is read from the rows that own it (see
+// half_len64 / half_len32); smask[c] bit l flags row 32 c + l as an identity
+// row (no nonzero off-diagonal value), which uses its diagonal alone and
+// keeps in its upper slots the transposed entries its neighbours need.
 enum Fmt : int { FMT_SELL = 0, FMT_CSRW = 1, FMT_STENCIL = 2 };
 
 constexpr int kChunk = 32;          // rows per chunk
@@ -65,6 +71,8 @@ struct SysDesc {
     int pstride;           // chunk partials per quantity (nchunks rounded up to even)
     int sdim, sP, sL;      // FMT_STENCIL: dimension, nodes per line, stencil width
     int ngroups, gstride;  // reduction groups of kGroup chunks; group partials per quantity
+    int half, hpad;        // FMT_STENCIL: half stencil layout (1) or full (0)
+    const unsigned *smask; // half stencil: identity-row mask per chunk [nchunks + 1; the last word: set-up check]
     const int *off;        // SELL: chunk offsets [nchunks + 1]; CSRW: row pointer [n + 1]
     const int *col;
     const double *val64;
@@ -79,6 +87,18 @@ struct SysDesc {
     unsigned *ticket;      // groups completed (0 between launches)
     int *done;             // final status word polled by the host (0 while running)
 };
+
+// Half stencil layout: U = 4 (3-D) or 1 (2-D) bands above the centre band.
+// FP64: per 32-row chunk, half_len64 positions position-major
+// (val64[32 H c + 32 p + lane]): p = 0 the diagonal, p = 1 the +1 entry,
+// p = 2 + 3 u + m position m of upper band U + 1 + u.  FP32: per chunk,
+// half_len32 floats per row: U groups of four (val32[32 H c + 128 u + 4 lane
+// + m]: band U + 1 + u in slots 0-2; slot 3 the diagonal in group 0, the +1
+// entry in group 1, zero above), and when U = 1 the +1 entry alone after the
+// groups (val32[32 H c + 128 U + lane]).
+__host__ __device__ __forceinline__ int half_u(int dim) { return dim == 3 ? 4 : 1; }
+__host__ __device__ __forceinline__ int half_len64(int dim) { return 2 + 3 * half_u(dim); }
+__host__ __device__ __forceinline__ int half_len32(int dim) { return 4 * half_u(dim) + (half_u(dim) < 2 ? 1 : 0); }
 
 // Column offset of stencil position k (column order).
 __host__ __device__ __forceinline__ int stencil_delta(int dim, int P, int k)

@@ -167,6 +167,144 @@ __device__ __forceinline__ float stencil_row(const float *__restrict__ val, int 
     return s;
 }
 
+// Half stencil rows (layout: serve.cuh).  The lower half of row i is read
+// from the rows that own it: (i, i + d + m - 1) of lower band b (centre d)
+// is row (i + d + m - 1)'s entry at position 2 - m of upper band U - 1 - b
+// (mirror bands), and (i, i - 1) is row (i - 1)'s +1 entry.  Those rows'
+// values are streamed by other warps in the same launch, at most a plane of
+// rows away, so the second read is served by L2.  The band values are
+// assembled in the full layout's (band, column) order and added as
+// stencil_row adds them, so a row sums to the same bits.
+template <int NB>
+__device__ __forceinline__ void half_identity(const unsigned *__restrict__ smask, int c, int lane, double (&av)[NB][3])
+{
+    constexpr int U = (NB - 1) / 2;
+    if ((__ldg(smask + c) >> lane) & 1u) {
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+                if (b != U || m != 1) av[b][m] = 0.0;
+    }
+}
+
+template <int NB>
+__device__ __forceinline__ void half_identity(const unsigned *__restrict__ smask, int c, int lane, float (&av)[NB][3])
+{
+    constexpr int U = (NB - 1) / 2;
+    if ((__ldg(smask + c) >> lane) & 1u) {
+#pragma unroll
+        for (int b = 0; b < NB; ++b)
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+                if (b != U || m != 1) av[b][m] = 0.0f;
+    }
+}
+
+template <int NB, typename G>
+__device__ __forceinline__ double stencil_row_half(const double *__restrict__ val, const unsigned *__restrict__ smask,
+                                                   int c, int lane, int n, int P, uint64_t pol, G gather)
+{
+    constexpr int DIM = NB == 9 ? 3 : 2, U = (NB - 1) / 2, H = 2 + 3 * U;
+    const int r0 = c * kChunk, i = r0 + lane, he = lane == 0 ? r0 - 1 : r0 + 32;
+    const double *own = val + (size_t)c * kChunk * H + lane;
+    auto at = [&](int q, int p) {
+        return q >= 0 ? ld_keep(val + ((size_t)(q >> 5) * H + p) * kChunk + (q & 31), pol) : 0.0;
+    };
+    double av[NB][3];
+    av[U][1] = ld_stream(own, pol);
+    av[U][2] = ld_stream(own + 32, pol);
+#pragma unroll
+    for (int ub = 0; ub < U; ++ub)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) av[U + 1 + ub][m] = ld_stream(own + 32 * (2 + 3 * ub + m), pol);
+    av[U][0] = at(i - 1, 1);
+#pragma unroll
+    for (int b = 0; b < U; ++b) {
+        const int q = i + band_offset(DIM, P, b), p = 2 + 3 * (U - 1 - b);
+        av[b][0] = at(q - 1, p + 2);
+        av[b][1] = at(q, p + 1);
+        av[b][2] = at(q + 1, p);
+    }
+    half_identity<NB>(smask, c, lane, av);
+    double s = 0.0;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) band(s, av[b][0], av[b][1], av[b][2], i, he, band_offset(DIM, P, b), n, lane, gather);
+    return s;
+}
+
+__device__ __forceinline__ float4 ld_f4(const float *p, uint64_t pol)
+{
+    float4 q;
+    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+        : "=f"(q.x), "=f"(q.y), "=f"(q.z), "=f"(q.w)
+        : "l"(p), "l"(pol));
+    return q;
+}
+
+template <int NB, typename G>
+__device__ __forceinline__ float stencil_row_half(const float *__restrict__ val, const unsigned *__restrict__ smask,
+                                                  int c, int lane, int n, int P, uint64_t pol, G gather)
+{
+    constexpr int DIM = NB == 9 ? 3 : 2, U = (NB - 1) / 2, H = 4 * U + (U < 2 ? 1 : 0);
+    const int r0 = c * kChunk, i = r0 + lane, he = lane == 0 ? r0 - 1 : r0 + 32, rows = (n + 31) & ~31;
+    const bool edge = lane == 0 || lane == 31;
+    const float *cv = val + (size_t)c * kChunk * H;
+    auto grp = [&](int q, int u) { return val + (size_t)(q >> 5) * kChunk * H + 128 * u + 4 * (q & 31); };
+    auto plus1 = [&](int q) {   // row q's +1 entry
+        return U >= 2 ? ld_f4(grp(q, 1), pol).w : ld_keep(val + (size_t)(q >> 5) * kChunk * H + 128 * U + (q & 31), pol);
+    };
+    float av[NB][3];
+    float4 u[U];
+#pragma unroll
+    for (int g = 0; g < U; ++g) {
+        asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
+            : "=f"(u[g].x), "=f"(u[g].y), "=f"(u[g].z), "=f"(u[g].w)
+            : "l"(cv + 128 * g + 4 * lane), "l"(pol));
+    }
+    const float pl = U >= 2 ? u[U >= 2 ? 1 : 0].w : ld_stream(cv + 128 * U + lane, pol);
+#pragma unroll
+    for (int ub = 0; ub < U; ++ub) {
+        av[U + 1 + ub][0] = u[ub].x;
+        av[U + 1 + ub][1] = u[ub].y;
+        av[U + 1 + ub][2] = u[ub].z;
+    }
+    av[U][1] = u[0].w;
+    av[U][2] = pl;
+    float lm = __shfl_up_sync(0xffffffffu, pl, 1);
+    if (lane == 0) lm = r0 > 0 ? plus1(r0 - 1) : 0.0f;
+    av[U][0] = lm;
+#pragma unroll
+    for (int b = 0; b < U; ++b) {
+        const int d = band_offset(DIM, P, b), ub = U - 1 - b, q = i + d;
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 g = q >= 0 ? ld_f4(grp(q, ub), pol) : z4;
+        const int hq = lane == 0 ? r0 + d - 1 : r0 + 32 + d;
+        const float4 h = (edge && hq >= 0 && hq < rows) ? ld_f4(grp(hq, ub), pol) : z4;
+        float left = __shfl_up_sync(0xffffffffu, g.z, 1);
+        float right = __shfl_down_sync(0xffffffffu, g.x, 1);
+        if (lane == 0) left = h.z;
+        if (lane == 31) right = h.x;
+        av[b][0] = left;
+        av[b][1] = g.y;
+        av[b][2] = right;
+    }
+    half_identity<NB>(smask, c, lane, av);
+    float s = 0.0f;
+#pragma unroll
+    for (int b = 0; b < NB; ++b) band(s, av[b][0], av[b][1], av[b][2], i, he, band_offset(DIM, P, b), n, lane, gather);
+    return s;
+}
+
+// Stencil row of a system, full or half layout.
+template <typename T, int NB, typename G>
+__device__ __forceinline__ T stencil_any(const SysDesc &d, const T *__restrict__ val, int c, int lane, uint64_t pol,
+                                         G gather)
+{
+    if (d.half) return stencil_row_half<NB>(val, d.smask, c, lane, d.n, d.sP, pol, gather);
+    return stencil_row<NB>(val, c, lane, d.n, d.sP, pol, gather);
+}
+
 // SELL and CSRW rows (uploaded CSR requests), out of line.
 template <typename T, typename G>
 __device__ __noinline__ T row_indexed(const SysDesc &d, const T *__restrict__ val, int c, int lane, uint64_t pol,
@@ -203,8 +341,8 @@ __device__ __forceinline__ T row_spmv(const SysDesc &d, const T *__restrict__ va
                                       G gather)
 {
     if (d.fmt == FMT_STENCIL) {
-        if (d.sdim == 3) return stencil_row<9>(val, c, lane, d.n, d.sP, pol, gather);
-        return stencil_row<3>(val, c, lane, d.n, d.sP, pol, gather);
+        if (d.sdim == 3) return stencil_any<T, 9>(d, val, c, lane, pol, gather);
+        return stencil_any<T, 3>(d, val, c, lane, pol, gather);
     }
     return row_indexed<T>(d, val, c, lane, pol, gather);
 }
@@ -357,8 +495,8 @@ __device__ __forceinline__ void k1_range(const WarpCtx &c, SysState *st, const R
         // step keep twice the loads in flight
         for (; ch + R.step < R.c1; ch += 2 * R.step) {
             const int chb = ch + R.step;
-            const T sa = stencil_row<3>(val, ch, lane, n, d.sP, pol, gather);
-            const T sb = stencil_row<3>(val, chb, lane, n, d.sP, pol, gather);
+            const T sa = stencil_any<T, 3>(d, val, ch, lane, pol, gather);
+            const T sb = stencil_any<T, 3>(d, val, chb, lane, pol, gather);
             double da = finish_row(ch, sa), db = finish_row(chb, sb);
             da = warp_sum(da);
             db = warp_sum(db);
@@ -682,7 +820,8 @@ __global__ void build_slot_kernel(SysDesc d, const int *__restrict__ row, const 
         }
         if (d.fmt == FMT_STENCIL) {
             // values zero-filled before; each stored entry to its position
-            if (i < n) {
+            // (the half layout is filled by half_build_slot_kernel)
+            if (i < n && !d.half) {
                 const int c = i / kChunk, lane = i % kChunk, L = d.sL, G4 = L / 4;
                 const size_t base = (size_t)c * kChunk * L + lane;
                 const size_t base32 = (size_t)c * kChunk * L;   // FP32: groups of four, then the tail
@@ -739,6 +878,72 @@ __global__ void build_slot_kernel(SysDesc d, const int *__restrict__ row, const 
     }
 }
 
+// Half stencil, pass 1: smask[c] bit l = row 32 c + l has no off-diagonal
+// value other than +0.0 (rows past n count as such).
+__global__ void half_mask_slot_kernel(SysDesc d, const int *__restrict__ row, const int *__restrict__ col,
+                                      const double *__restrict__ val)
+{
+    unsigned *mask = const_cast<unsigned *>(d.smask);
+    const int rows = d.nchunks * kChunk;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+        bool ident = true;
+        if (i < d.n)
+            for (int j = row[i]; j < row[i + 1]; ++j)
+                if (col[j] != i && __double_as_longlong(val[j]) != 0) ident = false;
+        const unsigned bits = __ballot_sync(0xffffffffu, ident);
+        if ((threadIdx.x & 31) == 0) mask[i >> 5] = bits;
+    }
+}
+
+// Half stencil, pass 2: the diagonal and upper half of every row, FP64 and
+// (mixed) FP32.  An identity row stores in its upper slots the transposed
+// entries (i + off, i) that its neighbours read as their lower half.  Pairs
+// of rows that are not identity rows must hold the same value bit for bit
+// in both directions; otherwise smask[nchunks] is set.
+__global__ void half_build_slot_kernel(SysDesc d, const int *__restrict__ row, const int *__restrict__ col,
+                                       const double *__restrict__ val)
+{
+    const int n = d.n, dim = d.sdim, P = d.sP, U = half_u(dim), H64 = half_len64(dim), H32 = half_len32(dim);
+    const unsigned *mask = d.smask;
+    unsigned *asym = const_cast<unsigned *>(d.smask) + d.nchunks;
+    double *ov = const_cast<double *>(d.val64);
+    float *of = const_cast<float *>(d.val32);
+    auto find = [&](int r, int cc) -> double {
+        for (int j = row[r]; j < row[r + 1]; ++j)
+            if (col[j] == cc) return val[j];
+        return 0.0;
+    };
+    auto flagged = [&](int q) { return (mask[q >> 5] >> (q & 31)) & 1u; };
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const bool fr = flagged(i);
+        auto upper = [&](int off) -> double {
+            const int q = i + off;
+            const bool inr = q < n;
+            if (fr) return inr ? find(q, i) : 0.0;
+            const double v = inr ? find(i, q) : 0.0;
+            if (inr && !flagged(q) && __double_as_longlong(v) != __double_as_longlong(find(q, i))) atomicOr(asym, 1u);
+            return v;
+        };
+        const int c = i / kChunk, lane = i % kChunk;
+        const double dg = find(i, i), p1 = upper(1);
+        double *o64 = ov + (size_t)c * kChunk * H64 + lane;
+        o64[0] = dg;
+        o64[kChunk] = p1;
+        float *o32 = d.mixed ? of + (size_t)c * kChunk * H32 : nullptr;
+        for (int u = 0; u < U; ++u)
+            for (int m = 0; m < 3; ++m) {
+                const double v = upper(band_offset(dim, P, U + 1 + u) + m - 1);
+                o64[kChunk * (2 + 3 * u + m)] = v;
+                if (o32) o32[128 * u + 4 * lane + m] = (float)v;
+            }
+        if (o32) {
+            o32[4 * lane + 3] = (float)dg;
+            if (U >= 2) o32[128 + 4 * lane + 3] = (float)p1;
+            else o32[128 * U + lane] = (float)p1;
+        }
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_round(int nw, int grid, const SysDesc *sys, SysState *state, const int *tab, cudaStream_t st)
@@ -757,6 +962,10 @@ cudaError_t launch_build_slot(const SysDesc &d, const int *row, const int *col, 
 {
     const long long rows = (long long)d.nchunks * kChunk;
     const int g = (int)std::min<long long>((rows + 255) / 256, 148LL * 16);
+    if (d.fmt == FMT_STENCIL && d.half) {
+        half_mask_slot_kernel<<<g, 256, 0, st>>>(d, row, col, val);
+        half_build_slot_kernel<<<g, 256, 0, st>>>(d, row, col, val);
+    }
     build_slot_kernel<<<g, 256, 0, st>>>(d, row, col, val);
     return cudaGetLastError();
 }

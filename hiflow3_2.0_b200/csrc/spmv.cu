@@ -631,6 +631,7 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
         }
         if (r < n) epilogue<T, EPI>(r, s, op, acc);
     }
+    pdl_trigger();
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
         if (grid_reduce<1>(vv, sc.partials, sc.ticket, out)) finalize(op, out[0]);
@@ -784,6 +785,7 @@ __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op,
         }
         if (r < n) epilogue<T, EPI>(r, s, op, acc);
     }
+    pdl_trigger();
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
         if (grid_reduce<1>(vv, sc.partials, sc.ticket, out)) finalize(op, out[0]);
@@ -804,7 +806,7 @@ void launch_one_wave(K kern, int &resident, const Scratch &s, int n_rows, const 
     const int cap = s.num_sms * resident;
     if (grid > cap) grid = cap;
     if (grid < 1) grid = 1;
-    kern<<<grid, kBlock, 0, st>>>(A, op, s);
+    launch_pdl(kern, grid, kBlock, 0, st, A, op, s);
 }
 
 template <typename T, int EPI>
@@ -824,15 +826,12 @@ void launch_epi(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp
             int grid = (chunks + kBlock / 32 - 1) / (kBlock / 32);
             // grid-stride warps in one wave of resident CTAs: a second,
             // partial wave left SMs idle at the end (FP32 128^3: 48.4 -> 45.3 us)
-            auto kern = A.st_nb == 3 ? spmv_stencil_kernel<T, EPI, 3> : spmv_stencil_kernel<T, EPI, 9>;
+            (void)grid;
             static int res_nb[2] = {0, 0};
-            int &resident = res_nb[A.st_nb == 9];
-            if (!resident && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kBlock, 0) != cudaSuccess)
-                resident = 4;
-            const int cap = s.num_sms * resident;
-            if (grid > cap) grid = cap;
-            if (grid < 1) grid = 1;
-            kern<<<grid, kBlock, 0, st>>>(A, op, s);
+            if (A.st_nb == 9)
+                launch_one_wave(spmv_stencil_kernel<T, EPI, 9>, res_nb[1], s, A.n_rows, A, op, st);
+            else
+                launch_one_wave(spmv_stencil_kernel<T, EPI, 3>, res_nb[0], s, A.n_rows, A, op, st);
             return;
         }
     }

@@ -6,6 +6,7 @@ Tolerances: FP64 SpMV 1e-13 relative to the row's magnitude sum_j |a_ij x_j|
 relative in FP64; preconditioner applies 1e-12 relative (the sweeps sum each
 row in a different order than the reference's serial loop).
 """
+import os
 import numpy as np
 import pytest
 
@@ -194,7 +195,7 @@ def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, tma, stencil, di
     assert np.all(np.abs(y32.numpy().astype(np.float64) - y32_ref) <= 2e-6 * sc + 1e-30)
 
 
-@pytest.mark.parametrize("dim,N,coef", [(2, 5, False), (2, 63, True), (3, 3, False), (3, 9, True), (3, 64, True)])
+@pytest.mark.parametrize("dim,N,coef", [(2, 20, False), (2, 63, True), (3, 9, False), (3, 13, True), (3, 64, True)])
 def test_spmv_half_stencil_bitwise(pf, b200, oracle, dim, N, coef, monkeypatch):
     """The half stencil layout (diagonal and upper half; the lower half read
     from the rows that own it) gives y bit for bit equal to the full stencil
@@ -306,3 +307,30 @@ def test_blas1_vs_numpy(pf, b200, oracle, n):
     d32 = pf.vector(xf, b200.F32).Dot(pf.vector(yf, b200.F32))
     np.testing.assert_allclose(d32, np.dot(xf.astype(np.float64), yf.astype(np.float64)), rtol=1e-5,
                                atol=1e-6 * np.sqrt(n))
+
+
+def test_reference_gpu_kernel_baseline(oracle):
+    """The reference's own GPU SpMV (kernel_spmv_csr_scalar, built for sm_100a
+    into baseline/_ref and timed in bench.py beside the platform's kernels)
+    computes y = A x: it is a correct baseline."""
+    import ctypes as C
+    so = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "baseline", "_ref",
+                      "libref_gpu_spmv.so")
+    if not os.path.exists(so):
+        pytest.skip("the reference GPU baseline is built only where the HiFlow3 sources are present")
+    L = C.CDLL(so)
+    row, col, val = oracle.q1_assemble(3, 20, 0, np.exp(np.random.default_rng(2).standard_normal(20 ** 3)))
+    n = len(row) - 1
+    x = np.random.default_rng(3).uniform(-1, 1, n)
+    for dtype, npd in ((0, np.float64), (1, np.float32)):
+        v, xx = val.astype(npd), x.astype(npd)
+        y = np.empty(n, npd)
+        ms = C.c_double()
+        assert L.refgpu_spmv(dtype, n, len(col), C.c_void_p(row.ctypes.data), C.c_void_p(col.ctypes.data),
+                             C.c_void_p(v.ctypes.data), C.c_void_p(xx.ctypes.data), C.c_void_p(y.ctypes.data), 3,
+                             C.byref(ms)) == 0
+        y_ref = oracle.spmv(row, col, v.astype(np.float64), xx.astype(np.float64))
+        sc = row_scale(row, col, v.astype(np.float64), xx.astype(np.float64))
+        tol = 1e-13 if dtype == 0 else 2e-6
+        assert np.all(np.abs(y.astype(np.float64) - y_ref) <= tol * sc + 1e-30)
+        assert ms.value > 0

@@ -135,6 +135,23 @@ def test_serve_alone_vs_mix_bitwise(b200, srv):
         assert r["res"] <= 1e-10 * r["res0"]
 
 
+def test_serve_half_stencil_bitwise(b200, srv, monkeypatch):
+    """Q1 Poisson requests stored as half stencils (diagonal and upper half,
+    the lower half read from the owning rows) solve to the same bits as with
+    the full stencil layout, FP64 and mixed, 2-D and 3-D."""
+    reqs = _mix_requests(b200)[:10]
+    out = {}
+    for half in ("1", "0"):
+        monkeypatch.setenv("B200LA_SERVE_HALF", half)
+        with srv.Server(budget_bytes=2e9, max_slots=32) as s:
+            ids = [s.submit(**r) for r in reqs]
+            out[half] = [s.wait(i) for i in ids]
+    for a, b in zip(out["1"], out["0"]):
+        assert a["status"] in (b200.SUCCESS_ABS, b200.SUCCESS_REL)
+        assert (a["iters"], a["outer"], a["status"], a["res"]) == (b["iters"], b["outer"], b["status"], b["res"])
+        assert np.array_equal(a["x"], b["x"])
+
+
 def test_serve_continuous_admission(b200, srv):
     # a long request is running when short ones arrive: they are admitted into
     # the running batch and finish first
