@@ -456,13 +456,17 @@ static void stencil_plan(b200la_csr *A, const std::vector<int> &uni)
     A->st_nb = L / 3;
 }
 
-// Whether the half stencil layout is built for symmetric stencil operators.
-// B200LA_HALF_STENCIL = 0: never, 1 (default): whenever the operator is
-// symmetric outside its identity rows.
-static bool half_policy()
+// Whether the half stencil layout is built for a symmetric stencil operator
+// of this precision.  B200LA_HALF_STENCIL = 0: never; 1 (default): FP64
+// only; 2: both precisions.  The half layout halves the HBM bytes of the
+// values but not the on-chip ones (each value is read twice from L2): the
+// FP64 product, bound by HBM, gains (128^3: 80.5 -> 73.4 us), the FP32 one,
+// already bound by on-chip latency, loses (45.5 -> 55.5 us).
+static bool half_policy(int dtype)
 {
     const char *e = std::getenv("B200LA_HALF_STENCIL");
-    return !e || std::atoi(e) != 0;
+    const int mode = e ? std::atoi(e) : 1;
+    return mode == 2 || (mode == 1 && dtype == B200LA_F64);
 }
 
 static void free_half(b200la_csr *A)
@@ -480,7 +484,7 @@ static void free_half(b200la_csr *A)
 static int build_half(b200la_ctx *ctx, b200la_csr *A)
 {
     const int nb = A->st_nb;
-    bool ok = half_policy() && A->st_val && (nb == 3 || nb == 9);
+    bool ok = half_policy(A->dtype) && A->st_val && (nb == 3 || nb == 9);
     for (int b = 0; ok && b < nb; ++b)
         if (A->st_union[3 * b + 1] != -A->st_union[3 * (nb - 1 - b) + 1]) ok = false;
     if (!ok) {

@@ -160,20 +160,8 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
 // state has left "iterate").  One thread per CTA reads it (through L2) and
 // broadcasts it: a load by every thread of the grid on one address would
 // serialise in L2.  Must be called by all threads of the CTA.
-// Programmatic dependent launch.  A kernel launched with programmatic stream
-// serialisation may begin while its predecessor in the stream is still
-// running; pdl_wait blocks until the predecessor has completed and its
-// writes are visible (a no-op after an ordinary launch).  pdl_trigger lets
-// the successor begin launching once every CTA of this grid has issued it or
-// exited.
-__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void pdl_trigger() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
-
-// Every kernel that may be launched programmatically calls this first, so
-// that it reads nothing of its predecessor's before the wait.
 __device__ __forceinline__ bool gate_closed(const int *gate)
 {
-    pdl_wait();
     if (!gate) return false;
     __shared__ int s_gate;
     if (threadIdx.x == 0) s_gate = __ldcg(gate);

@@ -9,15 +9,6 @@
 
 namespace b200 {
 
-bool pdl_enabled()
-{
-    static const bool on = [] {
-        const char *e = std::getenv("B200LA_PDL");
-        return e && std::atoi(e) != 0;
-    }();
-    return on;
-}
-
 
 namespace {
 
@@ -176,7 +167,6 @@ __global__ void __launch_bounds__(kBlock) cg_update_kernel(int n, int precond, T
         rr += (double)prr;
         rz += (double)prz;
     }
-    pdl_trigger();
     double v[2] = {rr, rz}, o[2];
     if (grid_reduce<2>(v, sc.partials, sc.ticket, o)) {
         const int it = st->iter + 1;
@@ -222,7 +212,6 @@ __global__ void cg_pupdate_kernel(int n, int precond, T *__restrict__ p, const T
         const T zi = (precond == 1) ? r[i] * invd[i] : (precond == 0 ? r[i] : z[i]);
         p[i] = beta * p[i] + zi;
     }
-    pdl_trigger();
 }
 
 template <typename T>
@@ -385,19 +374,17 @@ cudaError_t launch_cg_update(const Scratch &s, int dtype, int n, int precond, vo
                              const void *Ap, const void *invd, DevState *st, cudaStream_t stm)
 {
     const int g = stream_grid(&s, n);
-    cudaError_t e;
-    B200_DISPATCH(dtype, e = launch_pdl(cg_update_kernel<T>, g, kBlock, 0, stm, n, precond, (T *)x, (T *)r,
-                                        (const T *)p, (const T *)Ap, (const T *)invd, st, s));
-    return e != cudaSuccess ? e : cudaGetLastError();
+    B200_DISPATCH(dtype, cg_update_kernel<T><<<g, kBlock, 0, stm>>>(n, precond, (T *)x, (T *)r, (const T *)p,
+                                                                    (const T *)Ap, (const T *)invd, st, s));
+    return cudaGetLastError();
 }
 
 cudaError_t launch_cg_pupdate(int dtype, int n, int precond, void *p, const void *r, const void *invd, const void *z,
                               DevState *st, cudaStream_t stm)
 {
-    cudaError_t e;
-    B200_DISPATCH(dtype, e = launch_pdl(cg_pupdate_kernel<T>, stream_grid(nullptr, n), kBlock, 0, stm, n, precond,
-                                        (T *)p, (const T *)r, (const T *)invd, (const T *)z, st));
-    return e != cudaSuccess ? e : cudaGetLastError();
+    B200_DISPATCH(dtype, cg_pupdate_kernel<T><<<stream_grid(nullptr, n), kBlock, 0, stm>>>(
+                             n, precond, (T *)p, (const T *)r, (const T *)invd, (const T *)z, st));
+    return cudaGetLastError();
 }
 
 cudaError_t launch_cg_start(const Scratch &s, int dtype, int n, int precond, const void *r, const void *invd,

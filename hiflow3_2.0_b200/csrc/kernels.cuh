@@ -100,26 +100,6 @@ inline size_t half_len(int n, int nb, int dtype)
     return dtype == 1 ? rows * 4 * half_groups(nb) : rows * half_positions(nb);
 }
 
-// Programmatic dependent launch of the Krylov-loop kernels (B200LA_PDL=1):
-// each kernel's launch overlaps its predecessor's tail; the kernels wait
-// (gate_closed) before reading anything upstream.
-bool pdl_enabled();
-template <typename... P, typename... A>
-cudaError_t launch_pdl(void (*k)(P...), int grid, int block, size_t smem, cudaStream_t st, A... args)
-{
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(block);
-    cfg.dynamicSmemBytes = smem;
-    cfg.stream = st;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = at;
-    cfg.numAttrs = pdl_enabled() ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, k, static_cast<P>(args)...);
-}
-
 struct CsrView {
     const int *row;
     const int *col;

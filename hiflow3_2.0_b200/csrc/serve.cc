@@ -160,9 +160,12 @@ int plan_request(b200la_server *S, Req *q)
         q->slen = (long long)q->nchunks * b200::srv::kChunk * L;
         q->slen32 = (long long)q->nchunks * b200::srv::kChunk * L;
         // Poisson operators are symmetric outside their identity rows: half
-        // stencil (checked on the device at admission, full layout otherwise)
+        // stencil (checked on the device at admission, full layout
+        // otherwise).  B200LA_SERVE_HALF = 0: never; 1 (default): FP64
+        // requests; 2: FP64 and mixed requests.
         const char *hv = std::getenv("B200LA_SERVE_HALF");
-        q->half = r.q1_kind == 0 && !(hv && std::atoi(hv) == 0);
+        const int hm = hv ? std::atoi(hv) : 1;
+        q->half = r.q1_kind == 0 && (hm == 2 || (hm == 1 && !mixed));
         q->hlen64 = (long long)q->nchunks * b200::srv::kChunk * b200::srv::half_len64(r.q1_dim);
         q->hlen32 = (long long)q->nchunks * b200::srv::kChunk * b200::srv::half_len32(r.q1_dim);
     }

@@ -631,7 +631,6 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
         }
         if (r < n) epilogue<T, EPI>(r, s, op, acc);
     }
-    pdl_trigger();
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
         if (grid_reduce<1>(vv, sc.partials, sc.ticket, out)) finalize(op, out[0]);
@@ -785,7 +784,6 @@ __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op,
         }
         if (r < n) epilogue<T, EPI>(r, s, op, acc);
     }
-    pdl_trigger();
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
         if (grid_reduce<1>(vv, sc.partials, sc.ticket, out)) finalize(op, out[0]);
@@ -806,7 +804,7 @@ void launch_one_wave(K kern, int &resident, const Scratch &s, int n_rows, const 
     const int cap = s.num_sms * resident;
     if (grid > cap) grid = cap;
     if (grid < 1) grid = 1;
-    launch_pdl(kern, grid, kBlock, 0, st, A, op, s);
+    kern<<<grid, kBlock, 0, st>>>(A, op, s);
 }
 
 template <typename T, int EPI>

@@ -187,7 +187,7 @@ def test_spmv_pattern_dictionary(pf, b200, oracle, mode, stage, tma, stencil, di
     A.VectorMult(pf.vector(x), yv)
     assert spmv_ok(yv.numpy(), y_ref, sc, 1e-13)
     A32 = A.CastFrom(b200.F32)
-    assert A32.info()["storage"] == want
+    assert A32.info()["storage"] == ("stencil" if want == "half-stencil" else want)
     x32 = x.astype(np.float32)
     y32 = pf.vector(n, b200.F32)
     A32.VectorMult(pf.vector(x32, b200.F32), y32)
@@ -208,11 +208,11 @@ def test_spmv_half_stencil_bitwise(pf, b200, oracle, dim, N, coef, monkeypatch):
     n = len(row) - 1
     x, y0, b = rng.uniform(-1, 1, n), rng.uniform(-1, 1, n), rng.uniform(-1, 1, n)
     outs = {}
-    for half in ("1", "0"):
+    for half in ("2", "0"):
         monkeypatch.setenv("B200LA_HALF_STENCIL", half)
         A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
         A32 = A.CastFrom(b200.F32)
-        assert A.info()["storage"] == A32.info()["storage"] == ("half-stencil" if half == "1" else "stencil")
+        assert A.info()["storage"] == A32.info()["storage"] == ("half-stencil" if half == "2" else "stencil")
         res = []
         for M, dt in ((A, b200.F64), (A32, b200.F32)):
             cast = (lambda v: v) if dt == b200.F64 else (lambda v: v.astype(np.float32))
@@ -227,9 +227,19 @@ def test_spmv_half_stencil_bitwise(pf, b200, oracle, dim, N, coef, monkeypatch):
             res.append(np.array([M.Residual(pf.vector(cast(b), dt), xv, rv)]))
             res.append(rv.numpy())
         outs[half] = res
-    for a, c in zip(outs["1"], outs["0"]):
-        assert np.array_equal(a.view(np.uint8), c.view(np.uint8))
-    assert spmv_ok(outs["1"][0], oracle.spmv(row, col, val, x), row_scale(row, col, val, x), 1e-13)
+    # vectors bit for bit; the fused reductions (x.y, ||r||^2) sum the same
+    # products over a grid sized by each kernel's occupancy, so their order
+    # of summation, and possibly their last bit, differ
+    for k, (a, c) in enumerate(zip(outs["2"], outs["0"])):
+        if k % 5 in (2, 3):
+            np.testing.assert_allclose(a, c, rtol=1e-13)
+        else:
+            assert np.array_equal(a.view(np.uint8), c.view(np.uint8)), k
+    assert spmv_ok(outs["2"][0], oracle.spmv(row, col, val, x), row_scale(row, col, val, x), 1e-13)
+    # the default: FP64 operators take the half layout, FP32 ones the full one
+    monkeypatch.delenv("B200LA_HALF_STENCIL")
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    assert A.info()["storage"] == "half-stencil" and A.CastFrom(b200.F32).info()["storage"] == "stencil"
 
 
 def test_spmv_half_stencil_rejects_asymmetry(pf, b200, oracle):

@@ -6,8 +6,6 @@ reach the same relative residual within +-5% of the reference's iteration
 count (the counts usually coincide); solutions within 1e-8 relative of the
 reference's.
 """
-import os
-
 import numpy as np
 import pytest
 
@@ -340,42 +338,3 @@ def test_ilu0_level_sweep_beyond_ring(pf, b200, dim, N, kind, monkeypatch):
     for sweep in ("cta", "staged"):
         assert np.max(np.abs(out[sweep] - out["tickets"])) <= 1e-11 * np.max(np.abs(out["tickets"]))
 
-
-def test_programmatic_launch_changes_no_bits(b200):
-    """With B200LA_PDL=1 the Krylov-loop kernels are launched with
-    programmatic stream serialisation (each launch overlaps its predecessor's
-    tail, the kernel waits before reading upstream results): the CG and MPIR
-    solves give the same iterations and the same bits as ordinary launches.
-    Each run is a fresh process, since the switch is read once."""
-    import json
-    import subprocess
-    import sys
-    code = r'''
-import json, sys, numpy as np
-sys.path.insert(0, "tests")
-from conftest import load_platform
-b200 = load_platform()
-pf = b200.Platform(0)
-kc = np.exp(np.random.default_rng(3).standard_normal(20 ** 3))
-row, col, val = b200.q1_assemble(3, 20, 0, kc)
-b = b200.q1_rhs(7, 3, 20)
-A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
-cg = b200.CG(pf); cg.SetupOperator(A); cg.SetupPreconditioner(b200.Preconditioner.Jacobi(pf, A))
-cg.InitControl(10000, 0.0, 1e-10, 1e6)
-x = pf.vector(len(b)); cg.Solve(pf.vector(b), x)
-mp = b200.MPIR(pf); mp.SetupOperator(A); mp.SetupLowPrecisionOperator(A.CastFrom(b200.F32))
-mp.InitControl(50, 0.0, 1e-10, 1e6); mp.InitInnerControl(10000, 0.0, 1e-4, 1e6)
-xm = pf.vector(len(b)); mp.Solve(pf.vector(b), xm)
-print(json.dumps(dict(it=cg.iter(), x=x.numpy().view(np.uint64).tolist()[:4000:7],
-                      xsum=float(np.sum(x.numpy())), mo=mp.result.outer, mi=mp.result.iters,
-                      xm=xm.numpy().view(np.uint64).tolist()[:4000:7])))
-'''
-    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-    out = {}
-    for pdl in ("0", "1"):
-        env = dict(os.environ, B200LA_PDL=pdl)
-        p = subprocess.run([sys.executable, "-c", code], capture_output=True, text=True, env=env, cwd=root,
-                           timeout=600)
-        assert p.returncode == 0, p.stderr[-2000:]
-        out[pdl] = json.loads(p.stdout.strip().splitlines()[-1])
-    assert out["0"] == out["1"]
