@@ -146,6 +146,17 @@ def lib():
         "b200la_vec_add_values": ([_P, _I, _I, _P, _I, _P, _P], _I),
         "b200la_spmv_add_remote": ([_P, _P, _P, _P, _P, _P], _I),
         "b200la_enable_peer_access": ([_I, _I], _I),
+        "b200la_comm_unique_id": ([_P], _I),
+        "b200la_comm_create_nccl": ([_P, _P, _I, _I, _P], _I),
+        "b200la_comm_create_local": ([_I, _P], _I),
+        "b200la_comm_info": ([_P, C.POINTER(_I), C.POINTER(_I)], _I),
+        "b200la_comm_destroy": ([_P], _I),
+        "b200la_coupled_create": ([_P, _P, _P, _P, _P, _P, _P, _P], _I),
+        "b200la_coupled_destroy": ([_P], _I),
+        "b200la_coupled_update_ghost": ([_P, _P, _P, _P], _I),
+        "b200la_coupled_spmv": ([_P, _P, _P, _P], _I),
+        "b200la_coupled_dot": ([_P, _P, _P, _P, C.POINTER(_D)], _I),
+        "b200la_coupled_cg": ([_P, _P, _P, _P, _P, C.POINTER(Control), C.POINTER(Result)], _I),
         "b200la_vec_set_values": ([_P, _I, _I, _P, _I, _P, _P], _I),
         "b200la_csr_diag": ([_P, _P, _I, _I, _I, _P], _I),
         "b200la_csr_extract_submatrix": ([_P, _P, _I, _I, _I, _I, C.POINTER(_P)], _I),
@@ -745,7 +756,7 @@ class CSR_lMatrix:
         npat, uses = C.c_int(), C.c_int()
         self.pf.check(lib().b200la_csr_format(self.h, C.byref(npat), C.byref(uses)))
         out["row_patterns"], out["uses_pattern_dictionary"] = npat.value, bool(uses.value)
-        out["storage"] = {0: "csr", 1: "dictionary", 2: "stencil", 3: "half-stencil"}[uses.value]
+        out["storage"] = {0: "csr", 1: "dictionary", 2: "stencil", 3: "half-stencil", 4: "lattice"}[uses.value]
         return out
 
     def CastFrom(self, dtype):

@@ -38,7 +38,7 @@ from . import CSR_lMatrix, F64, B200Error, Control, Result, lib, rowblock_split
 
 __all__ = ["RowPartition", "LaCouplings", "DistTransport", "LocalTransport", "CoupledVector", "CoupledMatrix",
            "BlockPrecond", "CoupledCG", "CoupledGMRES", "CoupledMPIR", "CoupledAsyncJacobi", "exchange",
-           "exchange_async"]
+           "exchange_async", "Comm", "NativeCoupledMatrix"]
 
 
 class RowPartition:
@@ -721,3 +721,130 @@ class CoupledAsyncJacobi:
             status = check(ctl, it, res, self.res0)
         self.iter, self.res = it, res
         return status
+
+
+# ------------------------------------------------------------ native coupled layer (C ABI)
+
+COMM_ID_BYTES = 128
+
+
+class Comm:
+    """A b200la_comm: the communicator of the native coupled layer.
+
+    ``Comm.local_group(size)`` -- communicators for ranks that are threads of
+    this process (device copies ordered by events, a host barrier);
+    ``Comm.nccl(platform, uid, rank, size)`` -- an NCCL communicator of this
+    rank on the platform's GPU, ``uid`` from ``Comm.unique_id()`` on rank 0,
+    handed to every rank by the caller (a torch.distributed broadcast, MPI)."""
+
+    def __init__(self, handle):
+        self.h = handle
+        r, n = C.c_int(), C.c_int()
+        lib().b200la_comm_info(self.h, C.byref(r), C.byref(n))
+        self.rank, self.size = r.value, n.value
+
+    @staticmethod
+    def unique_id():
+        buf = (C.c_char * COMM_ID_BYTES)()
+        rc = lib().b200la_comm_unique_id(buf)
+        if rc:
+            raise B200Error(rc, "comm_unique_id: NCCL could not be loaded")
+        return bytes(buf)
+
+    @classmethod
+    def nccl(cls, platform, uid, rank, size):
+        buf = (C.c_char * COMM_ID_BYTES).from_buffer_copy(uid)
+        h = C.c_void_p()
+        platform.check(lib().b200la_comm_create_nccl(platform.h, buf, rank, size, C.byref(h)), "comm_create_nccl")
+        return cls(h)
+
+    @classmethod
+    def local_group(cls, size):
+        arr = (C.c_void_p * size)()
+        rc = lib().b200la_comm_create_local(size, arr)
+        if rc:
+            raise B200Error(rc, "comm_create_local")
+        return [cls(C.c_void_p(arr[q])) for q in range(size)]
+
+    def close(self):
+        if self.h:
+            lib().b200la_comm_destroy(self.h)
+            self.h = None
+
+
+class NativeCoupledMatrix:
+    """CoupledMatrix on the C ABI (b200la_coupled_*): the couplings are set up
+    on the host once through ``transport`` (the index lists every peer needs,
+    as LaCouplings::InitializeCouplings does with MPI), and the data path --
+    border gather, ghost exchange overlapping the diagonal-block product,
+    off-diagonal product, cross-rank sums, the coupled CG -- runs in the
+    library over ``comm``."""
+
+    def __init__(self, platform, comm, transport, partition, rank, row, col, val, dtype=F64):
+        n_global = int(partition.offsets[-1])
+        r0, r1 = partition.range(rank)
+        (rd, cd, vd), (ro, co, vo), ghosts = rowblock_split(row, col, val, n_global, r0, r1)
+        self.pf, self.comm, self.rank, self.dtype = platform, comm, rank, dtype
+        self.couplings = LaCouplings(partition, rank, ghosts).setup(transport)
+        self.n_local = r1 - r0
+        self.diag = CSR_lMatrix.from_csr(platform, rd, cd, vd, n_cols=self.n_local, dtype=dtype)
+        self.offdiag = (CSR_lMatrix.from_csr(platform, ro, co, vo, n_cols=len(ghosts), dtype=dtype)
+                        if len(co) else None)
+        cp = self.couplings
+        self._go = np.ascontiguousarray(cp.ghost_offsets, np.int32)
+        self._bo = np.ascontiguousarray(cp.border_offsets, np.int32)
+        self._bi = np.ascontiguousarray(cp.border_indices, np.int32)
+        h = C.c_void_p()
+        platform.check(lib().b200la_coupled_create(platform.h, comm.h, self.diag.h,
+                                                   self.offdiag.h if self.offdiag is not None else None,
+                                                   self._go.ctypes.data, self._bo.ctypes.data,
+                                                   self._bi.ctypes.data if self._bi.size else None, C.byref(h)),
+                       "coupled_create")
+        self.h = h
+        self.iter, self.res, self.res0, self.status = 0, 0.0, 0.0, 0
+
+    def vector(self, data_or_n=None):
+        return self.pf.vector(self.n_local if data_or_n is None else data_or_n, self.dtype)
+
+    def UpdateGhost(self, x):
+        """The ghost values of x (CoupledVector::UpdateGhost), as a host array."""
+        import torch
+        g = torch.zeros(len(self.couplings.ghost_global),
+                        dtype=torch.float64 if self.dtype == F64 else torch.float32, device=f"cuda:{self.pf.device}")
+        self.pf.check(lib().b200la_coupled_update_ghost(self.pf.h, self.h, x.ptr,
+                                                        C.c_void_p(g.data_ptr()) if g.numel() else None),
+                      "coupled_update_ghost")
+        return g.cpu().numpy()
+
+    def VectorMult(self, x, y):
+        self.pf.check(lib().b200la_coupled_spmv(self.pf.h, self.h, x.ptr, y.ptr), "coupled_spmv")
+
+    def Dot(self, x, y):
+        out = C.c_double()
+        self.pf.check(lib().b200la_coupled_dot(self.pf.h, self.h, x.ptr, y.ptr, C.byref(out)), "coupled_dot")
+        return out.value
+
+    def CG(self, b, x, precond=None, maxits=100000, abstol=0.0, reltol=1e-10, divtol=1e6):
+        """CG<LAD>::Solve over the coupled rows; precond None or "jacobi"
+        (the Jacobi preconditioner of this rank's diagonal block)."""
+        P = None
+        if precond == "jacobi":
+            from . import Preconditioner
+            P = Preconditioner.Jacobi(self.pf, self.diag)
+        ctl, res = Control(maxits, abstol, reltol, divtol), Result()
+        self.pf.check(lib().b200la_coupled_cg(self.pf.h, self.h, P.h if P is not None else None, b.ptr, x.ptr,
+                                              C.byref(ctl), C.byref(res)), "coupled_cg")
+        self.iter, self.res, self.res0, self.status = res.iters, res.res, res.res0, res.status
+        return res.status
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.pf.sync()
+            lib().b200la_coupled_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -89,6 +89,9 @@ struct b200la_csr {
     void *sh_val = nullptr;
     unsigned *sh_mask = nullptr;
     int sh_use = 0;                   // SpMV runs on it instead of the full layout
+    // lattice layout (multicoloured structured Q1 operators): see kernels.cuh
+    void *lt_val = nullptr;
+    b200::LatticeDesc *lt = nullptr;
 };
 
 struct b200la_precond {
@@ -117,6 +120,7 @@ int ctx_work(b200la_ctx *ctx, size_t bytes, void **out);
 int ctx_work_outer(b200la_ctx *ctx, size_t bytes, void **out);
 int ctx_check_device_error(b200la_ctx *ctx);
 int spmv_run(b200la_ctx *ctx, const b200la_csr *A, const b200::Seg &seg, b200::SpmvOp op);
+bool spmv_can_fold(const b200la_csr *A);
 int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row, const int *col, const void *val,
                int dtype, int n_seg, const int *seg_off, b200la_csr **out);
 // precond.cu
@@ -126,6 +130,17 @@ int syncfree_apply(b200la_ctx *ctx, const b200la_precond *P, const void *r, void
 void syncfree_free(b200la_precond *P);
 // solvers.cu
 void graph_cache_clear(b200la_ctx *ctx);
+// lattice.cu
+namespace lattice {
+bool grid(int n, const int *row, const int *col, int *mx, int *my, int *mz);
+bool perm_ok(int mx, int my, int mz, const std::vector<int> &perm, const std::vector<int> &off);
+bool values(int mx, int my, int mz, const b200::host::Csr &M, int part, b200::LatticeDesc &d,
+            std::vector<double> &out);
+}  // namespace lattice
+int lattice_attach(b200la_ctx *ctx, b200la_csr *A, const b200::host::Csr &Mh, int mx, int my, int mz, int part);
+bool lattice_segment(const b200la_csr *A, const b200::Seg &seg, int *c0, int *c1);
+void lattice_free(b200la_csr *A);
+int lattice_refresh(b200la_ctx *ctx, b200la_csr *A);
 
 namespace b200 {
 cudaError_t sweeps_configure();

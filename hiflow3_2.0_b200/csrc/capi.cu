@@ -254,6 +254,7 @@ extern "C" const char *b200la_status_string(int s)
     case B200LA_PENDING: return "request pending";
     case B200LA_ERR_IO: return "file I/O failed";
     case B200LA_ERR_FORMAT: return "unsupported or malformed file";
+    case B200LA_ERR_COMM: return "communicator failed";
     default: return "unknown status";
     }
 }
@@ -723,6 +724,7 @@ extern "C" int b200la_csr_destroy(b200la_csr *A)
     if (A->sell_val) cudaFree(A->sell_val);
     if (A->st_val) cudaFree(A->st_val);
     free_half(A);
+    lattice_free(A);
     delete A;
     return B200LA_OK;
 }
@@ -749,6 +751,8 @@ extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, 
     B->sh_val = nullptr;
     B->sh_mask = nullptr;
     B->sh_use = 0;
+    B->lt_val = nullptr;   // the lattice layout stays with A (built by the preconditioners)
+    B->lt = nullptr;
     const size_t pad = 8, es = dsize(dtype);
     cudaError_t e;
     if (A->pid) {
@@ -819,7 +823,9 @@ extern "C" int b200la_csr_format(const b200la_csr *A, int *npat, int *uses_dict)
     if (!A) return B200LA_ERR_ARG;
     if (npat) *npat = A->pid ? A->npat : 0;
     if (uses_dict)
-        *uses_dict = (A->st_use && A->sh_use && A->sh_val) ? 3 : (A->st_use && A->st_val) ? 2
+        *uses_dict = (A->lt && A->lt_val)                     ? 4
+                     : (A->st_use && A->sh_use && A->sh_val) ? 3
+                     : (A->st_use && A->st_val)              ? 2
                                                                  : (A->pid && A->use_pat) ? 1 : 0;
     return B200LA_OK;
 }
@@ -840,8 +846,9 @@ extern "C" int b200la_csr_set_values(b200la_ctx *ctx, b200la_csr *A, const void 
     if (!ctx || !A || (A->nnz && !val)) return B200LA_ERR_ARG;
     if (A->nnz) CK(cudaMemcpyAsync(A->val, val, dsize(A->dtype) * A->nnz, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    const int rc = build_sell(ctx, A);
-    return rc ? rc : build_stencil(ctx, A);
+    int rc = build_sell(ctx, A);
+    if (!rc) rc = build_stencil(ctx, A);
+    return rc ? rc : lattice_refresh(ctx, A);
 }
 
 extern "C" int b200la_csr_scale(b200la_ctx *ctx, b200la_csr *A, double alpha, int mode)
@@ -851,8 +858,9 @@ extern "C" int b200la_csr_scale(b200la_ctx *ctx, b200la_csr *A, double alpha, in
     if (A->nnz) CK(launch_csr_scale(A->dtype, A->n, A->row, A->col, A->val, alpha, mode, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     // the SpMV layouts derived from the values follow them
-    const int rc = build_sell(ctx, A);
-    return rc ? rc : build_stencil(ctx, A);
+    int rc = build_sell(ctx, A);
+    if (!rc) rc = build_stencil(ctx, A);
+    return rc ? rc : lattice_refresh(ctx, A);
 }
 
 extern "C" int b200la_csr_diag(b200la_ctx *ctx, const b200la_csr *A, int start, int end, int inverse, void *out)
@@ -931,8 +939,21 @@ extern "C" int b200la_csr_invdiag(b200la_ctx *ctx, const b200la_csr *A, void *ou
 
 // ------------------------------------------------------------------- SpMV
 
+// Whether the SpMV of A can fold the Jacobi-CG direction update into its
+// gathers (SpmvOp::fold_p): A's product runs on a stencil layout.
+bool spmv_can_fold(const b200la_csr *A)
+{
+    return A && !A->lt && A->st_use && A->st_val && (A->st_nb == 3 || A->st_nb == 9) && A->n == A->m;
+}
+
 int spmv_run(b200la_ctx *ctx, const b200la_csr *A, const Seg &seg, SpmvOp op)
 {
+    int c0, c1;
+    if (lattice_segment(A, seg, &c0, &c1)) {
+        CK(launch_lattice(ctx_scratch(ctx), A->dtype, *A->lt, A->lt_val, c0, c1, op, ctx->stream));
+        ctx->launches += 1;
+        return B200LA_OK;
+    }
     CK(launch_spmv(ctx_scratch(ctx), csr_view(A), seg, op, ctx->stream));
     ctx->launches += 1;
     return B200LA_OK;

@@ -205,11 +205,15 @@ __global__ void cg_pupdate_kernel(int n, int precond, T *__restrict__ p, const T
         T *pe = reinterpret_cast<T *>(&pv);
         const T *re = reinterpret_cast<const T *>(&rv), *de = reinterpret_cast<const T *>(&dv);
 #pragma unroll
-        for (int k = 0; k < W; ++k) pe[k] = beta * pe[k] + (precond == 1 ? re[k] * de[k] : re[k]);
+        for (int k = 0; k < W; ++k) pe[k] = precond == 1 ? cg_direction(beta, pe[k], re[k], de[k]) : beta * pe[k] + re[k];
         reinterpret_cast<V *>(p)[iv] = pv;
     }
     for (int i = nv * W + tid; i < n; i += stride) {
-        const T zi = (precond == 1) ? r[i] * invd[i] : (precond == 0 ? r[i] : z[i]);
+        if (precond == 1) {
+            p[i] = cg_direction(beta, p[i], r[i], invd[i]);
+            continue;
+        }
+        const T zi = precond == 0 ? r[i] : z[i];
         p[i] = beta * p[i] + zi;
     }
 }

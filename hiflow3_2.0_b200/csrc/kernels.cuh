@@ -43,6 +43,18 @@ __device__ __forceinline__ int check_state(DevState *st, int step, double value)
     if (step >= st->maxits) return kFailMaxits;
     return kIterate;
 }
+// The Jacobi-CG direction p_new = beta p + z with z = r d (cg.cc:241 and
+// lpreconditioner.cc:127-165): one rounding of r d, then one fused
+// multiply-add -- the same bits wherever it is formed (the direction update
+// kernel, or the SpMV that folds it into its gathers).
+__device__ __forceinline__ double cg_direction(double beta, double p, double r, double d)
+{
+    return fma(beta, p, __dmul_rn(r, d));
+}
+__device__ __forceinline__ float cg_direction(float beta, float p, float r, float d)
+{
+    return fmaf(beta, p, __fmul_rn(r, d));
+}
 #endif
 
 // SpMV kernel variants (chosen per matrix when it is created):
@@ -145,6 +157,39 @@ struct CsrView {
     int sh_use;
 };
 
+// Lattice layout of an operator in the multicolour numbering of a structured
+// Q1 node grid (mx x my x mz nodes, lexicographic, x fastest), coloured by
+// node parity -- colour c = px + 2 py + 4 pz holds the nodes whose coordinate
+// parities are (px, py, pz), in lexicographic order.  This is the colouring
+// and permutation the greedy multicolouring gives on such a grid.  Row t of
+// colour c is node (2 xs + px, 2 ys + py, 2 zs + pz) with t = (zs ny + ys) nx
+// + xs, and its neighbour at (dx, dy, dz) sits in colour c ^ (|dx| + 2|dy| +
+// 4|dz|) at a row computed the same way, so no index is stored: a colour
+// keeps, per 32-row chunk, the values of its nslot neighbour positions
+// k-major (slot k of all 32 rows together), zero where a row lacks the
+// neighbour.  Slots are ordered by (neighbour colour, dz, dy, dx), which is
+// the row's ascending column order in the coloured numbering.
+constexpr int kLatMaxColours = 8;
+constexpr int kLatMaxSlots = 27;
+struct LatticeColour {
+    int row0, rows;          // rows [row0, row0 + rows) of the coloured numbering
+    int nx, ny;              // sublattice extents in x and y
+    int px, py, pz;          // coordinate parities of the colour
+    int nslot;               // stored positions per row
+    int chunk0;              // first chunk of the colour (chunks of all colours numbered together)
+    int pad;
+    long long val0;          // offset of the colour's values (elements)
+    // slot k: (dx + 1) | (dy + 1) << 2 | (dz + 1) << 4 | neighbour colour << 8
+    unsigned slot[kLatMaxSlots];
+};
+struct LatticeDesc {
+    int ncol, mx, my, mz;    // colours (4 in 2-D, 8 in 3-D) and node extents (mz = 1 in 2-D)
+    int chunks;              // chunks of all colours
+    int part;                // 0 strictly lower, 1 strictly upper, 2 whole operator
+    int pad[2];
+    LatticeColour col[kLatMaxColours];
+};
+
 constexpr int kMaxPatterns = 1024;
 constexpr int kMaxPatternDeltas = 6144;
 constexpr int kMaxGatherLines = 64;
@@ -161,6 +206,15 @@ struct SpmvOp {
     double *dot_out = nullptr;
     DevState *st = nullptr;
     const int *gate = nullptr;    // skip the launch body when *gate != 0
+    // Jacobi-CG direction folded into the product (EPI_DOT_X on the stencil
+    // layouts only, see spmv_can_fold): x holds the previous direction p, and
+    // every gathered column j uses p_new[j] = beta p[j] + r[j] d[j]
+    // (cg_direction, beta = *fold_beta); the row's own p_new goes to fold_p
+    // and into the dot.  Replaces the separate direction update of the loop.
+    void *fold_p = nullptr;
+    const void *fold_r = nullptr;
+    const void *fold_d = nullptr;
+    const double *fold_beta = nullptr;
 };
 
 struct Scratch {
@@ -186,6 +240,10 @@ cudaError_t launch_csr_to_stencil(int dtype, int n, const int *row, const int *c
 cudaError_t launch_stencil_to_half(int dtype, int n, int nb, const int *center, const void *st_val, void *sh_val,
                                    unsigned *sh_mask, int *asym, cudaStream_t st);
 cudaError_t launch_spmv(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st);
+// Lattice-layout SpMV / colour sweep over colours [c0, c1): y by the epilogue
+// of op (EPI_SET, EPI_ADD, EPI_DOT_X, EPI_RESID, EPI_SGS_F/B, EPI_ILU_F/B).
+cudaError_t launch_lattice(const Scratch &s, int dtype, const LatticeDesc &d, const void *val, int c0, int c1,
+                           const SpmvOp &op, cudaStream_t st);
 
 // ---- BLAS1 (dtype 0 double, 1 float; scalars in double) ----
 cudaError_t launch_dot(const Scratch &s, int dtype, int n, const void *x, const void *y, double *out,

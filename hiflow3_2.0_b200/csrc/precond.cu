@@ -196,6 +196,22 @@ static int build_block(b200la_ctx *ctx, int kind, int n, const int *row, const i
             return rc;
         }
     }
+    // a parity-coloured structured Q1 grid: index-free lattice layouts of the
+    // sweeps' two parts and of the coloured operator (the CSR stays for
+    // everything else, and is used alone when any entry does not fit)
+    int mx, my, mz;
+    if (kind != B200LA_PRECOND_ILU0_LS && lattice::grid(n, row, col, &mx, &my, &mz) &&
+        lattice::perm_ok(mx, my, mz, perm, off)) {
+        if ((rc = lattice_attach(ctx, P->L, L, mx, my, mz, 0)) || (rc = lattice_attach(ctx, P->U, U, mx, my, mz, 1)) ||
+            (A_perm && (rc = lattice_attach(ctx, *A_perm, Ap, mx, my, mz, 2)))) {
+            if (A_perm) {
+                b200la_csr_destroy(*A_perm);
+                *A_perm = nullptr;
+            }
+            b200la_precond_destroy(P);
+            return rc;
+        }
+    }
     *out = P;
     return B200LA_OK;
 }

@@ -18,6 +18,7 @@
 // and its norm, and the multicolour Gauss-Seidel / ILU sweep updates.
 #include "common.cuh"
 #include "kernels.cuh"
+#include "spmv_epi.cuh"
 
 #include <cmath>
 
@@ -35,59 +36,6 @@ struct TileSmem {
     __host__ __device__ static constexpr int stage_bytes() { return val_bytes<T>() + col_bytes() + row_bytes(); }
 };
 
-__device__ __forceinline__ void finalize(const SpmvOp &op, double v)
-{
-    DevState *st = op.st;
-    switch (op.fin) {
-    case FIN_STORE: *op.dot_out = v; break;
-    case FIN_CG_ALPHA:
-        st->pap = v;
-        st->alpha = st->rho / v;
-        break;
-    case FIN_RES_INIT: {
-        st->rr = v;
-        const double res = sqrt(v);
-        st->res = res;
-        st->iter = 0;
-        if (st->hist && st->hist_len > 0) st->hist[0] = res;
-        st->status = check_state(st, 0, res);
-        break;
-    }
-    default: break;
-    }
-}
-
-template <typename T, int EPI>
-__device__ __forceinline__ void epilogue(int r, T s, const SpmvOp &op, double &acc)
-{
-    T *y = static_cast<T *>(op.y);
-    if constexpr (EPI == EPI_SET) {
-        y[r] = s;
-    } else if constexpr (EPI == EPI_ADD) {
-        y[r] += s;
-    } else if constexpr (EPI == EPI_DOT_X) {
-        y[r] = s;
-        acc += (double)(__ldg(static_cast<const T *>(op.x) + r) * s);
-    } else if constexpr (EPI == EPI_RESID) {
-        const T v = static_cast<const T *>(op.b)[r] - s;
-        y[r] = v;
-        acc += (double)(v * v);
-    } else if constexpr (EPI == EPI_SGS_F) {
-        y[r] = (-static_cast<const T *>(op.b)[r] + s) * static_cast<const T *>(op.d1)[r];
-    } else if constexpr (EPI == EPI_SGS_B) {
-        y[r] = (y[r] * static_cast<const T *>(op.d2)[r] + s) * static_cast<const T *>(op.d1)[r];
-    } else if constexpr (EPI == EPI_ILU_F) {
-        y[r] = -(-static_cast<const T *>(op.b)[r] + s);
-    } else if constexpr (EPI == EPI_ILU_B) {
-        y[r] = (-y[r] + s) * static_cast<const T *>(op.d1)[r];
-    }
-}
-
-template <int EPI>
-constexpr bool reduces()
-{
-    return EPI == EPI_DOT_X || EPI == EPI_RESID;
-}
 
 // Rows too long for a tile: one warp per row straight from global memory.
 template <typename T, int EPI>
@@ -529,6 +477,24 @@ void launch_tile(int grid, const CsrView &A, const Seg &seg, const SpmvOp &op, c
         <<<grid, kBlock, ST * TileSmem<CAP>::template stage_bytes<T>() + ST * 8, st>>>(A, seg, op, s);
 }
 
+// Row epilogue of the stencil kernels; with FOLD (EPI_DOT_X only) the row's
+// own new direction is formed from the same inputs as at every gather, stored,
+// and used in the dot: y_i = s, p_new_i = beta p_i + r_i d_i, acc += p_new_i s.
+template <typename T, int EPI, bool FOLD>
+__device__ __forceinline__ void fold_epilogue(int r, T s, const SpmvOp &op, T beta, double &acc)
+{
+    if constexpr (FOLD) {
+        static_assert(EPI == EPI_DOT_X, "the direction fold goes with the p.Ap epilogue");
+        const T pn = cg_direction(beta, static_cast<const T *>(op.x)[r], static_cast<const T *>(op.fold_r)[r],
+                                  static_cast<const T *>(op.fold_d)[r]);
+        static_cast<T *>(op.fold_p)[r] = pn;
+        static_cast<T *>(op.y)[r] = s;
+        acc += (double)(pn * s);
+    } else {
+        epilogue<T, EPI>(r, s, op, acc);
+    }
+}
+
 template <typename T, int W>
 struct StencilVec;
 template <>
@@ -560,10 +526,14 @@ struct StencilVec<float, 4> {
 // values arrive k-major (three 128- or 256-byte lines per band) with no
 // index of any kind; products are added in column order.  Columns outside
 // [0, n) belong to zero entries and are clamped into range.
-template <typename T, int EPI, int NB>
+template <typename T, int EPI, int NB, bool FOLD = false>
 __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp op, Scratch sc)
 {
     if (gate_closed(op.gate)) return;
+    const T *__restrict__ fr = static_cast<const T *>(op.fold_r);
+    const T *__restrict__ fd = static_cast<const T *>(op.fold_d);
+    T beta = T(0);
+    if constexpr (FOLD) beta = (T)cta_scalar(op.fold_beta);
     // positions per lane and load: FP32 values come in groups of four (one
     // 16-byte load per lane), FP64 one by one
     constexpr int W = stencil_group<T>();
@@ -572,6 +542,11 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
     const V *__restrict__ sv = static_cast<const V *>(A.st_val);
     const T *__restrict__ x = static_cast<const T *>(op.x);
     const uint64_t pol = l2_policy(0);
+    // x at column j, or with FOLD the direction beta p_j + r_j d_j formed at the gather
+    auto gx = [&](int j) -> T {
+        if constexpr (FOLD) return cg_direction(beta, ld_keep(x + j, pol), ld_keep(fr + j, pol), ld_keep(fd + j, pol));
+        else return ld_keep(x + j, pol);
+    };
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     const int nw = gridDim.x * (kBlock / 32);
@@ -594,8 +569,8 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
                 const int d = cen[b];
-                const T w = ld_keep(x + min(max(r + d, 0), last), pol);
-                const T h = edge ? ld_keep(x + min(max(he + d, 0), last), pol) : T(0);
+                const T w = gx(min(max(r + d, 0), last));
+                const T h = edge ? gx(min(max(he + d, 0), last)) : T(0);
                 T left = __shfl_up_sync(0xffffffffu, w, 1);
                 T right = __shfl_down_sync(0xffffffffu, w, 1);
                 if (lane == 0) left = h;
@@ -614,8 +589,8 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
                     const int d = cen[b0 + bb];
 #pragma unroll
                     for (int m = 0; m < 3; ++m) StencilVec<T, W>::load(v + 32 * (3 * (b0 + bb) + m), pol, a + 3 * bb + m);
-                    w[bb] = ld_keep(x + min(max(r + d, 0), last), pol);
-                    h[bb] = edge ? ld_keep(x + min(max(he + d, 0), last), pol) : T(0);
+                    w[bb] = gx(min(max(r + d, 0), last));
+                    h[bb] = edge ? gx(min(max(he + d, 0), last)) : T(0);
                 }
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb) {
@@ -629,7 +604,7 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
                 }
             }
         }
-        if (r < n) epilogue<T, EPI>(r, s, op, acc);
+        if (r < n) fold_epilogue<T, EPI, FOLD>(r, s, op, beta, acc);
     }
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
@@ -738,14 +713,22 @@ struct HalfRow<double, NB> {
     }
 };
 
-template <typename T, int EPI, int NB>
+template <typename T, int EPI, int NB, bool FOLD = false>
 __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op, Scratch sc)
 {
     if (gate_closed(op.gate)) return;
     constexpr int U = (NB - 1) / 2;
+    const T *__restrict__ fr = static_cast<const T *>(op.fold_r);
+    const T *__restrict__ fd = static_cast<const T *>(op.fold_d);
+    T beta = T(0);
+    if constexpr (FOLD) beta = (T)cta_scalar(op.fold_beta);
     const T *__restrict__ x = static_cast<const T *>(op.x);
     const unsigned *__restrict__ mask = A.sh_mask;
     const uint64_t pol = l2_policy(0);
+    auto gx = [&](int j) -> T {
+        if constexpr (FOLD) return cg_direction(beta, ld_keep(x + j, pol), ld_keep(fr + j, pol), ld_keep(fd + j, pol));
+        else return ld_keep(x + j, pol);
+    };
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     const int nw = gridDim.x * (kBlock / 32);
@@ -772,8 +755,8 @@ __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op,
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
             const int d = cen[b];
-            const T w = ld_keep(x + min(max(r + d, 0), last), pol);
-            const T h = edge ? ld_keep(x + min(max(he + d, 0), last), pol) : T(0);
+            const T w = gx(min(max(r + d, 0), last));
+            const T h = edge ? gx(min(max(he + d, 0), last)) : T(0);
             T left = __shfl_up_sync(0xffffffffu, w, 1);
             T right = __shfl_down_sync(0xffffffffu, w, 1);
             if (lane == 0) left = h;
@@ -782,7 +765,7 @@ __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op,
             s += av[b][1] * w;
             s += av[b][2] * right;
         }
-        if (r < n) epilogue<T, EPI>(r, s, op, acc);
+        if (r < n) fold_epilogue<T, EPI, FOLD>(r, s, op, beta, acc);
     }
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
@@ -810,6 +793,18 @@ void launch_one_wave(K kern, int &resident, const Scratch &s, int n_rows, const 
 template <typename T, int EPI>
 void launch_epi(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st)
 {
+    if constexpr (EPI == EPI_DOT_X) {
+        if (op.fold_p) {
+            // the caller checked spmv_can_fold: a stencil layout over the whole operator
+            static int res_f[4] = {0, 0, 0, 0};
+            const bool half = A.sh_use && A.sh_val;
+            if (half && A.st_nb == 9) launch_one_wave(spmv_half_kernel<T, EPI, 9, true>, res_f[0], s, A.n_rows, A, op, st);
+            else if (half) launch_one_wave(spmv_half_kernel<T, EPI, 3, true>, res_f[1], s, A.n_rows, A, op, st);
+            else if (A.st_nb == 9) launch_one_wave(spmv_stencil_kernel<T, EPI, 9, true>, res_f[2], s, A.n_rows, A, op, st);
+            else launch_one_wave(spmv_stencil_kernel<T, EPI, 3, true>, res_f[3], s, A.n_rows, A, op, st);
+            return;
+        }
+    }
     if constexpr (EPI == EPI_SET || EPI == EPI_ADD || EPI == EPI_DOT_X || EPI == EPI_RESID) {
         if (A.sh_use && A.sh_val && A.st_use && seg.r0 == 0 && seg.r1 == A.n_rows && (A.st_nb == 3 || A.st_nb == 9)) {
             static int res_nb[2] = {0, 0};

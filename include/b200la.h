@@ -42,7 +42,8 @@ typedef enum {
     B200LA_ERR_NOTFOUND = 9,   /* unknown serving request id */
     B200LA_PENDING = 10,       /* serving request still queued or running */
     B200LA_ERR_IO = 11,        /* a file could not be opened, read or written */
-    B200LA_ERR_FORMAT = 12     /* unsupported or malformed file contents */
+    B200LA_ERR_FORMAT = 12,    /* unsupported or malformed file contents */
+    B200LA_ERR_COMM = 13       /* the communicator failed (NCCL error, NCCL absent, a rank that never arrived) */
 } b200la_status;
 
 /* IterateControl (src/common/iterate_control.h) */
@@ -130,7 +131,11 @@ int b200la_csr_info(const b200la_csr *A, int *n_rows, int *n_cols, int *nnz, int
  * matrix's row-pattern dictionary (0: none), *uses_dict = 1 when SpMV reads
  * the dictionary instead of the explicit column indices, 2 when it reads the
  * stencil layout (row patterns within 3 or 9 bands of three consecutive
- * column offsets: values only, no indices). */
+ * column offsets: values only, no indices), 3 the half stencil layout
+ * (symmetric stencil operators: diagonal and upper half), 4 the lattice
+ * layout (an operator or sweep part of a multicolour preconditioner on a
+ * parity-coloured structured Q1 grid: values by neighbour slot, no
+ * indices). */
 int b200la_csr_format(const b200la_csr *A, int *npat, int *uses_dict);
 /* lMatrix::CopyTo a host CSR (host arrays, val of the matrix dtype). */
 int b200la_csr_download(b200la_ctx *ctx, const b200la_csr *A, int *row, int *col, void *val);
@@ -414,6 +419,61 @@ int b200la_spmv_add_remote(b200la_ctx *ctx, const b200la_csr *A_offdiag, const v
  * (cudaDeviceEnablePeerAccess; B200LA_ERR_DEVICE when the pair has no peer
  * path).  Same device: nothing to do. */
 int b200la_enable_peer_access(int device, int peer_device);
+
+/* Communicator of the ranks of a coupled system, one rank per GPU: replaces
+ * the MPI communicator behind CoupledVector / CoupledMatrix (the Isend /
+ * Irecv of CoupledVector::SendBorder / ReceiveGhost, coupled_vector.cc:975-1128,
+ * and the MPI_Allreduce of CoupledVector::Dot, coupled_vector.cc:331-344).
+ * NCCL communicators: rank 0 makes an id with b200la_comm_unique_id (the
+ * process's libnccl.so.2, loaded at run time), the caller hands the
+ * B200LA_COMM_ID_BYTES bytes to every rank (as HiFlow3 would with
+ * MPI_Bcast), and each rank creates its communicator on its context's device
+ * (ncclCommInitRank).  Local communicators: b200la_comm_create_local makes
+ * nranks communicators for ranks that are host threads of one process (each
+ * with its own context, on one GPU or on several); their transfers are
+ * device copies ordered by events and the threads meet at a host barrier
+ * (60 s limit, then B200LA_ERR_COMM), so no kernel waits for another rank. */
+#define B200LA_COMM_ID_BYTES 128
+typedef struct b200la_comm b200la_comm;
+int b200la_comm_unique_id(void *id);
+int b200la_comm_create_nccl(b200la_ctx *ctx, const void *id, int rank, int nranks, b200la_comm **out);
+int b200la_comm_create_local(int nranks, b200la_comm **out);
+int b200la_comm_info(const b200la_comm *comm, int *rank, int *nranks);
+int b200la_comm_destroy(b200la_comm *comm);
+
+/* The coupled operator of one rank: LaCouplings (la_couplings.cc:62-230) plus
+ * CoupledMatrix (coupled_matrix.cc:433-467).  diag: the owned rows and
+ * columns; offdiag: the owned rows against the ghost columns (NULL when
+ * there are none), both as b200la_rowblock_split returns them and kept by
+ * the caller while the coupled operator lives.  ghost_offsets (nranks + 1):
+ * the ghosts owned by rank q are ghost columns [ghost_offsets[q],
+ * ghost_offsets[q+1]); border_offsets (nranks + 1) and border_indices: rank
+ * q reads, in that order, the owned rows border_indices[border_offsets[q] ..
+ * border_offsets[q+1]) as its ghosts owned here. */
+typedef struct b200la_coupled b200la_coupled;
+int b200la_coupled_create(b200la_ctx *ctx, b200la_comm *comm, const b200la_csr *diag, const b200la_csr *offdiag,
+                          const int *ghost_offsets, const int *border_offsets, const int *border_indices,
+                          b200la_coupled **out);
+int b200la_coupled_destroy(b200la_coupled *M);
+/* CoupledVector::UpdateGhost: the ghost values of x (owned values, device)
+ * into ghost (device, n_ghost values; NULL: only the operator's own ghost
+ * buffer).  Synchronous. */
+int b200la_coupled_update_ghost(b200la_ctx *ctx, b200la_coupled *M, const void *x, void *ghost);
+/* CoupledMatrix::VectorMult: y = A x over this rank's rows; the border is
+ * packed on the context's stream, exchanged on a second stream while the
+ * diagonal block is multiplied, and the off-diagonal block is added after
+ * it.  Stream-ordered; every rank calls it. */
+int b200la_coupled_spmv(b200la_ctx *ctx, b200la_coupled *M, const void *x, void *y);
+/* CoupledVector::Dot: the sum over all ranks of x . y (owned values). */
+int b200la_coupled_dot(b200la_ctx *ctx, b200la_coupled *M, const void *x, const void *y, double *out);
+/* CG<LAD>::Solve over the coupled operator (cg.cc:164-248), with no
+ * preconditioner or with the Jacobi preconditioner of this rank's diagonal
+ * block (P from b200la_precond_jacobi on diag: block-Jacobi with point
+ * blocks, as PreconditionerBlockJacobiStand binds op.diagonal()).  The
+ * recurrence scalars stay on the device and are reduced across ranks by the
+ * communicator; every rank gets the same iteration count and status. */
+int b200la_coupled_cg(b200la_ctx *ctx, b200la_coupled *M, const b200la_precond *P, const void *b, void *x,
+                      const b200la_control *ctl, b200la_result *res);
 
 /* ---------------------------------------------------------------- file I/O */
 /* Host arrays.  MatrixMarket matrices: replaces CPU_CSR_lMatrix::ReadFile / WriteFile

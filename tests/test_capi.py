@@ -60,3 +60,18 @@ def test_hiflow_adapter_library_loads():
     assert "hiflow::la::B200_lVector<double>::Dot" in out and "hiflow::la::B200_CSR_lMatrix<float>::VectorMult" in out
     ldd = subprocess.run(["ldd", so], capture_output=True, text=True).stdout
     assert "libb200la.so" in ldd and "not found" not in ldd
+
+
+def test_local_communicators_on_the_host(b200):
+    """Local communicators are host objects until a rank first uses one."""
+    L = b200.lib()
+    arr = (ctypes.c_void_p * 3)()
+    assert L.b200la_comm_create_local(3, arr) == 0
+    for q in range(3):
+        r, n = ctypes.c_int(), ctypes.c_int()
+        assert L.b200la_comm_info(ctypes.c_void_p(arr[q]), ctypes.byref(r), ctypes.byref(n)) == 0
+        assert (r.value, n.value) == (q, 3)
+    for q in range(3):
+        assert L.b200la_comm_destroy(ctypes.c_void_p(arr[q])) == 0
+    assert L.b200la_comm_create_local(0, arr) == 1
+    assert L.b200la_status_string(13) == b"communicator failed"
