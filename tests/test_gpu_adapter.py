@@ -112,7 +112,13 @@ def test_benchmark_local_solver_flow_on_b200_objects(ad, ref, oracle, b200, tmp_
     x_true = np.random.default_rng(1).uniform(-1, 1, n)
     b = ref.spmv(row, col, val, x_true)
     files = {k: str(tmp_path / f"{k}.txt") for k in ("A", "b", "x_result", "x_start")}
-    b200.write_matrix_market(files["A"], row, col, val)
+    # the reference's writer puts entries as "column row value", so a file it
+    # writes reads back as the transpose: write A^T to have A read back (A is
+    # not symmetric: its Dirichlet rows are identity rows)
+    import scipy.sparse as sp
+    At = sp.csr_matrix((val, col, row), shape=(n, n)).T.tocsr()
+    At.sort_indices()
+    b200.write_matrix_market(files["A"], At.indptr, At.indices, At.data)
     b200.write_vector(files["b"], b)
     b200.write_vector(files["x_result"], x_true)
     b200.write_vector(files["x_start"], np.zeros(n))
