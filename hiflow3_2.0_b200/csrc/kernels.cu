@@ -130,7 +130,8 @@ __device__ __forceinline__ void cg_update_elem(T alpha, T &x, T &r, T p, T ap, T
 template <typename T>
 __global__ void __launch_bounds__(kBlock) cg_update_kernel(int n, int precond, T *__restrict__ x, T *__restrict__ r,
                                                            const T *__restrict__ p, const T *__restrict__ Ap,
-                                                           const T *__restrict__ invd, DevState *st, Scratch sc)
+                                                           const T *__restrict__ invd, DevState *st, Scratch sc,
+                                                           unsigned long long cond)
 {
     if (gate_closed(&st->status)) return;
     using V = typename Vec16<T>::type;
@@ -182,6 +183,7 @@ __global__ void __launch_bounds__(kBlock) cg_update_kernel(int n, int precond, T
             st->beta = g / st->rho;
             st->rho = g;
         }
+        if (cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, status == kIterate ? 1u : 0u);
     }
 }
 
@@ -375,11 +377,12 @@ cudaError_t launch_scatter(int dtype, int n, const int *idx, const void *vals, v
 }
 
 cudaError_t launch_cg_update(const Scratch &s, int dtype, int n, int precond, void *x, void *r, const void *p,
-                             const void *Ap, const void *invd, DevState *st, cudaStream_t stm)
+                             const void *Ap, const void *invd, DevState *st, cudaStream_t stm,
+                             unsigned long long cond)
 {
     const int g = stream_grid(&s, n);
     B200_DISPATCH(dtype, cg_update_kernel<T><<<g, kBlock, 0, stm>>>(n, precond, (T *)x, (T *)r, (const T *)p,
-                                                                    (const T *)Ap, (const T *)invd, st, s));
+                                                                    (const T *)Ap, (const T *)invd, st, s, cond));
     return cudaGetLastError();
 }
 

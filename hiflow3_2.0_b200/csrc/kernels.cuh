@@ -263,8 +263,12 @@ cudaError_t launch_fill(int dtype, int n, double v, void *y, cudaStream_t st);
 // precond == 2: the caller reduces r.z after its own apply).  The last CTA
 // advances iter, stores res, runs Check and, when iterating, sets
 // beta = rz / rho and rho = rz (precond 0/1).
+// cond: a graph conditional handle (0: none) that the last CTA sets to
+// "keep iterating" after its Check -- the loop condition of a device-side
+// while node around the iterations.
 cudaError_t launch_cg_update(const Scratch &s, int dtype, int n, int precond, void *x, void *r, const void *p,
-                             const void *Ap, const void *invd, DevState *st, cudaStream_t stm);
+                             const void *Ap, const void *invd, DevState *st, cudaStream_t stm,
+                             unsigned long long cond = 0);
 // p = beta p + z with z = invd .* r (precond 1), z = r (precond 0), or z given.
 cudaError_t launch_cg_pupdate(int dtype, int n, int precond, void *p, const void *r, const void *invd,
                               const void *z, DevState *st, cudaStream_t stm);

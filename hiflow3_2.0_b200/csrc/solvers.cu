@@ -76,6 +76,67 @@ static int get_graph(b200la_ctx *ctx, const std::vector<const void *> &key, Body
     return B200LA_OK;
 }
 
+// The same for a graph whose single node is a device-side while loop: its
+// body is `body(h)` captured once (K iterations), and the loop runs again as
+// long as the conditional handle h -- set by the update kernel after each
+// Check -- says "iterate".  One launch runs the solve to its stop; the host
+// waits once instead of once per batch, and no batch of gated iterations
+// runs after the stop.
+template <class Body>
+static int get_while_graph(b200la_ctx *ctx, const std::vector<const void *> &key, Body body, cudaGraphExec_t *exec,
+                           int *nodes)
+{
+    for (auto &g : ctx->graphs)
+        if (g.key == key) {
+            *exec = g.exec;
+            *nodes = g.launches;
+            return B200LA_OK;
+        }
+    if (ctx->graphs.size() >= 32) graph_cache_clear(ctx);
+    cudaGraph_t graph = nullptr;
+    SK(cudaGraphCreate(&graph, 0));
+    struct GraphGuard {
+        cudaGraph_t g;
+        ~GraphGuard()
+        {
+            if (g) cudaGraphDestroy(g);
+        }
+    } guard{graph};
+    cudaGraphConditionalHandle h;
+    SK(cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams prm = {cudaGraphNodeTypeConditional};
+    prm.conditional.handle = h;
+    prm.conditional.type = cudaGraphCondTypeWhile;
+    prm.conditional.size = 1;
+    cudaGraphNode_t node;
+    SK(cudaGraphAddNode(&node, graph, nullptr, 0, &prm));
+    cudaGraph_t loop = prm.conditional.phGraph_out[0];
+    SK(cudaStreamBeginCaptureToGraph(ctx->stream, loop, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    const long long before = ctx->launches;
+    const int rc = body((unsigned long long)h);
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &loop);
+    if (rc) return rc;
+    if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_CUDA, "loop body capture", e);
+    GraphEntry g;
+    g.key = key;
+    g.launches = (int)(ctx->launches - before);
+    ctx->launches = before;
+    e = cudaGraphInstantiate(&g.exec, graph, 0);
+    if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_CUDA, "loop graph instantiate", e);
+    ctx->graphs.push_back(g);
+    *exec = g.exec;
+    *nodes = g.launches;
+    return B200LA_OK;
+}
+
+// Device-side loop control of the CG iterations (B200LA_GRAPH_LOOP=0: host
+// reads the stop state after every batch instead).
+static bool loop_policy()
+{
+    const char *e = std::getenv("B200LA_GRAPH_LOOP");
+    return !e || std::atoi(e) != 0;
+}
+
 static void state_init(DevState &s, const b200la_control *ctl, double *hist, int hist_len)
 {
     std::memset(&s, 0, sizeof s);
@@ -140,6 +201,7 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
     // first product, with beta = 0 from state_init, forms p = z of the start
     const bool fold = pc == 1 && w.z && spmv_can_fold(A) && !std::getenv("B200LA_NOFOLD");
     int parity = 0;
+    unsigned long long cond = 0;   // loop condition of the device-side while node (when captured in one)
 
     auto iteration = [&]() -> int {
         void *p_old = (fold && parity) ? w.z : w.p, *p_cur = p_old;
@@ -162,7 +224,7 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
         int r2 = spmv_run(ctx, A, A->all, o);
         if (r2) return r2;
         // x += alpha p; r -= alpha Ap; res = ||r||; Check       (cg.cc:221-230)
-        SK(launch_cg_update(sc, dt, n, pc, x, w.r, p_cur, w.Ap, invd, ctx->st, ctx->stream));
+        SK(launch_cg_update(sc, dt, n, pc, x, w.r, p_cur, w.Ap, invd, ctx->st, ctx->stream, cond));
         ctx->launches += 1;
         if (fold) return B200LA_OK;   // p = beta p + z happens in the next product (cg.cc:241)
         if (pc == 2) {
@@ -197,23 +259,43 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
             SK(cudaStreamSynchronize(ctx->stream));
         }
     }
-    if (!no_graph) rc = get_graph(
-        ctx, {A, P, b, x, w.r, w.p, w.Ap, w.z, (const void *)(intptr_t)K, (const void *)(intptr_t)pc, ctx->stream,
-              (const void *)(intptr_t)fold},
-        [&]() -> int {
-            for (int k = 0; k < K; ++k) {
-                int r2 = iteration();
-                if (r2) return r2;
-            }
-            return B200LA_OK;
-        },
-        &exec, &nodes);
+    const bool loop = !no_graph && loop_policy();
+    const std::vector<const void *> key = {A, P, b, x, w.r, w.p, w.Ap, w.z, (const void *)(intptr_t)K,
+                                           (const void *)(intptr_t)pc, ctx->stream, (const void *)(intptr_t)fold,
+                                           (const void *)(intptr_t)loop};
+    auto batch = [&]() -> int {
+        for (int k = 0; k < K; ++k) {
+            int r2 = iteration();
+            if (r2) return r2;
+        }
+        return B200LA_OK;
+    };
+    if (loop)
+        rc = get_while_graph(
+            ctx, key,
+            [&](unsigned long long h) -> int {
+                cond = h;
+                const int r2 = batch();
+                cond = 0;
+                return r2;
+            },
+            &exec, &nodes);
+    else if (!no_graph)
+        rc = get_graph(ctx, key, batch, &exec, &nodes);
     if (rc) return rc;
     SK(cudaMemcpyAsync(hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
     SK(cudaStreamSynchronize(ctx->stream));
     long long graph_launches = 0;
+    if (loop && hs->status == kIterate) {
+        // one launch; the loop ends on the device at the stop of IterateControl
+        const int it0 = hs->iter;
+        SK(cudaGraphLaunch(exec, ctx->stream));
+        SK(cudaMemcpyAsync(hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
+        SK(cudaStreamSynchronize(ctx->stream));
+        graph_launches += (long long)nodes * std::max(1, (hs->iter - it0 + K - 1) / K);
+    }
     const long long max_batches = (long long)ctl->maxits / K + 2;
-    for (long long bt = 0; !no_graph && hs->status == kIterate && bt < max_batches; ++bt) {
+    for (long long bt = 0; !no_graph && !loop && hs->status == kIterate && bt < max_batches; ++bt) {
         SK(cudaGraphLaunch(exec, ctx->stream));
         graph_launches += nodes;
         SK(cudaMemcpyAsync(hs, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));

@@ -381,3 +381,39 @@ def test_folded_direction_matches_separate_update(pf, b200, oracle, monkeypatch,
     assert f[2] < u[2]   # fewer launches: the separate direction update is gone
     ref = oracle.pcg(row, col, val, b, precond=oracle.invdiag(row, col, val), ctl=control(20000, 0, 1e-10, 1e6))
     assert within5(f[0], ref["iters"]), (f[0], ref["iters"])
+
+
+@pytest.mark.parametrize("precond", ["none", "jacobi", "mcsgs"])
+def test_device_loop_matches_host_batches(pf, b200, monkeypatch, precond):
+    """The CG iterations run in a device-side while loop (one graph launch per
+    solve; the update kernel sets the loop condition after its Check).  The
+    arithmetic is the same as with the host reading the stop state between
+    batches, so iterations, residuals and solutions are bitwise equal, also
+    for maxits stops and for stops inside a batch."""
+    row, col, val = b200.q1_assemble(3, 14)
+    b = b200.q1_rhs(5, 3, 14)
+    out = {}
+    for loop in ("1", "0"):
+        monkeypatch.setenv("B200LA_GRAPH_LOOP", loop)
+        if precond == "mcsgs":
+            P = b200.Preconditioner.MultiColoringSGS(pf, row, col, val)
+            A, bb = P.A_perm, b[P.perm]
+        else:
+            A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+            P = b200.Preconditioner.Jacobi(pf, A) if precond == "jacobi" else None
+            bb = b
+        res = []
+        for maxits, tol in ((100000, 1e-10), (37, 1e-10), (100000, 1e-3)):
+            cg = b200.CG(pf)
+            cg.SetupOperator(A)
+            cg.SetupPreconditioner(P)
+            cg.InitControl(maxits, 0.0, tol, 1e6)
+            x = pf.vector(len(bb))
+            st = cg.Solve(pf.vector(bb), x)
+            res.append((st, cg.iter(), cg.result.res, x.numpy()))
+        out[loop] = res
+    monkeypatch.delenv("B200LA_GRAPH_LOOP")
+    for a, c in zip(out["1"], out["0"]):
+        assert a[:3] == c[:3]
+        assert np.array_equal(a[3], c[3])
+    assert out["1"][1][0] == b200.FAIL_MAXITS and out["1"][1][1] == 37
