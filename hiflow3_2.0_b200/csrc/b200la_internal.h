@@ -92,6 +92,9 @@ struct b200la_csr {
     // lattice layout (multicoloured structured Q1 operators): see kernels.cuh
     void *lt_val = nullptr;
     b200::LatticeDesc *lt = nullptr;
+    // FP32 Jacobi scaling (float)(1 / a_ii) of an FP64 operator, kept for the
+    // defect correction's inner solves; dropped when the values change
+    float *invd32 = nullptr;
 };
 
 struct b200la_precond {

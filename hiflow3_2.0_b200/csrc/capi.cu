@@ -72,6 +72,13 @@ static bool stencil_policy(int dtype)
     return mode == 2 || (mode == 1 && dtype == B200LA_F32);
 }
 
+// The cached FP32 Jacobi scaling no longer matches changed values.
+static void drop_invd32(b200la_csr *A)
+{
+    if (A->invd32) cudaFree(A->invd32);
+    A->invd32 = nullptr;
+}
+
 CsrView csr_view(const b200la_csr *A)
 {
     CsrView v;
@@ -725,6 +732,7 @@ extern "C" int b200la_csr_destroy(b200la_csr *A)
     if (A->st_val) cudaFree(A->st_val);
     free_half(A);
     lattice_free(A);
+    if (A->invd32) cudaFree(A->invd32);
     delete A;
     return B200LA_OK;
 }
@@ -753,6 +761,7 @@ extern "C" int b200la_csr_cast(b200la_ctx *ctx, const b200la_csr *A, int dtype, 
     B->sh_use = 0;
     B->lt_val = nullptr;   // the lattice layout stays with A (built by the preconditioners)
     B->lt = nullptr;
+    B->invd32 = nullptr;
     const size_t pad = 8, es = dsize(dtype);
     cudaError_t e;
     if (A->pid) {
@@ -846,6 +855,7 @@ extern "C" int b200la_csr_set_values(b200la_ctx *ctx, b200la_csr *A, const void 
     if (!ctx || !A || (A->nnz && !val)) return B200LA_ERR_ARG;
     if (A->nnz) CK(cudaMemcpyAsync(A->val, val, dsize(A->dtype) * A->nnz, cudaMemcpyHostToDevice, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    drop_invd32(A);
     int rc = build_sell(ctx, A);
     if (!rc) rc = build_stencil(ctx, A);
     return rc ? rc : lattice_refresh(ctx, A);
@@ -857,6 +867,7 @@ extern "C" int b200la_csr_scale(b200la_ctx *ctx, b200la_csr *A, double alpha, in
         return ctx_msg(ctx, B200LA_ERR_ARG, "csr_scale: invalid argument");
     if (A->nnz) CK(launch_csr_scale(A->dtype, A->n, A->row, A->col, A->val, alpha, mode, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    drop_invd32(A);
     // the SpMV layouts derived from the values follow them
     int rc = build_sell(ctx, A);
     if (!rc) rc = build_stencil(ctx, A);

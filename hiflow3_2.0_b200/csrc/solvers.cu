@@ -395,17 +395,23 @@ extern "C" int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_
     char *base = static_cast<char *>(wk);
     double *r = reinterpret_cast<double *>(base);
     double *invd64 = reinterpret_cast<double *>(base + v8);
-    float *invd32 = reinterpret_cast<float *>(base + 2 * v8);
+    float *invd32 = nullptr;   // the operator's cached FP32 Jacobi scaling (below)
     float *rl = reinterpret_cast<float *>(base + 2 * v8 + v4);
     float *cl = reinterpret_cast<float *>(base + 2 * v8 + 2 * v4);
     CgWork w{base + 2 * v8 + 3 * v4, base + 2 * v8 + 4 * v4, base + 2 * v8 + 5 * v4, base + 2 * v8 + 6 * v4};
     const long long l0 = ctx->launches;
 
+    // FP32 Jacobi from the FP64 diagonal (1/a_ii rounded once), made at the
+    // operator's first defect correction and kept with it until its values change
+    if (!A64->invd32) {
+        b200la_csr *Am = const_cast<b200la_csr *>(A64);
+        SK(cudaMalloc(&Am->invd32, sizeof(float) * std::max(n, 1)));
+        SK(launch_invdiag(B200LA_F64, n, A64->row, A64->col, A64->val, invd64, ctx->stream));
+        SK(launch_cast(B200LA_F64, invd64, B200LA_F32, Am->invd32, n, ctx->stream));
+        ctx->launches += 2;
+    }
+    invd32 = A64->invd32;
     SK(cudaEventRecord(ctx->ev0, ctx->stream));
-    // FP32 Jacobi from the FP64 diagonal (1/a_ii rounded once)
-    SK(launch_invdiag(B200LA_F64, n, A64->row, A64->col, A64->val, invd64, ctx->stream));
-    SK(launch_cast(B200LA_F64, invd64, B200LA_F32, invd32, n, ctx->stream));
-    ctx->launches += 2;
     b200la_precond J;
     J.kind = B200LA_PRECOND_JACOBI;
     J.n = n;

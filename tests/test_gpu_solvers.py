@@ -417,3 +417,32 @@ def test_device_loop_matches_host_batches(pf, b200, monkeypatch, precond):
         assert a[:3] == c[:3]
         assert np.array_equal(a[3], c[3])
     assert out["1"][1][0] == b200.FAIL_MAXITS and out["1"][1][1] == 37
+
+
+def test_mpir_jacobi_scaling_follows_value_changes(pf, b200):
+    """The defect correction keeps the FP32 Jacobi scaling of its FP64
+    operator between solves; scaling the operator drops it, so the next
+    solve matches one on a freshly built operator bit for bit."""
+    row, col, val = b200.q1_assemble(3, 12)
+    b = b200.q1_rhs(9, 3, 12)
+    n = len(b)
+    A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    mp = b200.MPIR(pf)
+    mp.SetupOperator(A)
+    mp.InitControl(50, 0.0, 1e-10, 1e6)
+    x1 = pf.vector(n)
+    assert mp.Solve(pf.vector(b), x1) == b200.SUCCESS_REL
+    x1b = pf.vector(n)
+    mp.Solve(pf.vector(b), x1b)
+    assert np.array_equal(x1.numpy(), x1b.numpy())      # the cached scaling gives the same solve
+    A.Scale(3.0)
+    x2 = pf.vector(n)
+    mp.Solve(pf.vector(b), x2)
+    B = b200.CSR_lMatrix.from_csr(pf, row, col, 3.0 * val)
+    mq = b200.MPIR(pf)
+    mq.SetupOperator(B)
+    mq.InitControl(50, 0.0, 1e-10, 1e6)
+    x3 = pf.vector(n)
+    mq.Solve(pf.vector(b), x3)
+    assert np.array_equal(x2.numpy(), x3.numpy())
+    assert mp.result.iters == mq.result.iters
