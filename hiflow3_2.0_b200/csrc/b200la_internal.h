@@ -123,7 +123,6 @@ int ctx_work(b200la_ctx *ctx, size_t bytes, void **out);
 int ctx_work_outer(b200la_ctx *ctx, size_t bytes, void **out);
 int ctx_check_device_error(b200la_ctx *ctx);
 int spmv_run(b200la_ctx *ctx, const b200la_csr *A, const b200::Seg &seg, b200::SpmvOp op);
-bool spmv_can_fold(const b200la_csr *A);
 int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row, const int *col, const void *val,
                int dtype, int n_seg, const int *seg_off, b200la_csr **out);
 // precond.cu

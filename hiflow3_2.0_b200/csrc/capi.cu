@@ -950,20 +950,17 @@ extern "C" int b200la_csr_invdiag(b200la_ctx *ctx, const b200la_csr *A, void *ou
 
 // ------------------------------------------------------------------- SpMV
 
-// Whether the SpMV of A can fold the Jacobi-CG direction update into its
-// gathers (SpmvOp::fold_p): A's product runs on a stencil layout.
-bool spmv_can_fold(const b200la_csr *A)
-{
-    return A && !A->lt && A->st_use && A->st_val && (A->st_nb == 3 || A->st_nb == 9) && A->n == A->m;
-}
-
 int spmv_run(b200la_ctx *ctx, const b200la_csr *A, const Seg &seg, SpmvOp op)
 {
     int c0, c1;
     if (lattice_segment(A, seg, &c0, &c1)) {
-        CK(launch_lattice(ctx_scratch(ctx), A->dtype, *A->lt, A->lt_val, c0, c1, op, ctx->stream));
-        ctx->launches += 1;
-        return B200LA_OK;
+        const cudaError_t e = launch_lattice(ctx_scratch(ctx), A->dtype, *A->lt, A->lt_val, c0, c1, op, ctx->stream);
+        if (e != cudaErrorNotSupported) {   // not supported: this epilogue and range run on the CSR below
+            CK(e);
+            ctx->launches += 1;
+            return B200LA_OK;
+        }
+        cudaGetLastError();
     }
     CK(launch_spmv(ctx_scratch(ctx), csr_view(A), seg, op, ctx->stream));
     ctx->launches += 1;

@@ -45,8 +45,7 @@ __device__ __forceinline__ int check_state(DevState *st, int step, double value)
 }
 // The Jacobi-CG direction p_new = beta p + z with z = r d (cg.cc:241 and
 // lpreconditioner.cc:127-165): one rounding of r d, then one fused
-// multiply-add -- the same bits wherever it is formed (the direction update
-// kernel, or the SpMV that folds it into its gathers).
+// multiply-add.
 __device__ __forceinline__ double cg_direction(double beta, double p, double r, double d)
 {
     return fma(beta, p, __dmul_rn(r, d));
@@ -206,15 +205,6 @@ struct SpmvOp {
     double *dot_out = nullptr;
     DevState *st = nullptr;
     const int *gate = nullptr;    // skip the launch body when *gate != 0
-    // Jacobi-CG direction folded into the product (EPI_DOT_X on the stencil
-    // layouts only, see spmv_can_fold): x holds the previous direction p, and
-    // every gathered column j uses p_new[j] = beta p[j] + r[j] d[j]
-    // (cg_direction, beta = *fold_beta); the row's own p_new goes to fold_p
-    // and into the dot.  Replaces the separate direction update of the loop.
-    void *fold_p = nullptr;
-    const void *fold_r = nullptr;
-    const void *fold_d = nullptr;
-    const double *fold_beta = nullptr;
 };
 
 struct Scratch {

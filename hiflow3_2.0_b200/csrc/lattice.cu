@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <array>
 #include <cstdlib>
+#include <type_traits>
 #include <vector>
 
 namespace b200 {
@@ -33,7 +34,134 @@ namespace {
 
 constexpr int kLatGroup = 9;   // slots whose loads are issued together
 
-template <typename T, int EPI>
+// Neighbour slots of colour c for a part (0 strictly lower: neighbour colour
+// < c; 1 strictly upper: > c; 2 every position with the diagonal), ordered by
+// (neighbour colour, dz, dy, dx) -- the row's ascending column order.  The
+// same table drives the host's placement of the values and, as a compile-time
+// constant, the kernels.
+struct SlotTab {
+    int n;
+    signed char dx[kLatMaxSlots], dy[kLatMaxSlots], dz[kLatMaxSlots], cp[kLatMaxSlots];
+};
+
+__host__ __device__ constexpr SlotTab slot_table(int dim, int c, int part)
+{
+    SlotTab t{};
+    for (int dz = dim == 3 ? -1 : 0; dz <= (dim == 3 ? 1 : 0); ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int m = (dx != 0 ? 1 : 0) + (dy != 0 ? 2 : 0) + (dz != 0 ? 4 : 0);
+                const int cp = c ^ m;
+                if ((part == 0 && cp < c) || (part == 1 && cp > c) || part == 2) {
+                    t.dx[t.n] = (signed char)dx;
+                    t.dy[t.n] = (signed char)dy;
+                    t.dz[t.n] = (signed char)dz;
+                    t.cp[t.n] = (signed char)cp;
+                    ++t.n;
+                }
+            }
+    // insertion sort by (cp, dz, dy, dx)
+    for (int i = 1; i < t.n; ++i)
+        for (int j = i; j > 0; --j) {
+            const int a = ((t.cp[j - 1] * 4 + t.dz[j - 1] + 1) * 4 + t.dy[j - 1] + 1) * 4 + t.dx[j - 1] + 1;
+            const int b = ((t.cp[j] * 4 + t.dz[j] + 1) * 4 + t.dy[j] + 1) * 4 + t.dx[j] + 1;
+            if (a <= b) break;
+            signed char v = 0;
+            v = t.dx[j - 1]; t.dx[j - 1] = t.dx[j]; t.dx[j] = v;
+            v = t.dy[j - 1]; t.dy[j - 1] = t.dy[j]; t.dy[j] = v;
+            v = t.dz[j - 1]; t.dz[j - 1] = t.dz[j]; t.dz[j] = v;
+            v = t.cp[j - 1]; t.cp[j - 1] = t.cp[j]; t.cp[j] = v;
+        }
+    return t;
+}
+
+template <int DIM, int C, int PART>
+struct Slots {
+    static constexpr SlotTab tab = slot_table(DIM, C, PART);
+};
+
+// the sublattice step of an offset: floor((parity + d) / 2)
+__host__ __device__ constexpr int sub_step(int parity, int d) { return parity + d < 0 ? -1 : (parity + d) / 2; }
+
+template <int K, int N, class F>
+__device__ __forceinline__ void static_for(F &&f)
+{
+    if constexpr (K < N) {
+        f(std::integral_constant<int, K>());
+        static_for<K + 1, N>(f);
+    }
+}
+
+// One 32-row chunk of colour C (chunk g of the launch's numbering): each lane
+// forms its row's lattice position, one row base per neighbour colour, and
+// then, slot by slot, a column that is that base plus compile-time multiples
+// of the neighbour colour's extents.  Neighbours outside the grid (their
+// values are zero) are not loaded.
+template <typename T, int EPI, int DIM, int PART, int C>
+__device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__restrict__ val,
+                                              const T *__restrict__ x, int g, int lane, const SpmvOp &op,
+                                              uint64_t pol, double &acc)
+{
+    constexpr SlotTab S = Slots<DIM, C, PART>::tab;
+    constexpr int px = C & 1, py = (C >> 1) & 1, pz = (C >> 2) & 1;
+    const LatticeColour &L = d.col[C];
+    const int t = ((g - L.chunk0) << 5) + lane;
+    const bool active = t < L.rows;
+    // padding lanes of a colour's last chunk take its last row's node
+    const int tt = active ? t : L.rows - 1;
+    const int q = tt / L.nx, xs = tt - q * L.nx;
+    int ys = q, zs = 0;
+    if constexpr (DIM == 3) {
+        zs = q / L.ny;
+        ys = q - zs * L.ny;
+    }
+    const int X = 2 * xs + px, Y = 2 * ys + py, Z = 2 * zs + pz;
+    const bool xlo = X > 0, xhi = X < d.mx - 1, ylo = Y > 0, yhi = Y < d.my - 1, zlo = Z > 0, zhi = Z < d.mz - 1;
+    int base[kLatMaxColours];
+    static_for<0, kLatMaxColours>([&](auto cc) {
+        constexpr int cp = decltype(cc)::value;
+        bool used = false;
+        for (int k = 0; k < S.n; ++k) used |= S.cp[k] == cp;
+        if (used) {
+            const LatticeColour &P = d.col[cp];
+            base[cp] = P.row0 + (zs * P.ny + ys) * P.nx + xs;
+        }
+    });
+    const T *v = val + L.val0 + (size_t)(g - L.chunk0) * (S.n * 32) + lane;
+    T s = T(0);
+    static_for<0, (S.n + kLatGroup - 1) / kLatGroup>([&](auto gg) {
+        constexpr int k0 = decltype(gg)::value * kLatGroup;
+        constexpr int cnt = S.n - k0 < kLatGroup ? S.n - k0 : kLatGroup;
+        T a[kLatGroup], w[kLatGroup];
+        static_for<0, cnt>([&](auto jj) {
+            constexpr int j = decltype(jj)::value, k = k0 + j;
+            constexpr int dx = S.dx[k], dy = S.dy[k], dz = S.dz[k], cp = S.cp[k];
+            constexpr int ex = sub_step(px, dx), ey = sub_step(py, dy), ez = sub_step(pz, dz);
+            const LatticeColour &P = d.col[cp];
+            int col = base[cp] + ex;
+            if constexpr (ey != 0) col += ey * P.nx;
+            if constexpr (ez != 0) col += ez * (P.ny * P.nx);
+            bool ok = true;
+            if constexpr (dx < 0) ok = ok && xlo;
+            if constexpr (dx > 0) ok = ok && xhi;
+            if constexpr (dy < 0) ok = ok && ylo;
+            if constexpr (dy > 0) ok = ok && yhi;
+            if constexpr (dz < 0) ok = ok && zlo;
+            if constexpr (dz > 0) ok = ok && zhi;
+            a[j] = ld_stream(v + 32 * k, pol);
+            w[j] = ok ? ld_keep(x + col, pol) : T(0);
+        });
+        static_for<0, cnt>([&](auto jj) {
+            constexpr int j = decltype(jj)::value;
+            s += a[j] * w[j];
+        });
+    });
+    if (active) epilogue<T, EPI>(L.row0 + t, s, op, acc);
+}
+
+// CF >= 0: every chunk belongs to colour CF (one sweep step); CF < 0: chunks
+// of colours [c0, c1), each dispatched to its colour's compiled body.
+template <typename T, int EPI, int DIM, int PART, int CF>
 __global__ void __launch_bounds__(kBlock) lattice_kernel(const __grid_constant__ LatticeDesc d,
                                                          const T *__restrict__ val, int c0, int c1, SpmvOp op,
                                                          Scratch sc)
@@ -46,43 +174,18 @@ __global__ void __launch_bounds__(kBlock) lattice_kernel(const __grid_constant__
     const int nw = gridDim.x * (kBlock / 32);
     const int g0 = d.col[c0].chunk0;
     const int g1 = d.col[c1 - 1].chunk0 + ((d.col[c1 - 1].rows + 31) >> 5);
-    const unsigned mx = d.mx, my = d.my, mz = d.mz;
     double acc = 0.0;
     for (int g = g0 + gw; g < g1; g += nw) {
-        int c = c0;
-        while (c + 1 < c1 && g >= d.col[c + 1].chunk0) ++c;
-        const LatticeColour &L = d.col[c];
-        const int t = ((g - L.chunk0) << 5) + lane;
-        const bool active = t < L.rows;
-        // padding lanes of a colour's last chunk take its last row's node
-        const int tt = active ? t : L.rows - 1;
-        const int q = tt / L.nx, xs = tt - q * L.nx, zs = q / L.ny, ys = q - zs * L.ny;
-        const int X = 2 * xs + L.px, Y = 2 * ys + L.py, Z = 2 * zs + L.pz;
-        const int ns = L.nslot;
-        const T *v = val + L.val0 + (size_t)(g - L.chunk0) * ns * 32 + lane;
-        T s = T(0);
-        for (int k0 = 0; k0 < ns; k0 += kLatGroup) {
-            T a[kLatGroup], w[kLatGroup];
-#pragma unroll
-            for (int j = 0; j < kLatGroup; ++j) {
-                const int k = k0 + j;
-                a[j] = T(0);
-                w[j] = T(0);
-                if (k < ns) {
-                    const unsigned sl = L.slot[k];
-                    const int xn = X + (int)(sl & 3u) - 1, yn = Y + (int)((sl >> 2) & 3u) - 1,
-                              zn = Z + (int)((sl >> 4) & 3u) - 1;
-                    const LatticeColour &P = d.col[sl >> 8];
-                    a[j] = ld_stream(v + 32 * k, pol);
-                    if ((unsigned)xn < mx && (unsigned)yn < my && (unsigned)zn < mz)
-                        w[j] = ld_keep(x + P.row0 + ((zn >> 1) * P.ny + (yn >> 1)) * P.nx + (xn >> 1), pol);
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < kLatGroup; ++j)
-                if (k0 + j < ns) s += a[j] * w[j];
+        if constexpr (CF >= 0) {
+            lattice_chunk<T, EPI, DIM, PART, CF>(d, val, x, g, lane, op, pol, acc);
+        } else {
+            int c = c0;
+            while (c + 1 < c1 && g >= d.col[c + 1].chunk0) ++c;
+            static_for<0, (DIM == 3 ? 8 : 4)>([&](auto cc) {
+                constexpr int C = decltype(cc)::value;
+                if (c == C) lattice_chunk<T, EPI, DIM, PART, C>(d, val, x, g, lane, op, pol, acc);
+            });
         }
-        if (active) epilogue<T, EPI>(L.row0 + t, s, op, acc);
     }
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
@@ -90,47 +193,74 @@ __global__ void __launch_bounds__(kBlock) lattice_kernel(const __grid_constant__
     }
 }
 
-template <typename T, int EPI>
-cudaError_t launch_t(const Scratch &s, const LatticeDesc &d, const void *val, int c0, int c1, const SpmvOp &op,
+template <typename T, int EPI, int DIM, int PART, int CF>
+cudaError_t launch_k(const Scratch &s, const LatticeDesc &d, const void *val, int c0, int c1, const SpmvOp &op,
                      cudaStream_t st)
 {
     static int resident = 0;
-    if (!resident && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, lattice_kernel<T, EPI>, kBlock, 0) !=
-                         cudaSuccess)
+    auto kern = lattice_kernel<T, EPI, DIM, PART, CF>;
+    if (!resident && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kBlock, 0) != cudaSuccess)
         resident = 4;
     const int chunks = d.col[c1 - 1].chunk0 + ((d.col[c1 - 1].rows + 31) >> 5) - d.col[c0].chunk0;
     int grid = (chunks + kBlock / 32 - 1) / (kBlock / 32);
     grid = std::min(grid, std::min(s.num_sms * std::max(resident, 1), kMaxGrid));
     grid = std::max(grid, 1);
-    lattice_kernel<T, EPI><<<grid, kBlock, 0, st>>>(d, static_cast<const T *>(val), c0, c1, op, s);
+    kern<<<grid, kBlock, 0, st>>>(d, static_cast<const T *>(val), c0, c1, op, s);
     return cudaGetLastError();
 }
 
-template <typename T>
-cudaError_t launch_dt(const Scratch &s, const LatticeDesc &d, const void *val, int c0, int c1, const SpmvOp &op,
-                      cudaStream_t st)
+// One sweep step: colour c0 of a strictly lower / upper part.
+template <typename T, int EPI, int DIM, int PART>
+cudaError_t launch_sweep(const Scratch &s, const LatticeDesc &d, const void *val, int c0, const SpmvOp &op,
+                         cudaStream_t st)
 {
-    switch (op.epi) {
-    case EPI_SET: return launch_t<T, EPI_SET>(s, d, val, c0, c1, op, st);
-    case EPI_ADD: return launch_t<T, EPI_ADD>(s, d, val, c0, c1, op, st);
-    case EPI_DOT_X: return launch_t<T, EPI_DOT_X>(s, d, val, c0, c1, op, st);
-    case EPI_RESID: return launch_t<T, EPI_RESID>(s, d, val, c0, c1, op, st);
-    case EPI_SGS_F: return launch_t<T, EPI_SGS_F>(s, d, val, c0, c1, op, st);
-    case EPI_SGS_B: return launch_t<T, EPI_SGS_B>(s, d, val, c0, c1, op, st);
-    case EPI_ILU_F: return launch_t<T, EPI_ILU_F>(s, d, val, c0, c1, op, st);
-    case EPI_ILU_B: return launch_t<T, EPI_ILU_B>(s, d, val, c0, c1, op, st);
-    default: return cudaErrorInvalidValue;
+    cudaError_t e = cudaErrorNotSupported;
+    static_for<0, (DIM == 3 ? 8 : 4)>([&](auto cc) {
+        constexpr int C = decltype(cc)::value;
+        if (c0 == C) e = launch_k<T, EPI, DIM, PART, C>(s, d, val, c0, c0 + 1, op, st);
+    });
+    return e;
+}
+
+template <typename T, int DIM>
+cudaError_t launch_dim(const Scratch &s, const LatticeDesc &d, const void *val, int c0, int c1, const SpmvOp &op,
+                       cudaStream_t st)
+{
+    const int part = d.part;
+    if (part == 2) {
+        switch (op.epi) {
+        case EPI_SET: return launch_k<T, EPI_SET, DIM, 2, -1>(s, d, val, c0, c1, op, st);
+        case EPI_ADD: return launch_k<T, EPI_ADD, DIM, 2, -1>(s, d, val, c0, c1, op, st);
+        case EPI_DOT_X: return launch_k<T, EPI_DOT_X, DIM, 2, -1>(s, d, val, c0, c1, op, st);
+        case EPI_RESID: return launch_k<T, EPI_RESID, DIM, 2, -1>(s, d, val, c0, c1, op, st);
+        default: return cudaErrorNotSupported;
+        }
     }
+    if (c1 != c0 + 1) return cudaErrorNotSupported;
+    if (part == 0 && op.epi == EPI_SGS_F) return launch_sweep<T, EPI_SGS_F, DIM, 0>(s, d, val, c0, op, st);
+    if (part == 0 && op.epi == EPI_ILU_F) return launch_sweep<T, EPI_ILU_F, DIM, 0>(s, d, val, c0, op, st);
+    if (part == 1 && op.epi == EPI_SGS_B) return launch_sweep<T, EPI_SGS_B, DIM, 1>(s, d, val, c0, op, st);
+    if (part == 1 && op.epi == EPI_ILU_B) return launch_sweep<T, EPI_ILU_B, DIM, 1>(s, d, val, c0, op, st);
+    return cudaErrorNotSupported;
 }
 
 }  // namespace
 
+// cudaErrorNotSupported: no lattice kernel for this part, epilogue and
+// colour range (the caller then runs the CSR path).
 cudaError_t launch_lattice(const Scratch &s, int dtype, const LatticeDesc &d, const void *val, int c0, int c1,
                            const SpmvOp &op, cudaStream_t st)
 {
     if (c0 < 0 || c1 > d.ncol || c0 >= c1) return cudaErrorInvalidValue;
-    return dtype == 0 ? launch_dt<double>(s, d, val, c0, c1, op, st) : launch_dt<float>(s, d, val, c0, c1, op, st);
+    if (d.ncol == 8)
+        return dtype == 0 ? launch_dim<double, 3>(s, d, val, c0, c1, op, st)
+                          : launch_dim<float, 3>(s, d, val, c0, c1, op, st);
+    return dtype == 0 ? launch_dim<double, 2>(s, d, val, c0, c1, op, st)
+                      : launch_dim<float, 2>(s, d, val, c0, c1, op, st);
 }
+
+// The host's slot table (the kernels use the same one at compile time).
+SlotTab lattice_slots(int dim, int c, int part) { return slot_table(dim, c, part); }
 
 }  // namespace b200
 
@@ -188,31 +318,14 @@ bool perm_ok(int mx, int my, int mz, const std::vector<int> &perm, const std::ve
     return k == perm.size() && (size_t)off[ncol] == k;
 }
 
-// Slots of colour c for a part: 0 strictly lower (neighbour colour < c),
-// 1 strictly upper (> c), 2 all positions with the diagonal.
+// Slots of colour c for a part, packed for the descriptor (the table the kernels use).
 static std::vector<unsigned> slots(int c, int dim3, int part)
 {
-    struct S {
-        int cp, dz, dy, dx;
-    };
-    std::vector<S> v;
-    for (int dz = dim3 ? -1 : 0; dz <= (dim3 ? 1 : 0); ++dz)
-        for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-                const int m = (dx != 0) + 2 * (dy != 0) + 4 * (dz != 0);
-                const int cp = c ^ m;
-                if ((part == 0 && cp < c) || (part == 1 && cp > c) || part == 2) v.push_back({cp, dz, dy, dx});
-            }
-    std::sort(v.begin(), v.end(), [](const S &a, const S &b) {
-        if (a.cp != b.cp) return a.cp < b.cp;
-        if (a.dz != b.dz) return a.dz < b.dz;
-        if (a.dy != b.dy) return a.dy < b.dy;
-        return a.dx < b.dx;
-    });
+    const b200::SlotTab t = b200::lattice_slots(dim3 ? 3 : 2, c, part);
     std::vector<unsigned> out;
-    for (const S &s : v)
-        out.push_back((unsigned)(s.dx + 1) | (unsigned)(s.dy + 1) << 2 | (unsigned)(s.dz + 1) << 4 |
-                      (unsigned)s.cp << 8);
+    for (int k = 0; k < t.n; ++k)
+        out.push_back((unsigned)(t.dx[k] + 1) | (unsigned)(t.dy[k] + 1) << 2 | (unsigned)(t.dz[k] + 1) << 4 |
+                      (unsigned)t.cp[k] << 8);
     return out;
 }
 

@@ -195,38 +195,22 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
     }
     SK(launch_cg_start(sc, dt, n, pc, w.r, invd, w.z, w.p, ctx->st, ctx->stream));
     ctx->launches += 1;
-    // Jacobi on a stencil layout: the direction update p = beta p + D^-1 r
-    // is formed inside the next product's gathers (two launches per
-    // iteration instead of three); p alternates between w.p and w.z, and the
-    // first product, with beta = 0 from state_init, forms p = z of the start
-    const bool fold = pc == 1 && w.z && spmv_can_fold(A) && !std::getenv("B200LA_NOFOLD");
-    int parity = 0;
     unsigned long long cond = 0;   // loop condition of the device-side while node (when captured in one)
 
     auto iteration = [&]() -> int {
-        void *p_old = (fold && parity) ? w.z : w.p, *p_cur = p_old;
         // Ap = A p; alpha = rho / (Ap.p)                       (cg.cc:219-220)
         SpmvOp o;
         o.epi = EPI_DOT_X;
         o.fin = FIN_CG_ALPHA;
-        o.x = p_old;
+        o.x = w.p;
         o.y = w.Ap;
         o.st = ctx->st;
         o.gate = gate;
-        if (fold) {
-            p_cur = parity ? w.p : w.z;
-            o.fold_p = p_cur;
-            o.fold_r = w.r;
-            o.fold_d = invd;
-            o.fold_beta = &ctx->st->beta;
-            parity ^= 1;
-        }
         int r2 = spmv_run(ctx, A, A->all, o);
         if (r2) return r2;
         // x += alpha p; r -= alpha Ap; res = ||r||; Check       (cg.cc:221-230)
-        SK(launch_cg_update(sc, dt, n, pc, x, w.r, p_cur, w.Ap, invd, ctx->st, ctx->stream, cond));
+        SK(launch_cg_update(sc, dt, n, pc, x, w.r, w.p, w.Ap, invd, ctx->st, ctx->stream, cond));
         ctx->launches += 1;
-        if (fold) return B200LA_OK;   // p = beta p + z happens in the next product (cg.cc:241)
         if (pc == 2) {
             // z = M^-1 r; gamma = r.z; beta = gamma / rho     (cg.cc:236-240)
             r2 = precond_apply_async(ctx, P, w.r, w.z, gate);
@@ -240,8 +224,7 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
         return B200LA_OK;
     };
 
-    // an even batch keeps the folded direction's buffers in step across batches
-    const int K = fold ? (batch_size() + 1) / 2 * 2 : batch_size();
+    const int K = batch_size();
     cudaGraphExec_t exec = nullptr;
     int nodes = 0;
     const bool no_graph = std::getenv("B200LA_NOGRAPH") != nullptr;
@@ -261,8 +244,7 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
     }
     const bool loop = !no_graph && loop_policy();
     const std::vector<const void *> key = {A, P, b, x, w.r, w.p, w.Ap, w.z, (const void *)(intptr_t)K,
-                                           (const void *)(intptr_t)pc, ctx->stream, (const void *)(intptr_t)fold,
-                                           (const void *)(intptr_t)loop};
+                                           (const void *)(intptr_t)pc, ctx->stream, (const void *)(intptr_t)loop};
     auto batch = [&]() -> int {
         for (int k = 0; k < K; ++k) {
             int r2 = iteration();
@@ -389,8 +371,8 @@ extern "C" int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_
     } guard{A32, own32};
     const size_t v8 = ((8 * (size_t)std::max(n, 1) + 255) / 256) * 256, v4 = ((4 * (size_t)std::max(n, 1) + 255) / 256) * 256;
     void *wk;
-    // r (f64), invd64 scratch (f64), invd32, rl, cl, and the inner CG's r, p, Ap, second p (f32)
-    int rc = ctx_work(ctx, 2 * v8 + 7 * v4, &wk);
+    // r (f64), invd64 scratch (f64), rl, cl, and the inner CG's r, p, Ap (f32)
+    int rc = ctx_work(ctx, 2 * v8 + 6 * v4, &wk);
     if (rc) return rc;
     char *base = static_cast<char *>(wk);
     double *r = reinterpret_cast<double *>(base);
@@ -398,7 +380,7 @@ extern "C" int b200la_mpir(b200la_ctx *ctx, const b200la_csr *A64, const b200la_
     float *invd32 = nullptr;   // the operator's cached FP32 Jacobi scaling (below)
     float *rl = reinterpret_cast<float *>(base + 2 * v8 + v4);
     float *cl = reinterpret_cast<float *>(base + 2 * v8 + 2 * v4);
-    CgWork w{base + 2 * v8 + 3 * v4, base + 2 * v8 + 4 * v4, base + 2 * v8 + 5 * v4, base + 2 * v8 + 6 * v4};
+    CgWork w{base + 2 * v8 + 3 * v4, base + 2 * v8 + 4 * v4, base + 2 * v8 + 5 * v4, nullptr};
     const long long l0 = ctx->launches;
 
     // FP32 Jacobi from the FP64 diagonal (1/a_ii rounded once), made at the

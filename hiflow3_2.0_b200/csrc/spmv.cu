@@ -477,24 +477,6 @@ void launch_tile(int grid, const CsrView &A, const Seg &seg, const SpmvOp &op, c
         <<<grid, kBlock, ST * TileSmem<CAP>::template stage_bytes<T>() + ST * 8, st>>>(A, seg, op, s);
 }
 
-// Row epilogue of the stencil kernels; with FOLD (EPI_DOT_X only) the row's
-// own new direction is formed from the same inputs as at every gather, stored,
-// and used in the dot: y_i = s, p_new_i = beta p_i + r_i d_i, acc += p_new_i s.
-template <typename T, int EPI, bool FOLD>
-__device__ __forceinline__ void fold_epilogue(int r, T s, const SpmvOp &op, T beta, double &acc)
-{
-    if constexpr (FOLD) {
-        static_assert(EPI == EPI_DOT_X, "the direction fold goes with the p.Ap epilogue");
-        const T pn = cg_direction(beta, static_cast<const T *>(op.x)[r], static_cast<const T *>(op.fold_r)[r],
-                                  static_cast<const T *>(op.fold_d)[r]);
-        static_cast<T *>(op.fold_p)[r] = pn;
-        static_cast<T *>(op.y)[r] = s;
-        acc += (double)(pn * s);
-    } else {
-        epilogue<T, EPI>(r, s, op, acc);
-    }
-}
-
 template <typename T, int W>
 struct StencilVec;
 template <>
@@ -526,14 +508,10 @@ struct StencilVec<float, 4> {
 // values arrive k-major (three 128- or 256-byte lines per band) with no
 // index of any kind; products are added in column order.  Columns outside
 // [0, n) belong to zero entries and are clamped into range.
-template <typename T, int EPI, int NB, bool FOLD = false>
+template <typename T, int EPI, int NB>
 __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp op, Scratch sc)
 {
     if (gate_closed(op.gate)) return;
-    const T *__restrict__ fr = static_cast<const T *>(op.fold_r);
-    const T *__restrict__ fd = static_cast<const T *>(op.fold_d);
-    T beta = T(0);
-    if constexpr (FOLD) beta = (T)cta_scalar(op.fold_beta);
     // positions per lane and load: FP32 values come in groups of four (one
     // 16-byte load per lane), FP64 one by one
     constexpr int W = stencil_group<T>();
@@ -542,11 +520,7 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
     const V *__restrict__ sv = static_cast<const V *>(A.st_val);
     const T *__restrict__ x = static_cast<const T *>(op.x);
     const uint64_t pol = l2_policy(0);
-    // x at column j, or with FOLD the direction beta p_j + r_j d_j formed at the gather
-    auto gx = [&](int j) -> T {
-        if constexpr (FOLD) return cg_direction(beta, ld_keep(x + j, pol), ld_keep(fr + j, pol), ld_keep(fd + j, pol));
-        else return ld_keep(x + j, pol);
-    };
+    auto gx = [&](int j) -> T { return ld_keep(x + j, pol); };
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     const int nw = gridDim.x * (kBlock / 32);
@@ -604,7 +578,7 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
                 }
             }
         }
-        if (r < n) fold_epilogue<T, EPI, FOLD>(r, s, op, beta, acc);
+        if (r < n) epilogue<T, EPI>(r, s, op, acc);
     }
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
@@ -711,24 +685,37 @@ struct HalfRow<double, NB> {
             av[b][2] = at(hv, q + 1, p, pol);
         }
     }
+    // the three values of band b alone (the same loads as values())
+    static __device__ __forceinline__ void band(const double *__restrict__ hv, int d, int c, int lane, int b,
+                                                uint64_t pol, double (&a)[3])
+    {
+        const int r = (c << 5) + lane;
+        const double *own = hv + (size_t)c * H * 32 + lane;
+        if (b > U) {
+#pragma unroll
+            for (int m = 0; m < 3; ++m) a[m] = ld_stream(own + 32 * (2 + 3 * (b - U - 1) + m), pol);
+        } else if (b == U) {
+            a[0] = at(hv, r - 1, 1, pol);
+            a[1] = ld_stream(own, pol);
+            a[2] = ld_stream(own + 32, pol);
+        } else {
+            const int q = r + d, p = 2 + 3 * (U - 1 - b);
+            a[0] = at(hv, q - 1, p + 2, pol);
+            a[1] = at(hv, q, p + 1, pol);
+            a[2] = at(hv, q + 1, p, pol);
+        }
+    }
 };
 
-template <typename T, int EPI, int NB, bool FOLD = false>
+template <typename T, int EPI, int NB>
 __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op, Scratch sc)
 {
     if (gate_closed(op.gate)) return;
     constexpr int U = (NB - 1) / 2;
-    const T *__restrict__ fr = static_cast<const T *>(op.fold_r);
-    const T *__restrict__ fd = static_cast<const T *>(op.fold_d);
-    T beta = T(0);
-    if constexpr (FOLD) beta = (T)cta_scalar(op.fold_beta);
     const T *__restrict__ x = static_cast<const T *>(op.x);
     const unsigned *__restrict__ mask = A.sh_mask;
     const uint64_t pol = l2_policy(0);
-    auto gx = [&](int j) -> T {
-        if constexpr (FOLD) return cg_direction(beta, ld_keep(x + j, pol), ld_keep(fr + j, pol), ld_keep(fd + j, pol));
-        else return ld_keep(x + j, pol);
-    };
+    auto gx = [&](int j) -> T { return ld_keep(x + j, pol); };
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     const int nw = gridDim.x * (kBlock / 32);
@@ -741,6 +728,41 @@ __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op,
     for (int c = gw; c < nch; c += nw) {
         const int r0 = c << 5, r = r0 + lane;
         const int he = lane == 0 ? r0 - 1 : r0 + 32;
+        if constexpr (sizeof(T) == 8) {
+            // FP64: groups of three bands, their value loads and gathers
+            // issued together (register pressure of one group, not of the row)
+            const bool ident = (__ldg(mask + c) >> lane) & 1u;
+            T s = T(0);
+#pragma unroll
+            for (int b0 = 0; b0 < NB; b0 += 3) {
+                T a[3][3], w[3], h[3];
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb) {
+                    const int b = b0 + bb, d = cen[b];
+                    HalfRow<double, NB>::band(static_cast<const double *>(A.sh_val), d, c, lane, b, pol, a[bb]);
+                    if (ident) {
+                        // identity row: its upper slots serve the neighbours; off-diagonals are zero
+#pragma unroll
+                        for (int m = 0; m < 3; ++m)
+                            if (b != U || m != 1) a[bb][m] = T(0);
+                    }
+                    w[bb] = gx(min(max(r + d, 0), last));
+                    h[bb] = edge ? gx(min(max(he + d, 0), last)) : T(0);
+                }
+#pragma unroll
+                for (int bb = 0; bb < 3; ++bb) {
+                    T left = __shfl_up_sync(0xffffffffu, w[bb], 1);
+                    T right = __shfl_down_sync(0xffffffffu, w[bb], 1);
+                    if (lane == 0) left = h[bb];
+                    if (lane == 31) right = h[bb];
+                    s += a[bb][0] * left;
+                    s += a[bb][1] * w[bb];
+                    s += a[bb][2] * right;
+                }
+            }
+            if (r < n) epilogue<T, EPI>(r, s, op, acc);
+            continue;
+        }
         T av[NB][3];
         HalfRow<T, NB>::values(A.sh_val, cen, c, lane, rows, pol, av);
         if ((__ldg(mask + c) >> lane) & 1u) {
@@ -765,7 +787,7 @@ __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op,
             s += av[b][1] * w;
             s += av[b][2] * right;
         }
-        if (r < n) fold_epilogue<T, EPI, FOLD>(r, s, op, beta, acc);
+        if (r < n) epilogue<T, EPI>(r, s, op, acc);
     }
     if constexpr (reduces<EPI>()) {
         double vv[1] = {acc}, out[1];
@@ -793,18 +815,6 @@ void launch_one_wave(K kern, int &resident, const Scratch &s, int n_rows, const 
 template <typename T, int EPI>
 void launch_epi(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp &op, cudaStream_t st)
 {
-    if constexpr (EPI == EPI_DOT_X) {
-        if (op.fold_p) {
-            // the caller checked spmv_can_fold: a stencil layout over the whole operator
-            static int res_f[4] = {0, 0, 0, 0};
-            const bool half = A.sh_use && A.sh_val;
-            if (half && A.st_nb == 9) launch_one_wave(spmv_half_kernel<T, EPI, 9, true>, res_f[0], s, A.n_rows, A, op, st);
-            else if (half) launch_one_wave(spmv_half_kernel<T, EPI, 3, true>, res_f[1], s, A.n_rows, A, op, st);
-            else if (A.st_nb == 9) launch_one_wave(spmv_stencil_kernel<T, EPI, 9, true>, res_f[2], s, A.n_rows, A, op, st);
-            else launch_one_wave(spmv_stencil_kernel<T, EPI, 3, true>, res_f[3], s, A.n_rows, A, op, st);
-            return;
-        }
-    }
     if constexpr (EPI == EPI_SET || EPI == EPI_ADD || EPI == EPI_DOT_X || EPI == EPI_RESID) {
         if (A.sh_use && A.sh_val && A.st_use && seg.r0 == 0 && seg.r1 == A.n_rows && (A.st_nb == 3 || A.st_nb == 9)) {
             static int res_nb[2] = {0, 0};
