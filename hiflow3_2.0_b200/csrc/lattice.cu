@@ -83,8 +83,10 @@ struct Slots {
 // the sublattice step of an offset: floor((parity + d) / 2)
 __host__ __device__ constexpr int sub_step(int parity, int d) { return parity + d < 0 ? -1 : (parity + d) / 2; }
 
+// f(integral_constant<K>) for K in [K, N): host code (the launch dispatch)
+// and device code (the unrolled slot loops) both use it
 template <int K, int N, class F>
-__device__ __forceinline__ void static_for(F &&f)
+__host__ __device__ __forceinline__ void static_for(F &&f)
 {
     if constexpr (K < N) {
         f(std::integral_constant<int, K>());
