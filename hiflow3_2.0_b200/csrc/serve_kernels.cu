@@ -211,25 +211,41 @@ __device__ __forceinline__ double stencil_row_half(const double *__restrict__ va
     auto at = [&](int q, int p) {
         return q >= 0 ? ld_keep(val + ((size_t)(q >> 5) * H + p) * kChunk + (q & 31), pol) : 0.0;
     };
-    double av[NB][3];
-    av[U][1] = ld_stream(own, pol);
-    av[U][2] = ld_stream(own + 32, pol);
-#pragma unroll
-    for (int ub = 0; ub < U; ++ub)
-#pragma unroll
-        for (int m = 0; m < 3; ++m) av[U + 1 + ub][m] = ld_stream(own + 32 * (2 + 3 * ub + m), pol);
-    av[U][0] = at(i - 1, 1);
-#pragma unroll
-    for (int b = 0; b < U; ++b) {
-        const int q = i + band_offset(DIM, P, b), p = 2 + 3 * (U - 1 - b);
-        av[b][0] = at(q - 1, p + 2);
-        av[b][1] = at(q, p + 1);
-        av[b][2] = at(q + 1, p);
-    }
-    half_identity<NB>(smask, c, lane, av);
+    const bool ident = (__ldg(smask + c) >> lane) & 1u;
     double s = 0.0;
+    // groups of three bands: the values of a group (own upper slots, or the
+    // owners' slots for the lower bands) are loaded together, then its
+    // gathers and products -- the registers of one group, not of the row
 #pragma unroll
-    for (int b = 0; b < NB; ++b) band(s, av[b][0], av[b][1], av[b][2], i, he, band_offset(DIM, P, b), n, lane, gather);
+    for (int b0 = 0; b0 < NB; b0 += 3) {
+        double a[3][3];
+#pragma unroll
+        for (int bb = 0; bb < 3; ++bb) {
+            const int b = b0 + bb;
+            if (b > U) {
+#pragma unroll
+                for (int m = 0; m < 3; ++m) a[bb][m] = ld_stream(own + 32 * (2 + 3 * (b - U - 1) + m), pol);
+            } else if (b == U) {
+                a[bb][0] = at(i - 1, 1);
+                a[bb][1] = ld_stream(own, pol);
+                a[bb][2] = ld_stream(own + 32, pol);
+            } else {
+                const int q = i + band_offset(DIM, P, b), p = 2 + 3 * (U - 1 - b);
+                a[bb][0] = at(q - 1, p + 2);
+                a[bb][1] = at(q, p + 1);
+                a[bb][2] = at(q + 1, p);
+            }
+            if (ident) {
+                // identity row: its upper slots serve the neighbours; off-diagonals are zero
+#pragma unroll
+                for (int m = 0; m < 3; ++m)
+                    if (b != U || m != 1) a[bb][m] = 0.0;
+            }
+        }
+#pragma unroll
+        for (int bb = 0; bb < 3; ++bb)
+            band(s, a[bb][0], a[bb][1], a[bb][2], i, he, band_offset(DIM, P, b0 + bb), n, lane, gather);
+    }
     return s;
 }
 
