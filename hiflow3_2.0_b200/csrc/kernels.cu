@@ -127,7 +127,10 @@ __device__ __forceinline__ void cg_update_elem(T alpha, T &x, T &r, T p, T ap, T
     if (jac) rz += r * (r * d);
 }
 
-template <typename T>
+// COND: the last CTA also sets the conditional handle cond (a kernel with the
+// device-side graph call is a separate instance: profilers replay only the
+// plain one, which the host-polled batches use)
+template <typename T, bool COND>
 __global__ void __launch_bounds__(kBlock) cg_update_kernel(int n, int precond, T *__restrict__ x, T *__restrict__ r,
                                                            const T *__restrict__ p, const T *__restrict__ Ap,
                                                            const T *__restrict__ invd, DevState *st, Scratch sc,
@@ -183,7 +186,7 @@ __global__ void __launch_bounds__(kBlock) cg_update_kernel(int n, int precond, T
             st->beta = g / st->rho;
             st->rho = g;
         }
-        if (cond) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, status == kIterate ? 1u : 0u);
+        if constexpr (COND) cudaGraphSetConditional((cudaGraphConditionalHandle)cond, status == kIterate ? 1u : 0u);
     }
 }
 
@@ -381,8 +384,12 @@ cudaError_t launch_cg_update(const Scratch &s, int dtype, int n, int precond, vo
                              unsigned long long cond)
 {
     const int g = stream_grid(&s, n);
-    B200_DISPATCH(dtype, cg_update_kernel<T><<<g, kBlock, 0, stm>>>(n, precond, (T *)x, (T *)r, (const T *)p,
-                                                                    (const T *)Ap, (const T *)invd, st, s, cond));
+    if (cond)
+        B200_DISPATCH(dtype, cg_update_kernel<T, true><<<g, kBlock, 0, stm>>>(n, precond, (T *)x, (T *)r, (const T *)p,
+                                                                          (const T *)Ap, (const T *)invd, st, s, cond));
+    else
+        B200_DISPATCH(dtype, cg_update_kernel<T, false><<<g, kBlock, 0, stm>>>(
+                                 n, precond, (T *)x, (T *)r, (const T *)p, (const T *)Ap, (const T *)invd, st, s, 0ull));
     return cudaGetLastError();
 }
 

@@ -74,6 +74,11 @@ enum Epi : int {
     EPI_SGS_B = 5,   // y_i = (y_i * d2_i + s) * d1_i      (MC-SGS diagonal + backward, d2 = -d)
     EPI_ILU_F = 6,   // y_i = -(-b_i + s)                  (ILU forward, unit L)
     EPI_ILU_B = 7,   // y_i = (-y_i + s) * d1_i            (ILU backward, d1 = -1/u_ii)
+    // the last colour's forward step followed by its backward step, which has
+    // no couplings (nothing lies right of the last colour): the two epilogues
+    // in turn, with the backward sum 0 -- the same roundings as two launches
+    EPI_SGS_FB = 8,  // y_i = (-b_i + s) * d1_i;  y_i = (y_i * d2_i + 0) * d1_i
+    EPI_ILU_FB = 9,  // y_i = -(-b_i + s);        y_i = (-y_i + 0) * d1_i
 };
 
 // What the last CTA does with a reduced value v (EPI_DOT_X / EPI_RESID).

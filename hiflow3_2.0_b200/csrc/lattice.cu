@@ -241,6 +241,10 @@ cudaError_t launch_dim(const Scratch &s, const LatticeDesc &d, const void *val, 
     if (c1 != c0 + 1) return cudaErrorNotSupported;
     if (part == 0 && op.epi == EPI_SGS_F) return launch_sweep<T, EPI_SGS_F, DIM, 0>(s, d, val, c0, op, st);
     if (part == 0 && op.epi == EPI_ILU_F) return launch_sweep<T, EPI_ILU_F, DIM, 0>(s, d, val, c0, op, st);
+    if (part == 0 && c0 == d.ncol - 1 && op.epi == EPI_SGS_FB)
+        return launch_k<T, EPI_SGS_FB, DIM, 0, (DIM == 3 ? 7 : 3)>(s, d, val, c0, c1, op, st);
+    if (part == 0 && c0 == d.ncol - 1 && op.epi == EPI_ILU_FB)
+        return launch_k<T, EPI_ILU_FB, DIM, 0, (DIM == 3 ? 7 : 3)>(s, d, val, c0, c1, op, st);
     if (part == 1 && op.epi == EPI_SGS_B) return launch_sweep<T, EPI_SGS_B, DIM, 1>(s, d, val, c0, op, st);
     if (part == 1 && op.epi == EPI_ILU_B) return launch_sweep<T, EPI_ILU_B, DIM, 1>(s, d, val, c0, op, st);
     return cudaErrorNotSupported;

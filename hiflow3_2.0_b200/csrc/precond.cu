@@ -13,6 +13,7 @@
 #include "b200la_internal.h"
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -264,20 +265,28 @@ int precond_apply_async(b200la_ctx *ctx, const b200la_precond *P, const void *r,
     }
     if (P->use_syncfree) return syncfree_apply(ctx, P, r, z, gate);
     const bool sgs = (P->kind == B200LA_PRECOND_MCSGS);
+    // on the lattice layout the last block's backward step has no couplings:
+    // it runs in the epilogue of that block's forward step (one launch less)
+    const int nb = P->nblocks;
+    int c0, c1;
+    const bool fuse = nb > 1 && P->L->lt && P->U->lt && P->U->lt->ncol == nb && P->U->lt->col[nb - 1].nslot == 0 &&
+                      lattice_segment(P->L, P->L->segs[nb], &c0, &c1) && !std::getenv("B200LA_NOFUSE_LAST");
     // forward sweep over the blocks: z_i from r_i and the already-final z of earlier blocks
-    for (int b = 0; b < P->nblocks; ++b) {
+    for (int b = 0; b < nb; ++b) {
         SpmvOp op;
         op.epi = sgs ? EPI_SGS_F : EPI_ILU_F;
+        if (fuse && b == nb - 1) op.epi = sgs ? EPI_SGS_FB : EPI_ILU_FB;
         op.x = z;
         op.y = z;
         op.b = r;
         op.d1 = P->iDv;
+        op.d2 = P->Dv;
         op.gate = gate;
         int rc = spmv_run(ctx, P->L, P->L->segs[1 + b], op);
         if (rc) return rc;
     }
     // diagonal step folded into the backward sweep, blocks in reverse order
-    for (int b = P->nblocks - 1; b >= 0; --b) {
+    for (int b = nb - 1 - (fuse ? 1 : 0); b >= 0; --b) {
         SpmvOp op;
         op.epi = sgs ? EPI_SGS_B : EPI_ILU_B;
         op.x = z;

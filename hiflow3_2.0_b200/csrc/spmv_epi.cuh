@@ -53,6 +53,13 @@ __device__ __forceinline__ void epilogue(int r, T s, const SpmvOp &op, double &a
         y[r] = -(-static_cast<const T *>(op.b)[r] + s);
     } else if constexpr (EPI == EPI_ILU_B) {
         y[r] = (-y[r] + s) * static_cast<const T *>(op.d1)[r];
+    } else if constexpr (EPI == EPI_SGS_FB) {
+        const T d1 = static_cast<const T *>(op.d1)[r];
+        const T f = (-static_cast<const T *>(op.b)[r] + s) * d1;
+        y[r] = (f * static_cast<const T *>(op.d2)[r] + T(0)) * d1;
+    } else if constexpr (EPI == EPI_ILU_FB) {
+        const T f = -(-static_cast<const T *>(op.b)[r] + s);
+        y[r] = (-f + T(0)) * static_cast<const T *>(op.d1)[r];
     }
 }
 
