@@ -210,6 +210,10 @@ struct SpmvOp {
     double *dot_out = nullptr;
     DevState *st = nullptr;
     const int *gate = nullptr;    // skip the launch body when *gate != 0
+    // launch as a programmatic dependent of the previous kernel on the stream
+    // (lattice colour sweeps: the value loads overlap the previous colour's
+    // tail; every read of what that colour wrote waits for its completion)
+    int pdl = 0;
 };
 
 struct Scratch {

@@ -94,6 +94,12 @@ __host__ __device__ __forceinline__ void static_for(F &&f)
     }
 }
 
+// Programmatic dependent launch: let the next launch on the stream start its
+// CTAs now, and wait for the previous launch's completion (and memory) --
+// both no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 // One 32-row chunk of colour C (chunk g of the launch's numbering): each lane
 // forms its row's lattice position, one row base per neighbour colour, and
 // then, slot by slot, a column that is that base plus compile-time multiples
@@ -136,6 +142,12 @@ __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__r
         constexpr int cnt = S.n - k0 < kLatGroup ? S.n - k0 : kLatGroup;
         T a[kLatGroup], w[kLatGroup];
         static_for<0, cnt>([&](auto jj) {
+            constexpr int j = decltype(jj)::value;
+            a[j] = ld_stream(v + 32 * (k0 + j), pol);
+        });
+        // x (what earlier colours wrote) only after the previous launch completed
+        if constexpr (decltype(gg)::value == 0) grid_dependency_wait();
+        static_for<0, cnt>([&](auto jj) {
             constexpr int j = decltype(jj)::value, k = k0 + j;
             constexpr int dx = S.dx[k], dy = S.dy[k], dz = S.dz[k], cp = S.cp[k];
             constexpr int ex = sub_step(px, dx), ey = sub_step(py, dy), ez = sub_step(pz, dz);
@@ -150,7 +162,6 @@ __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__r
             if constexpr (dy > 0) ok = ok && yhi;
             if constexpr (dz < 0) ok = ok && zlo;
             if constexpr (dz > 0) ok = ok && zhi;
-            a[j] = ld_stream(v + 32 * k, pol);
             w[j] = ok ? ld_keep(x + col, pol) : T(0);
         });
         static_for<0, cnt>([&](auto jj) {
@@ -158,6 +169,7 @@ __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__r
             s += a[j] * w[j];
         });
     });
+    if constexpr (S.n == 0) grid_dependency_wait();   // the epilogue reads and writes vectors
     if (active) epilogue<T, EPI>(L.row0 + t, s, op, acc);
 }
 
@@ -169,6 +181,7 @@ __global__ void __launch_bounds__(kBlock) lattice_kernel(const __grid_constant__
                                                          Scratch sc)
 {
     if (gate_closed(op.gate)) return;
+    grid_dependents_launch();
     const T *__restrict__ x = static_cast<const T *>(op.x);
     const uint64_t pol = l2_policy(0);
     const int lane = threadIdx.x & 31;
@@ -207,8 +220,20 @@ cudaError_t launch_k(const Scratch &s, const LatticeDesc &d, const void *val, in
     int grid = (chunks + kBlock / 32 - 1) / (kBlock / 32);
     grid = std::min(grid, std::min(s.num_sms * std::max(resident, 1), kMaxGrid));
     grid = std::max(grid, 1);
-    kern<<<grid, kBlock, 0, st>>>(d, static_cast<const T *>(val), c0, c1, op, s);
-    return cudaGetLastError();
+    if (!op.pdl) {
+        kern<<<grid, kBlock, 0, st>>>(d, static_cast<const T *>(val), c0, c1, op, s);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kBlock);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, d, static_cast<const T *>(val), c0, c1, op, s);
 }
 
 // One sweep step: colour c0 of a strictly lower / upper part.

@@ -271,11 +271,16 @@ int precond_apply_async(b200la_ctx *ctx, const b200la_precond *P, const void *r,
     int c0, c1;
     const bool fuse = nb > 1 && P->L->lt && P->U->lt && P->U->lt->ncol == nb && P->U->lt->col[nb - 1].nslot == 0 &&
                       lattice_segment(P->L, P->L->segs[nb], &c0, &c1) && !std::getenv("B200LA_NOFUSE_LAST");
+    // lattice sweeps after the first launch as programmatic dependents of the
+    // previous one (B200LA_PDL=0: plain stream order)
+    const char *pe = std::getenv("B200LA_PDL");
+    const int pdl = (P->L->lt && P->U->lt && (!pe || std::atoi(pe) != 0)) ? 1 : 0;
     // forward sweep over the blocks: z_i from r_i and the already-final z of earlier blocks
     for (int b = 0; b < nb; ++b) {
         SpmvOp op;
         op.epi = sgs ? EPI_SGS_F : EPI_ILU_F;
         if (fuse && b == nb - 1) op.epi = sgs ? EPI_SGS_FB : EPI_ILU_FB;
+        op.pdl = b > 0 ? pdl : 0;   // the first waits for the whole stream (the gate is read before any wait)
         op.x = z;
         op.y = z;
         op.b = r;
@@ -289,6 +294,7 @@ int precond_apply_async(b200la_ctx *ctx, const b200la_precond *P, const void *r,
     for (int b = nb - 1 - (fuse ? 1 : 0); b >= 0; --b) {
         SpmvOp op;
         op.epi = sgs ? EPI_SGS_B : EPI_ILU_B;
+        op.pdl = pdl;
         op.x = z;
         op.y = z;
         op.d1 = P->iDv;

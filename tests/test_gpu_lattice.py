@@ -163,3 +163,48 @@ def test_non_grid_operator_keeps_csr(pf, b200, golden, monkeypatch):
     Mq.sort_indices()
     P = build(b200, pf, Mq.indptr, Mq.indices, Mq.data, True, monkeypatch)
     assert P.A_perm.info()["storage"] != "lattice"
+
+
+@pytest.mark.parametrize("kind", ["sgs", "ilu"])
+def test_last_colour_fused_step_is_bitwise(pf, b200, monkeypatch, kind):
+    """The last colour's backward step (no couplings) runs in the epilogue of
+    its forward step: the same roundings as the two separate launches."""
+    row, col, val = b200.q1_assemble(3, 13, 0, np.exp(np.random.default_rng(4).normal(0.0, 1.0, 13 ** 3)))
+    n = len(row) - 1
+    P = build(b200, pf, row, col, val, True, monkeypatch, kind=kind)
+    r = np.random.default_rng(8).uniform(-1, 1, n)
+    out = []
+    for flag in (None, "1"):
+        if flag:
+            monkeypatch.setenv("B200LA_NOFUSE_LAST", flag)
+        z = pf.vector(n)
+        P.ApplyPreconditioner(pf.vector(r), z)
+        out.append(z.numpy())
+    monkeypatch.delenv("B200LA_NOFUSE_LAST")
+    assert np.array_equal(out[0].view(np.uint64), out[1].view(np.uint64))
+
+
+def test_programmatic_launch_sweeps_are_bitwise(pf, b200, monkeypatch):
+    """Colour sweeps after the first launch as programmatic dependents (their
+    value loads overlap the previous colour; the gathers wait for it): the
+    same bits as plain stream order, in a single apply and inside PCG."""
+    row, col, val = b200.q1_assemble(3, 16)
+    b = b200.q1_rhs(3, 3, 16)
+    n = len(row) - 1
+    P = build(b200, pf, row, col, val, True, monkeypatch)
+    r = np.random.default_rng(6).uniform(-1, 1, n)
+    out = []
+    for flag in ("1", "0"):
+        monkeypatch.setenv("B200LA_PDL", flag)
+        z = pf.vector(n)
+        P.ApplyPreconditioner(pf.vector(r), z)
+        cg = b200.CG(pf)
+        cg.SetupOperator(P.A_perm)
+        cg.SetupPreconditioner(P)
+        cg.InitControl(1000, 0.0, 1e-8, 1e6)
+        x = pf.vector(n)
+        assert cg.Solve(pf.vector(b[P.perm]), x) == b200.SUCCESS_REL
+        out.append((z.numpy(), cg.iter(), x.numpy()))
+    monkeypatch.delenv("B200LA_PDL")
+    assert np.array_equal(out[0][0], out[1][0]) and out[0][1] == out[1][1]
+    assert np.array_equal(out[0][2], out[1][2])
