@@ -156,6 +156,12 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned by
         : "memory");
 }
 
+// Programmatic dependent launch: let the next launch on the stream start its
+// CTAs now, and wait for the previous launch's completion (and memory) --
+// both no-ops for a kernel launched without the attribute.
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;"); }
+
 // True when the stop-state word *gate is set (a solver's IterateControl
 // state has left "iterate").  One thread per CTA reads it (through L2) and
 // broadcasts it: a load by every thread of the grid on one address would

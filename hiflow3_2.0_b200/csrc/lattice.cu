@@ -11,19 +11,24 @@
 // 12 (nnz - n) bytes with indices to 8 x 26 bytes per row, and the coloured
 // operator from 12 nnz + 4 n to 8 x 27 bytes per row.
 //
-// Set-up (host): lattice_grid() reads the node grid off row 0's columns,
-// lattice_perm_ok() checks that the colouring is the parity colouring, and
-// lattice_values() places every CSR entry of a part (strictly lower, strictly
+// Set-up (host): lattice::grid() reads the node grid off row 0's columns,
+// lattice::perm_ok() checks that the colouring is the parity colouring, and
+// lattice::values() places every CSR entry of a part (strictly lower, strictly
 // upper, or all) into its neighbour slot, failing on any entry that is not a
 // lattice neighbour of its row or that breaks the slot order -- the caller
 // then keeps the CSR path.  Products are added in slot order, which is the
 // row's CSR (ascending column) order; absent neighbours add nothing.
+//
+// Kernels: one instance per colour and part, so the slot table is a
+// compile-time constant (neighbour offsets, neighbour colours, which grid
+// bounds to test); the colour sweeps after the first launch of an apply run
+// as programmatic dependents of the previous one (value loads first, then
+// griddepcontrol.wait before anything an earlier colour wrote).
 #include "b200la.h"
 #include "b200la_internal.h"
 #include "spmv_epi.cuh"
 
 #include <algorithm>
-#include <array>
 #include <cstdlib>
 #include <type_traits>
 #include <vector>
@@ -93,12 +98,6 @@ __host__ __device__ __forceinline__ void static_for(F &&f)
         static_for<K + 1, N>(f);
     }
 }
-
-// Programmatic dependent launch: let the next launch on the stream start its
-// CTAs now, and wait for the previous launch's completion (and memory) --
-// both no-ops for a kernel launched without the attribute.
-__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
-__device__ __forceinline__ void grid_dependents_launch() { asm volatile("griddepcontrol.launch_dependents;"); }
 
 // One 32-row chunk of colour C (chunk g of the launch's numbering): each lane
 // forms its row's lattice position, one row base per neighbour colour, and
