@@ -130,6 +130,22 @@ __device__ __forceinline__ int ld_stream(const int *a, uint64_t pol)
     asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;" : "=r"(v) : "l"(a), "l"(pol));
     return v;
 }
+// Coherent (not .nc) loads with an L2 policy: for data that a kernel still
+// running when this one started -- a programmatic-launch predecessor -- writes
+// before the grid dependency wait; the read-only path may not see such writes.
+__device__ __forceinline__ double ld_coherent(const double *a, uint64_t pol)
+{
+    double v;
+    asm volatile("ld.global.L2::cache_hint.f64 %0, [%1], %2;" : "=d"(v) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+__device__ __forceinline__ float ld_coherent(const float *a, uint64_t pol)
+{
+    float v;
+    asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(a), "l"(pol) : "memory");
+    return v;
+}
+
 __device__ __forceinline__ double ld_keep(const double *a, uint64_t pol)
 {
     double v;

@@ -195,7 +195,6 @@ __global__ void cg_pupdate_kernel(int n, int precond, T *__restrict__ p, const T
                                   const T *__restrict__ invd, const T *__restrict__ z, DevState *st)
 {
     if (gate_closed(&st->status)) return;
-    grid_dependents_launch();   // the next product may start streaming its values
     using V = typename Vec16<T>::type;
     constexpr int W = Vec16<T>::W;
     const T beta = (T)cta_scalar(&st->beta);

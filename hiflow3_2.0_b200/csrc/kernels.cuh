@@ -211,8 +211,9 @@ struct SpmvOp {
     DevState *st = nullptr;
     const int *gate = nullptr;    // skip the launch body when *gate != 0
     // launch as a programmatic dependent of the previous kernel on the stream
-    // (lattice colour sweeps: the value loads overlap the previous colour's
-    // tail; every read of what that colour wrote waits for its completion)
+    // (lattice colour sweeps only: the value loads overlap the previous
+    // colour's tail; every read of what that colour wrote comes after the
+    // grid dependency wait, through coherent loads)
     int pdl = 0;
 };
 

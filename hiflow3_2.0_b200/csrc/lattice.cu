@@ -161,7 +161,7 @@ __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__r
             if constexpr (dy > 0) ok = ok && yhi;
             if constexpr (dz < 0) ok = ok && zlo;
             if constexpr (dz > 0) ok = ok && zhi;
-            w[j] = ok ? ld_keep(x + col, pol) : T(0);
+            w[j] = ok ? ld_coherent(x + col, pol) : T(0);
         });
         static_for<0, cnt>([&](auto jj) {
             constexpr int j = decltype(jj)::value;

@@ -197,10 +197,6 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
     ctx->launches += 1;
     unsigned long long cond = 0;   // loop condition of the device-side while node (when captured in one)
 
-    // the product as a programmatic dependent of the direction update before
-    // it: its value stream starts while that kernel finishes (B200LA_PDL_CG=0: off)
-    const char *pdl_env = std::getenv("B200LA_PDL_CG");
-    const int pdl = (!pdl_env || std::atoi(pdl_env) != 0) ? 1 : 0;
     auto iteration = [&]() -> int {
         // Ap = A p; alpha = rho / (Ap.p)                       (cg.cc:219-220)
         SpmvOp o;
@@ -210,7 +206,6 @@ static int cg_core(b200la_ctx *ctx, const b200la_csr *A, const b200la_precond *P
         o.y = w.Ap;
         o.st = ctx->st;
         o.gate = gate;
-        o.pdl = pdl;
         int r2 = spmv_run(ctx, A, A->all, o);
         if (r2) return r2;
         // x += alpha p; r -= alpha Ap; res = ||r||; Check       (cg.cc:221-230)

@@ -540,7 +540,6 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
             T a[G * W];
 #pragma unroll
             for (int g = 0; g < G; ++g) StencilVec<T, W>::load(v + 32 * g, pol, a + W * g);
-            grid_dependency_wait();   // x and y only after the previous launch (when launched as its dependent)
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
                 const int d = cen[b];
@@ -563,7 +562,6 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
                 for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
                     for (int m = 0; m < 3; ++m) StencilVec<T, W>::load(v + 32 * (3 * (b0 + bb) + m), pol, a + 3 * bb + m);
-                if (b0 == 0) grid_dependency_wait();
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb) {
                     const int d = cen[b0 + bb];
@@ -712,7 +710,7 @@ struct HalfRow<double, NB> {
 };
 
 template <typename T, int EPI, int NB>
-__global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op, Scratch sc)
+__global__ void __launch_bounds__(kBlock, (sizeof(T) == 8 ? 5 : 1)) spmv_half_kernel(CsrView A, SpmvOp op, Scratch sc)
 {
     if (gate_closed(op.gate)) return;
     constexpr int U = (NB - 1) / 2;
@@ -751,7 +749,6 @@ __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op,
                             if (b != U || m != 1) a[bb][m] = T(0);
                     }
                 }
-                if (b0 == 0) grid_dependency_wait();
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb) {
                     const int d = cen[b0 + bb];
@@ -774,7 +771,6 @@ __global__ void __launch_bounds__(kBlock) spmv_half_kernel(CsrView A, SpmvOp op,
         }
         T av[NB][3];
         HalfRow<T, NB>::values(A.sh_val, cen, c, lane, rows, pol, av);
-        grid_dependency_wait();
         if ((__ldg(mask + c) >> lane) & 1u) {
             // identity row: its upper slots serve the neighbours; off-diagonals are zero
 #pragma unroll
@@ -819,20 +815,7 @@ void launch_one_wave(K kern, int &resident, const Scratch &s, int n_rows, const 
     const int cap = s.num_sms * resident;
     if (grid > cap) grid = cap;
     if (grid < 1) grid = 1;
-    if (!op.pdl) {
-        kern<<<grid, kBlock, 0, st>>>(A, op, s);
-        return;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(grid);
-    cfg.blockDim = dim3(kBlock);
-    cfg.stream = st;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    cudaLaunchKernelEx(&cfg, kern, A, op, s);
+    kern<<<grid, kBlock, 0, st>>>(A, op, s);
 }
 
 template <typename T, int EPI>

@@ -403,36 +403,3 @@ def test_mpir_jacobi_scaling_follows_value_changes(pf, b200):
     mq.Solve(pf.vector(b), x3)
     assert np.array_equal(x2.numpy(), x3.numpy())
     assert mp.result.iters == mq.result.iters
-
-
-@pytest.mark.parametrize("layout", ["half", "full", "csr"])
-def test_programmatic_launch_of_cg_product_is_bitwise(pf, b200, monkeypatch, layout):
-    """The CG product launched as a programmatic dependent of the direction
-    update (its value loads start early; x only after the update completed):
-    the same bits as plain stream order, FP64 CG and the mixed solve."""
-    env = {"half": ("1", "2"), "full": ("0", "2"), "csr": ("0", "0")}[layout]
-    monkeypatch.setenv("B200LA_HALF_STENCIL", env[0])
-    monkeypatch.setenv("B200LA_STENCIL", env[1])
-    row, col, val = b200.q1_assemble(3, 18, 0, np.exp(np.random.default_rng(2).normal(0.0, 1.0, 18 ** 3)))
-    b = b200.q1_rhs(7, 3, 18)
-    n = len(b)
-    out = []
-    for flag in ("1", "0"):
-        monkeypatch.setenv("B200LA_PDL_CG", flag)
-        A = b200.CSR_lMatrix.from_csr(pf, row, col, val)
-        cg = b200.CG(pf)
-        cg.SetupOperator(A)
-        cg.SetupPreconditioner(b200.Preconditioner.Jacobi(pf, A))
-        cg.InitControl(20000, 0.0, 1e-10, 1e6)
-        x = pf.vector(n)
-        assert cg.Solve(pf.vector(b), x) == b200.SUCCESS_REL
-        mp = b200.MPIR(pf)
-        mp.SetupOperator(A)
-        mp.InitControl(50, 0.0, 1e-10, 1e6)
-        xm = pf.vector(n)
-        assert mp.Solve(pf.vector(b), xm) == b200.SUCCESS_REL
-        out.append((cg.iter(), x.numpy(), mp.result.iters, xm.numpy()))
-    for k in ("B200LA_PDL_CG", "B200LA_HALF_STENCIL", "B200LA_STENCIL"):
-        monkeypatch.delenv(k)
-    assert out[0][0] == out[1][0] and out[0][2] == out[1][2]
-    assert np.array_equal(out[0][1], out[1][1]) and np.array_equal(out[0][3], out[1][3])
