@@ -787,9 +787,11 @@ class NativeCoupledMatrix:
         self.pf, self.comm, self.rank, self.dtype = platform, comm, rank, dtype
         self.couplings = LaCouplings(partition, rank, ghosts).setup(transport)
         self.n_local = r1 - r0
+        self.diag_host = (rd, cd, vd)            # the local block, for block preconditioner set-ups
         self.diag = CSR_lMatrix.from_csr(platform, rd, cd, vd, n_cols=self.n_local, dtype=dtype)
         self.offdiag = (CSR_lMatrix.from_csr(platform, ro, co, vo, n_cols=len(ghosts), dtype=dtype)
                         if len(co) else None)
+        self._precs = {}
         cp = self.couplings
         self._go = np.ascontiguousarray(cp.ghost_offsets, np.int32)
         self._bo = np.ascontiguousarray(cp.border_offsets, np.int32)
@@ -825,12 +827,22 @@ class NativeCoupledMatrix:
         return out.value
 
     def CG(self, b, x, precond=None, maxits=100000, abstol=0.0, reltol=1e-10, divtol=1e6):
-        """CG<LAD>::Solve over the coupled rows; precond None or "jacobi"
-        (the Jacobi preconditioner of this rank's diagonal block)."""
+        """CG<LAD>::Solve over the coupled rows, block-Jacobi across ranks:
+        precond None, "jacobi" (the Jacobi preconditioner of this rank's
+        diagonal block) or "mcsgs" (the multicoloured symmetric Gauss-Seidel
+        of the block, PreconditionerMultiColoring on op.diagonal())."""
+        from . import Preconditioner
         P = None
-        if precond == "jacobi":
-            from . import Preconditioner
-            P = Preconditioner.Jacobi(self.pf, self.diag)
+        if precond is not None:
+            if precond not in self._precs:
+                if precond == "jacobi":
+                    self._precs[precond] = Preconditioner.Jacobi(self.pf, self.diag)
+                elif precond == "mcsgs":
+                    self._precs[precond] = Preconditioner.MultiColoringSGS(self.pf, *self.diag_host,
+                                                                           dtype=self.dtype)
+                else:
+                    raise ValueError(f"unknown block preconditioner {precond!r}")
+            P = self._precs[precond]
         ctl, res = Control(maxits, abstol, reltol, divtol), Result()
         self.pf.check(lib().b200la_coupled_cg(self.pf.h, self.h, P.h if P is not None else None, b.ptr, x.ptr,
                                               C.byref(ctl), C.byref(res)), "coupled_cg")

@@ -15,8 +15,9 @@
 // (device copies ordered by events, the host threads meeting at a barrier;
 // no kernel ever waits for another rank).  Border packing is a gather kernel,
 // the exchange runs on a second stream and overlaps the diagonal-block
-// product, and the coupled CG (cg.cc:164-248 with the Jacobi preconditioner
-// of each rank's block) keeps its scalars on the device: the local partial
+// product, and the coupled CG (cg.cc:164-248 with block-Jacobi: Jacobi, or a
+// multicolour / ILU preconditioner of each rank's diagonal block, as
+// PreconditionerMultiColoring binds op.diagonal()) keeps its scalars on the device: the local partial
 // sums are reduced across ranks by the communicator on the stream, and small
 // kernels apply IterateControl::Check to the global values.  The host reads
 // the stop state once per batch of iterations; every rank takes the same
@@ -220,6 +221,34 @@ __global__ void __launch_bounds__(kBlock) coupled_start_kernel(int n, int jac, c
     }
 }
 
+// p = z (a block preconditioner's output), local rho = r.z and rr partials
+template <typename T>
+__global__ void __launch_bounds__(kBlock) coupled_start_z_kernel(int n, const T *__restrict__ r,
+                                                                 const T *__restrict__ z, T *__restrict__ p,
+                                                                 double *out, Scratch sc)
+{
+    double rho = 0.0, rr = 0.0;
+    for (int i = blockIdx.x * kBlock + threadIdx.x; i < n; i += gridDim.x * kBlock) {
+        const T ri = r[i], zi = z[i];
+        p[i] = zi;
+        rho += (double)(ri * zi);
+        rr += (double)(ri * ri);
+    }
+    double v[2] = {rho, rr}, o[2];
+    if (grid_reduce<2>(v, sc.partials, sc.ticket, o)) {
+        out[0] = o[0];
+        out[1] = o[1];
+    }
+}
+
+// beta = rz / rho; rho = rz after a block preconditioner's apply: g = {r.z} (global)
+__global__ void coupled_beta_kernel(DevState *st, const double *g)
+{
+    if (st->status != kIterate) return;
+    st->beta = g[0] / st->rho;
+    st->rho = g[0];
+}
+
 // r = b - t
 template <typename T>
 __global__ void sub_kernel(int n, const T *__restrict__ b, const T *__restrict__ t, T *__restrict__ r)
@@ -247,8 +276,8 @@ __global__ void coupled_alpha_kernel(DevState *st, const double *g)
     st->alpha = st->rho / g[0];
 }
 
-// iteration count, residual, Check, beta: g = {rr, rz} (global)
-__global__ void coupled_check_kernel(DevState *st, const double *g)
+// iteration count, residual, Check, and (with_beta) beta: g = {rr, rz} (global)
+__global__ void coupled_check_kernel(DevState *st, const double *g, int with_beta)
 {
     if (st->status != kIterate) return;
     const int it = st->iter + 1;
@@ -259,7 +288,7 @@ __global__ void coupled_check_kernel(DevState *st, const double *g)
     if (st->hist && it < st->hist_len) st->hist[it] = res;
     const int s = check_state(st, it, res);
     st->status = s;
-    if (s == kIterate) {
+    if (s == kIterate && with_beta) {
         st->beta = g[1] / st->rho;
         st->rho = g[1];
     }
@@ -580,17 +609,30 @@ extern "C" int b200la_coupled_cg(b200la_ctx *ctx, b200la_coupled *M, const b200l
     NvtxScope nvtx_range("b200la_coupled_cg");
     if (!ctx || !M || !b || !x || !ctl || ctl->maxits < 0)
         return cfail(ctx, B200LA_ERR_ARG, "coupled_cg: invalid argument");
-    if (P && (P->kind != B200LA_PRECOND_JACOBI || P->n != M->n || P->dtype != M->dtype))
+    if (P && (P->n != M->n || P->dtype != M->dtype || (P->kind != B200LA_PRECOND_JACOBI && !P->perm_dev)))
         return cfail(ctx, B200LA_ERR_ARG,
-                     "coupled_cg: the preconditioner must be the Jacobi preconditioner of this rank's diagonal block");
-    const int n = M->n, dt = M->dtype, jac = P ? 1 : 0;
-    const void *invd = P ? P->invd : nullptr;
+                     "coupled_cg: the preconditioner must be built on this rank's diagonal block");
+    // 0 none, 1 Jacobi (fused into the update), 2 a block preconditioner in
+    // its own numbering: r gathered into it, applied, z scattered back
+    const int pk = !P ? 0 : (P->kind == B200LA_PRECOND_JACOBI ? 1 : 2);
+    const int n = M->n, dt = M->dtype, jac = pk == 1 ? 1 : 0;
+    const void *invd = pk == 1 ? P->invd : nullptr;
     const size_t vb = ((esize(dt) * std::max(n, 1) + 255) / 256) * 256;
     void *wk;
-    int rc = ctx_work(ctx, 3 * vb, &wk);
+    int rc = ctx_work(ctx, (pk == 2 ? 6 : 3) * vb, &wk);
     if (rc) return rc;
     char *base = static_cast<char *>(wk);
     void *r = base, *p = base + vb, *Ap = base + 2 * vb;
+    void *z = base + 3 * vb, *rp = base + 4 * vb, *zp = base + 5 * vb;
+    // z = P^T M^-1 P r on this rank's block (PreconditionerMultiColoring on op.diagonal())
+    auto block_apply = [&](const int *gate) -> int {
+        CCK(launch_gather(dt, n, P->perm_dev, r, rp, ctx->stream));
+        int r2 = precond_apply_async(ctx, P, rp, zp, gate);
+        if (r2) return r2;
+        CCK(launch_scatter(dt, n, P->perm_dev, zp, z, ctx->stream));
+        ctx->launches += 2;
+        return B200LA_OK;
+    };
     const Scratch sc = ctx_scratch(ctx);
     const int g = grid_for(ctx, n);
     double *red = ctx->dscal;      // [0..1] reductions
@@ -608,12 +650,21 @@ extern "C" int b200la_coupled_cg(b200la_ctx *ctx, b200la_coupled *M, const b200l
 
     // r = b - A x; z = M r; p = z; rho = r.z; res = ||r||; Check(0)   (cg.cc:200-214)
     if ((rc = coupled_spmv_async(ctx, M, x, Ap))) return rc;
-    if (dt == B200LA_F64) {
-        sub_kernel<double><<<g, kBlock, 0, ctx->stream>>>(n, (const double *)b, (const double *)Ap, (double *)r);
+    if (dt == B200LA_F64) sub_kernel<double><<<g, kBlock, 0, ctx->stream>>>(n, (const double *)b, (const double *)Ap, (double *)r);
+    else sub_kernel<float><<<g, kBlock, 0, ctx->stream>>>(n, (const float *)b, (const float *)Ap, (float *)r);
+    CCK(cudaGetLastError());
+    if (pk == 2) {
+        if ((rc = block_apply(nullptr))) return rc;
+        if (dt == B200LA_F64)
+            coupled_start_z_kernel<double><<<g, kBlock, 0, ctx->stream>>>(n, (const double *)r, (const double *)z,
+                                                                           (double *)p, red, sc);
+        else
+            coupled_start_z_kernel<float><<<g, kBlock, 0, ctx->stream>>>(n, (const float *)r, (const float *)z,
+                                                                          (float *)p, red, sc);
+    } else if (dt == B200LA_F64) {
         coupled_start_kernel<double><<<g, kBlock, 0, ctx->stream>>>(n, jac, (const double *)r, (const double *)invd,
                                                                      (double *)p, red, sc);
     } else {
-        sub_kernel<float><<<g, kBlock, 0, ctx->stream>>>(n, (const float *)b, (const float *)Ap, (float *)r);
         coupled_start_kernel<float><<<g, kBlock, 0, ctx->stream>>>(n, jac, (const float *)r, (const float *)invd,
                                                                     (float *)p, red, sc);
     }
@@ -642,9 +693,17 @@ extern "C" int b200la_coupled_cg(b200la_ctx *ctx, b200la_coupled *M, const b200l
                                                                         (const float *)invd, ctx->st, red, sc);
         CCK(cudaGetLastError());
         if ((r2 = comm_allreduce(ctx, M->comm, red, 2))) return r2;
-        coupled_check_kernel<<<1, 1, 0, ctx->stream>>>(ctx->st, red);
+        coupled_check_kernel<<<1, 1, 0, ctx->stream>>>(ctx->st, red, pk == 2 ? 0 : 1);
+        if (pk == 2) {
+            // z = M^-1 r on the block; rho = r.z across ranks; beta   (cg.cc:236-240)
+            if ((r2 = block_apply(&ctx->st->status))) return r2;
+            CCK(launch_dot_to(sc, dt, n, r, z, red, &ctx->st->status, ctx->stream));
+            if ((r2 = comm_allreduce(ctx, M->comm, red, 1))) return r2;
+            coupled_beta_kernel<<<1, 1, 0, ctx->stream>>>(ctx->st, red);
+            ctx->launches += 2;
+        }
         // p = beta p + z                                        (cg.cc:241)
-        CCK(launch_cg_pupdate(dt, n, jac, p, r, invd, nullptr, ctx->st, ctx->stream));
+        CCK(launch_cg_pupdate(dt, n, pk == 2 ? 2 : jac, p, r, invd, pk == 2 ? z : nullptr, ctx->st, ctx->stream));
         ctx->launches += 5;
         return B200LA_OK;
     };

@@ -21,6 +21,7 @@
 #include "spmv_epi.cuh"
 
 #include <cmath>
+#include <cstdlib>
 
 namespace b200 {
 
@@ -709,8 +710,10 @@ struct HalfRow<double, NB> {
     }
 };
 
-template <typename T, int EPI, int NB>
-__global__ void __launch_bounds__(kBlock, (sizeof(T) == 8 ? 5 : 1)) spmv_half_kernel(CsrView A, SpmvOp op, Scratch sc)
+// MINB: CTAs per SM the registers are budgeted for (FP64: 4 without spills,
+// 5 with about 100 spilled bytes in the reducing epilogues; B200LA_HALF_MINB)
+template <typename T, int EPI, int NB, int MINB = 1>
+__global__ void __launch_bounds__(kBlock, MINB) spmv_half_kernel(CsrView A, SpmvOp op, Scratch sc)
 {
     if (gate_closed(op.gate)) return;
     constexpr int U = (NB - 1) / 2;
@@ -823,8 +826,14 @@ void launch_epi(const Scratch &s, const CsrView &A, const Seg &seg, const SpmvOp
 {
     if constexpr (EPI == EPI_SET || EPI == EPI_ADD || EPI == EPI_DOT_X || EPI == EPI_RESID) {
         if (A.sh_use && A.sh_val && A.st_use && seg.r0 == 0 && seg.r1 == A.n_rows && (A.st_nb == 3 || A.st_nb == 9)) {
-            static int res_nb[2] = {0, 0};
-            if (A.st_nb == 9)
+            static int res_nb[3] = {0, 0, 0};
+            static const int minb = [] {
+                const char *e = std::getenv("B200LA_HALF_MINB");
+                return e ? std::atoi(e) : 0;
+            }();
+            if (A.st_nb == 9 && minb == 5 && sizeof(T) == 8)
+                launch_one_wave(spmv_half_kernel<T, EPI, 9, 5>, res_nb[2], s, A.n_rows, A, op, st);
+            else if (A.st_nb == 9)
                 launch_one_wave(spmv_half_kernel<T, EPI, 9>, res_nb[1], s, A.n_rows, A, op, st);
             else
                 launch_one_wave(spmv_half_kernel<T, EPI, 3>, res_nb[0], s, A.n_rows, A, op, st);

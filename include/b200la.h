@@ -466,10 +466,13 @@ int b200la_coupled_update_ghost(b200la_ctx *ctx, b200la_coupled *M, const void *
 int b200la_coupled_spmv(b200la_ctx *ctx, b200la_coupled *M, const void *x, void *y);
 /* CoupledVector::Dot: the sum over all ranks of x . y (owned values). */
 int b200la_coupled_dot(b200la_ctx *ctx, b200la_coupled *M, const void *x, const void *y, double *out);
-/* CG<LAD>::Solve over the coupled operator (cg.cc:164-248), with no
- * preconditioner or with the Jacobi preconditioner of this rank's diagonal
- * block (P from b200la_precond_jacobi on diag: block-Jacobi with point
- * blocks, as PreconditionerBlockJacobiStand binds op.diagonal()).  The
+/* CG<LAD>::Solve over the coupled operator (cg.cc:164-248), block-Jacobi
+ * across ranks: no preconditioner, the Jacobi preconditioner of this rank's
+ * diagonal block (b200la_precond_jacobi on diag, as
+ * PreconditionerBlockJacobiStand binds op.diagonal()), or a multicolour /
+ * ILU preconditioner built on the block's host CSR (b200la_precond_mcsgs,
+ * _ilu0, _ilup: r is gathered into its permuted numbering, the sweeps run,
+ * z is scattered back -- PreconditionerMultiColoring on op.diagonal()).  The
  * recurrence scalars stay on the device and are reduced across ranks by the
  * communicator; every rank gets the same iteration count and status. */
 int b200la_coupled_cg(b200la_ctx *ctx, b200la_coupled *M, const b200la_precond *P, const void *b, void *x,
