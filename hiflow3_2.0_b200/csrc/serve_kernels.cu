@@ -30,6 +30,8 @@
 // gathered vectors go through L1.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include "common.cuh"
 #include "serve.cuh"
 
@@ -607,8 +609,10 @@ __device__ __forceinline__ void k2_corr(const WarpCtx &c, const Run R)
     }
 }
 
-template <int NW>
-__global__ void __launch_bounds__(NW * 32, kMinCta256 * 8 / NW) k1_kernel(const SysDesc *__restrict__ sys,
+// MINC: 256-thread CTAs per SM the registers are budgeted for (4: 64
+// registers with some spilled; 3: 80 registers; B200LA_SERVE_K1_MINCTA)
+template <int NW, int MINC = kMinCta256>
+__global__ void __launch_bounds__(NW * 32, MINC * 8 / NW) k1_kernel(const SysDesc *__restrict__ sys,
                                                                        SysState *state, const int *__restrict__ tb)
 {
     __shared__ WarpCtx ctx[NW];
@@ -964,11 +968,17 @@ __global__ void half_build_slot_kernel(SysDesc d, const int *__restrict__ row, c
 
 cudaError_t launch_round(int nw, int grid, const SysDesc *sys, SysState *state, const int *tab, cudaStream_t st)
 {
+    static const int minc = [] {
+        const char *e = std::getenv("B200LA_SERVE_K1_MINCTA");
+        return e ? std::atoi(e) : kMinCta256;
+    }();
     if (nw == 4) {
-        k1_kernel<4><<<grid, 128, 0, st>>>(sys, state, tab);
+        if (minc == 3) k1_kernel<4, 3><<<grid, 128, 0, st>>>(sys, state, tab);
+        else k1_kernel<4><<<grid, 128, 0, st>>>(sys, state, tab);
         k2_kernel<4><<<grid, 128, 0, st>>>(sys, state, tab);
     } else {
-        k1_kernel<8><<<grid, 256, 0, st>>>(sys, state, tab);
+        if (minc == 3) k1_kernel<8, 3><<<grid, 256, 0, st>>>(sys, state, tab);
+        else k1_kernel<8><<<grid, 256, 0, st>>>(sys, state, tab);
         k2_kernel<8><<<grid, 256, 0, st>>>(sys, state, tab);
     }
     return cudaGetLastError();
