@@ -112,7 +112,7 @@ CsrView csr_view(const b200la_csr *A)
     v.n_rows = A->n;
     v.st_val = A->st_val;
     v.st_nb = A->st_nb;
-    v.st_use = A->st_use && A->st_val != nullptr;
+    v.st_use = A->st_use && (A->st_val != nullptr || (A->sh_use && A->sh_val != nullptr));
     for (int b = 0; b < kMaxBands; ++b) v.st_center[b] = b < A->st_nb ? A->st_union[3 * b + 1] : 0;
     v.sh_val = A->sh_val;
     v.sh_mask = A->sh_mask;
@@ -420,6 +420,8 @@ static void build_segment(const int *row, int s0, int s1, int lg, int cap, std::
 static int build_sell(b200la_ctx *ctx, b200la_csr *A)
 {
     if (!A->pid || !A->use_pat || A->n == 0) return B200LA_OK;
+    // its whole-operator products run on the stencil layout: no sliced copy
+    if (A->st_use && A->st_nb && A->seg_off.empty()) return B200LA_OK;
     const size_t es = dsize(A->dtype);
     cudaError_t e;
     if (!A->sell_off) {
@@ -525,6 +527,13 @@ static int build_half(b200la_ctx *ctx, b200la_csr *A)
         return B200LA_OK;
     }
     A->sh_use = 1;
+    // the half layout now carries the operator's products: the full layout's
+    // values are dropped (rebuilt from the CSR when the values change)
+    if (A->st_use && A->st_val) {
+        cudaFree(A->st_val);
+        A->st_val = nullptr;
+        A->bytes -= es * stencil_len(A->n, nb, A->dtype);
+    }
     return B200LA_OK;
 }
 
@@ -679,15 +688,15 @@ int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row,
                 return rc;
             }
         }
-        int rc = build_sell(ctx, A);
-        if (!rc && n_seg == 0) {
+        if (n_seg == 0) {
             std::vector<int> uni(pdel);
             std::sort(uni.begin(), uni.end());
             uni.erase(std::unique(uni.begin(), uni.end()), uni.end());
             stencil_plan(A, uni);
             A->st_use = stencil_policy(dtype);
-            rc = build_stencil(ctx, A);
         }
+        int rc = build_sell(ctx, A);
+        if (!rc && n_seg == 0) rc = build_stencil(ctx, A);
         if (rc) {
             b200la_csr_destroy(A);
             return rc;

@@ -111,10 +111,11 @@ struct Fabric {
     // mailboxes, one slot per rank
     std::vector<const void *> border;       // rank's border buffer
     std::vector<const int *> border_off;    // rank's border offsets (host), nranks + 1
-    std::vector<cudaEvent_t> ready, copied, summed;
+    std::vector<cudaEvent_t> ready;     // rank's last pack / contribution copy
+    std::vector<cudaEvent_t> done;      // rank's last ghost copy / contribution sum
     std::vector<const double *> contrib;    // rank's all-reduce contribution (device)
     explicit Fabric(int n)
-        : size(n), border(n), border_off(n), ready(n), copied(n), summed(n), contrib(n) {}
+        : size(n), border(n), border_off(n), ready(n), done(n), contrib(n) {}
 
     bool barrier()
     {
@@ -144,7 +145,7 @@ struct b200la_comm {
     int device = -1;
     ncclComm_t nc = nullptr;
     std::shared_ptr<Fabric> fab;
-    cudaEvent_t ev_ready = nullptr, ev_copied = nullptr, ev_summed = nullptr;
+    cudaEvent_t ev_ready = nullptr, ev_summed = nullptr;
     double *contrib = nullptr;          // local all-reduce contribution (8 doubles)
 };
 
@@ -333,9 +334,9 @@ static int comm_allreduce(b200la_ctx *ctx, b200la_comm *c, double *dev, int coun
     sum_contrib_kernel<<<1, 32, 0, ctx->stream>>>(f.size, tab, count, dev);
     CCK(cudaGetLastError());
     CCK(cudaEventRecord(c->ev_summed, ctx->stream));
-    f.summed[c->rank] = c->ev_summed;
+    f.done[c->rank] = c->ev_summed;
     if (!f.barrier()) return cfail(ctx, B200LA_ERR_COMM, "local all-reduce: a rank did not arrive");
-    for (int q = 0; q < f.size; ++q) CCK(cudaStreamWaitEvent(ctx->stream, f.summed[q], 0));
+    for (int q = 0; q < f.size; ++q) CCK(cudaStreamWaitEvent(ctx->stream, f.done[q], 0));
     // nobody records its events again before every rank has queued its waits
     if (!f.barrier()) return cfail(ctx, B200LA_ERR_COMM, "local all-reduce: a rank did not arrive");
     return B200LA_OK;
@@ -397,7 +398,6 @@ static int comm_local_setup(b200la_ctx *ctx, b200la_comm *c)
     if (c->kind != 1 || c->contrib) return B200LA_OK;
     c->device = ctx->device;
     CCK(cudaEventCreateWithFlags(&c->ev_ready, cudaEventDisableTiming));
-    CCK(cudaEventCreateWithFlags(&c->ev_copied, cudaEventDisableTiming));
     CCK(cudaEventCreateWithFlags(&c->ev_summed, cudaEventDisableTiming));
     CCK(cudaMalloc(&c->contrib, sizeof(double) * kMaxRed));
     return B200LA_OK;
@@ -418,7 +418,6 @@ extern "C" int b200la_comm_destroy(b200la_comm *c)
     cudaDeviceSynchronize();
     if (c->nc && nccl()) nccl()->CommDestroy(c->nc);
     if (c->ev_ready) cudaEventDestroy(c->ev_ready);
-    if (c->ev_copied) cudaEventDestroy(c->ev_copied);
     if (c->ev_summed) cudaEventDestroy(c->ev_summed);
     if (c->contrib) cudaFree(c->contrib);
     delete c;
@@ -535,11 +534,11 @@ static int exchange_begin(b200la_ctx *ctx, b200la_coupled *M, const void *x)
                             cudaMemcpyDeviceToDevice, M->xs));
     }
     CCK(cudaEventRecord(M->arrived, M->xs));
-    f.summed[c->rank] = M->arrived;
+    f.done[c->rank] = M->arrived;
     if (!f.barrier()) return cfail(ctx, B200LA_ERR_COMM, "ghost exchange: a rank did not arrive");
     // the border is packed again only after every reader has copied it
     for (int q = 0; q < P; ++q)
-        if (M->border_off[q + 1] > M->border_off[q]) CCK(cudaStreamWaitEvent(ctx->stream, f.summed[q], 0));
+        if (M->border_off[q + 1] > M->border_off[q]) CCK(cudaStreamWaitEvent(ctx->stream, f.done[q], 0));
     if (!f.barrier()) return cfail(ctx, B200LA_ERR_COMM, "ghost exchange: a rank did not arrive");
     return B200LA_OK;
 }
