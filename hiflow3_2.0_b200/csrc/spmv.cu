@@ -710,9 +710,11 @@ struct HalfRow<double, NB> {
     }
 };
 
-// MINB: CTAs per SM the registers are budgeted for (FP64: 4 without spills,
-// 5 with about 100 spilled bytes in the reducing epilogues; B200LA_HALF_MINB)
-template <typename T, int EPI, int NB, int MINB = 1>
+// MINB: CTAs per SM the registers are budgeted for.  FP64: 4 (64 registers,
+// no spills; unbounded, the compiler hoists every group's loads and takes
+// 152 registers, one CTA per SM), or 5 with about 100 spilled bytes in the
+// reducing epilogues (B200LA_HALF_MINB=5).
+template <typename T, int EPI, int NB, int MINB = (sizeof(T) == 8 ? 4 : 1)>
 __global__ void __launch_bounds__(kBlock, MINB) spmv_half_kernel(CsrView A, SpmvOp op, Scratch sc)
 {
     if (gate_closed(op.gate)) return;
@@ -815,7 +817,13 @@ void launch_one_wave(K kern, int &resident, const Scratch &s, int n_rows, const 
     int grid = (chunks + kBlock / 32 - 1) / (kBlock / 32);
     if (!resident && cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, kern, kBlock, 0) != cudaSuccess)
         resident = 4;
-    const int cap = s.num_sms * resident;
+    // B200LA_STENCIL_CTAS: fewer CTAs per SM than fit (the share of warps
+    // with one chunk more than the others sets the tail of the pass)
+    static const int cap_env = [] {
+        const char *e = std::getenv("B200LA_STENCIL_CTAS");
+        return e ? std::atoi(e) : 0;
+    }();
+    const int cap = s.num_sms * (cap_env > 0 ? std::min(cap_env, resident) : resident);
     if (grid > cap) grid = cap;
     if (grid < 1) grid = 1;
     kern<<<grid, kBlock, 0, st>>>(A, op, s);
