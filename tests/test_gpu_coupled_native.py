@@ -195,9 +195,9 @@ def test_native_coupled_cg_mcsgs_blocks(b200, world):
         M = cp.NativeCoupledMatrix(pf, comms[r], trs[r], part, r, lr, col[row[r0]:row[r1]], val[row[r0]:row[r1]])
         x = M.vector()
         st = M.CG(M.vector(b[r0:r1]), x, precond="mcsgs", maxits=5000, reltol=1e-10)
+        out = (r0, st, M.iter, x.numpy())    # before the Jacobi solve overwrites M.iter
         xj = M.vector()
         M.CG(M.vector(b[r0:r1]), xj, precond="jacobi", maxits=5000, reltol=1e-10)
-        out = (r0, st, M.iter, x.numpy())
         itj = M.iter
         M.close()
         return out + (itj,)
