@@ -136,16 +136,28 @@ __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__r
     });
     const T *v = val + L.val0 + (size_t)(g - L.chunk0) * (S.n * 32) + lane;
     T s = T(0);
+    // sweeps (PREALL): every value load of the row issued before the grid
+    // dependency wait, one round trip for all of them
+    constexpr bool PREALL = PART != 2 && S.n > 0;
+    T aall[PREALL ? S.n : 1];
+    if constexpr (PREALL) {
+        static_for<0, S.n>([&](auto kk) {
+            constexpr int k = decltype(kk)::value;
+            aall[k] = ld_stream(v + 32 * k, pol);
+        });
+        grid_dependency_wait();
+    }
     static_for<0, (S.n + kLatGroup - 1) / kLatGroup>([&](auto gg) {
         constexpr int k0 = decltype(gg)::value * kLatGroup;
         constexpr int cnt = S.n - k0 < kLatGroup ? S.n - k0 : kLatGroup;
         T a[kLatGroup], w[kLatGroup];
         static_for<0, cnt>([&](auto jj) {
             constexpr int j = decltype(jj)::value;
-            a[j] = ld_stream(v + 32 * (k0 + j), pol);
+            if constexpr (PREALL) a[j] = aall[k0 + j];
+            else a[j] = ld_stream(v + 32 * (k0 + j), pol);
         });
         // x (what earlier colours wrote) only after the previous launch completed
-        if constexpr (decltype(gg)::value == 0) grid_dependency_wait();
+        if constexpr (!PREALL && decltype(gg)::value == 0) grid_dependency_wait();
         static_for<0, cnt>([&](auto jj) {
             constexpr int j = decltype(jj)::value, k = k0 + j;
             constexpr int dx = S.dx[k], dy = S.dy[k], dz = S.dz[k], cp = S.cp[k];
