@@ -136,9 +136,11 @@ __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__r
     });
     const T *v = val + L.val0 + (size_t)(g - L.chunk0) * (S.n * 32) + lane;
     T s = T(0);
-    // sweeps (PREALL): every value load of the row issued before the grid
-    // dependency wait, one round trip for all of them
-    constexpr bool PREALL = PART != 2 && S.n > 0;
+    // PREALL: every value load of the row issued first (before the grid
+    // dependency wait of a sweep), one round trip for all of them.  Measured
+    // per kernel: faster for the sweeps and the reducing products, slower for
+    // the plain product y = Ax (89.8 -> 92.5 us at 128^3), which keeps groups
+    constexpr bool PREALL = S.n > 0 && !(PART == 2 && EPI == EPI_SET);
     T aall[PREALL ? S.n : 1];
     if constexpr (PREALL) {
         static_for<0, S.n>([&](auto kk) {
