@@ -194,7 +194,7 @@ extern "C" int b200la_create(int device, b200la_ctx **out)
         (e = cudaMemset(ctx->dev_err, 0, sizeof(int))) || (e = spmv_configure()) || (e = sweeps_configure())) {
         ctx->stream = ctx->own_stream;
         b200la_destroy(ctx);
-        return B200LA_ERR_CUDA;
+        return e == cudaErrorMemoryAllocation ? B200LA_ERR_ALLOC : B200LA_ERR_CUDA;
     }
     ctx->stream = ctx->own_stream;
     *out = ctx;

@@ -149,13 +149,6 @@ static void state_init(DevState &s, const b200la_control *ctl, double *hist, int
     s.hist_len = hist_len;
 }
 
-static int read_state(b200la_ctx *ctx, DevState *host)
-{
-    SK(cudaMemcpyAsync(host, ctx->st, sizeof(DevState), cudaMemcpyDeviceToHost, ctx->stream));
-    SK(cudaStreamSynchronize(ctx->stream));
-    return B200LA_OK;
-}
-
 // ------------------------------------------------------------------ CG
 
 struct CgWork {
