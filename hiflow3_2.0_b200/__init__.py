@@ -460,7 +460,17 @@ class Platform:
         """The platform's CUDA stream (every kernel of this platform runs on it)
         as a torch stream, for ordering other work against it with events."""
         torch = _torch()
-        return torch.cuda.ExternalStream(lib().b200la_get_stream(self.h) or 0, device=f"cuda:{self.device}")
+        if getattr(self, "_ts", None) is None:
+            self._ts = torch.cuda.ExternalStream(lib().b200la_get_stream(self.h) or 0, device=f"cuda:{self.device}")
+        return self._ts
+
+    def on_stream(self):
+        """Context in which torch allocates, fills and copies on the
+        platform's stream.  Every device tensor the platform hands to the
+        library is made inside it: the caching allocator then reuses a freed
+        block only in that stream's order, after the library's kernels that
+        still read it (a temporary input freed as soon as the call returns)."""
+        return _torch().cuda.stream(self.stream())
 
     def num_sms(self):
         return lib().b200la_num_sms(self.h)
@@ -501,10 +511,11 @@ class Platform:
     def vector(self, data_or_n, dtype=F64):
         torch = _torch()
         td = torch.float64 if dtype == F64 else torch.float32
-        if isinstance(data_or_n, int):
-            return lVector(self, torch.zeros(data_or_n, dtype=td, device=f"cuda:{self.device}"))
-        a = np.ascontiguousarray(data_or_n, dtype=np.float64 if dtype == F64 else np.float32)
-        return lVector(self, torch.from_numpy(a).to(f"cuda:{self.device}"))
+        with self.on_stream():
+            if isinstance(data_or_n, int):
+                return lVector(self, torch.zeros(data_or_n, dtype=td, device=f"cuda:{self.device}"))
+            a = np.ascontiguousarray(data_or_n, dtype=np.float64 if dtype == F64 else np.float32)
+            return lVector(self, torch.from_numpy(a).to(f"cuda:{self.device}"))
 
 
 def _dt(t):
@@ -545,7 +556,8 @@ class lVector:
         self.pf.check(lib().b200la_memcpy_d2d(self.pf.h, self.ptr, other.ptr, self.t.numel() * self.t.element_size()))
 
     def CloneWithoutContent(self):
-        return lVector(self.pf, _torch().zeros_like(self.t))
+        with self.pf.on_stream():
+            return lVector(self.pf, _torch().zeros_like(self.t))
 
     def Dot(self, other):
         out = C.c_double()
@@ -617,8 +629,9 @@ class lVector:
 
     def GetIndexedValues(self, idx):
         torch = _torch()
-        idx_t = torch.as_tensor(_i32(idx), device=self.t.device)
-        out = torch.empty(idx_t.numel(), dtype=self.t.dtype, device=self.t.device)
+        with self.pf.on_stream():
+            idx_t = torch.as_tensor(_i32(idx), device=self.t.device)
+            out = torch.empty(idx_t.numel(), dtype=self.t.dtype, device=self.t.device)
         self.pf.check(lib().b200la_gather(self.pf.h, self.dtype, idx_t.numel(), C.c_void_p(idx_t.data_ptr()),
                                           self.ptr, C.c_void_p(out.data_ptr())), "GetIndexedValues")
         self.pf.sync()
@@ -626,8 +639,9 @@ class lVector:
 
     def SetIndexedValues(self, idx, values):
         torch = _torch()
-        idx_t = torch.as_tensor(_i32(idx), device=self.t.device)
-        v = torch.as_tensor(np.asarray(values), dtype=self.t.dtype, device=self.t.device)
+        with self.pf.on_stream():
+            idx_t = torch.as_tensor(_i32(idx), device=self.t.device)
+            v = torch.as_tensor(np.asarray(values), dtype=self.t.dtype, device=self.t.device)
         self.pf.check(lib().b200la_scatter(self.pf.h, self.dtype, idx_t.numel(), C.c_void_p(idx_t.data_ptr()),
                                            C.c_void_p(v.data_ptr()), self.ptr), "SetIndexedValues")
         self.pf.sync()
@@ -686,7 +700,8 @@ class lVector:
     def extract_subvector(self, start, end):
         """A new vector holding x[start:end] (lvector_cpu.cc:419-457)."""
         self._range(start, end)
-        sub = lVector(self.pf, _torch().empty(end - start, dtype=self.t.dtype, device=self.t.device))
+        with self.pf.on_stream():
+            sub = lVector(self.pf, _torch().empty(end - start, dtype=self.t.dtype, device=self.t.device))
         if end > start:
             self.pf.check(lib().b200la_memcpy_d2d(self.pf.h, sub.ptr, self._at(start), (end - start) *
                                                   self.t.element_size()), "extract_subvector")
@@ -717,8 +732,9 @@ class lVector:
     def Reorder(self, perm):
         """out[i] = in[perm[i]] (CPU_lVector::Reorder, lvector_cpu.cc:75-94)."""
         torch = _torch()
-        p = torch.as_tensor(_i32(perm), device=self.t.device)
-        out = torch.empty_like(self.t)
+        with self.pf.on_stream():
+            p = torch.as_tensor(_i32(perm), device=self.t.device)
+            out = torch.empty_like(self.t)
         self.pf.check(lib().b200la_permute(self.pf.h, self.dtype, self.get_size(), C.c_void_p(p.data_ptr()),
                                            self.ptr, C.c_void_p(out.data_ptr())), "Reorder")
         self.pf.sync()
@@ -791,7 +807,8 @@ class CSR_lMatrix:
 
     def VectorMultDot(self, x, y):
         torch = _torch()
-        d = torch.zeros(1, dtype=torch.float64, device=x.t.device)
+        with self.pf.on_stream():
+            d = torch.zeros(1, dtype=torch.float64, device=x.t.device)
         self.pf.check(lib().b200la_spmv_dot(self.pf.h, self.h, x.ptr, y.ptr, C.c_void_p(d.data_ptr())),
                       "VectorMultDot")
         self.pf.sync()
@@ -799,7 +816,8 @@ class CSR_lMatrix:
 
     def Residual(self, b, x, r):
         torch = _torch()
-        d = torch.zeros(1, dtype=torch.float64, device=x.t.device)
+        with self.pf.on_stream():
+            d = torch.zeros(1, dtype=torch.float64, device=x.t.device)
         self.pf.check(lib().b200la_residual(self.pf.h, self.h, b.ptr, x.ptr, r.ptr, C.c_void_p(d.data_ptr())),
                       "Residual")
         self.pf.sync()

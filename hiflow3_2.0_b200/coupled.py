@@ -282,9 +282,10 @@ class CoupledVector:
         self.interior = platform.vector(data_or_n, dtype)
         td = torch.float64 if dtype == F64 else torch.float32
         dev = f"cuda:{platform.device}"
-        self.ghost = torch.zeros(len(couplings.ghost_global), dtype=td, device=dev)
-        self.border = torch.zeros(len(couplings.border_indices), dtype=td, device=dev)
-        self._bidx = torch.from_numpy(couplings.border_indices.astype(np.int32)).to(dev)
+        with platform.on_stream():
+            self.ghost = torch.zeros(len(couplings.ghost_global), dtype=td, device=dev)
+            self.border = torch.zeros(len(couplings.border_indices), dtype=td, device=dev)
+            self._bidx = torch.from_numpy(couplings.border_indices.astype(np.int32)).to(dev)
 
     def clone_without_content(self):
         return CoupledVector(self.pf, self.cp, self.tr, self.interior.get_size(), self.dtype)
@@ -374,8 +375,9 @@ class CoupledMatrix:
             import torch
             dev = f"cuda:{platform.device}"
             cp = self.couplings
-            self._gowner = torch.from_numpy(cp.ghost_owner.copy()).to(dev)
-            self._gindex = torch.from_numpy(cp.ghost_index.copy()).to(dev)
+            with platform.on_stream():
+                self._gowner = torch.from_numpy(cp.ghost_owner.copy()).to(dev)
+                self._gindex = torch.from_numpy(cp.ghost_index.copy()).to(dev)
             size = transport.size
             self._reads_from = [q for q in range(size) if cp.ghost_offsets[q + 1] > cp.ghost_offsets[q]]
             self._read_by = [q for q in range(size) if cp.border_offsets[q + 1] > cp.border_offsets[q]]
@@ -413,8 +415,8 @@ class CoupledMatrix:
                 self.pf.sync()
                 self._owner_tables.clear()
             host = torch.tensor(list(ptrs), dtype=torch.int64).pin_memory()
-            t = torch.empty(len(ptrs), dtype=torch.int64, device=f"cuda:{self.pf.device}")
-            with torch.cuda.stream(self.pf.stream()):
+            with self.pf.on_stream():
+                t = torch.empty(len(ptrs), dtype=torch.int64, device=f"cuda:{self.pf.device}")
                 t.copy_(host, non_blocking=True)
             self.pf.stream().synchronize()
             self._owner_tables[ptrs] = t
@@ -489,7 +491,8 @@ class BlockPrecond:
             from . import Preconditioner
             rd, cd, vd = A.diag_host
             self.P = Preconditioner.MultiColoringSGS(A.pf, rd, cd, vd, dtype=A.dtype)
-            self._perm = torch.from_numpy(np.asarray(self.P.perm, np.int32).copy()).to(f"cuda:{A.pf.device}")
+            with A.pf.on_stream():
+                self._perm = torch.from_numpy(np.asarray(self.P.perm, np.int32).copy()).to(f"cuda:{A.pf.device}")
             self._rp, self._zp = A.pf.vector(A.n_local, A.dtype), A.pf.vector(A.n_local, A.dtype)
 
     def apply(self, src, dst):
@@ -811,8 +814,9 @@ class NativeCoupledMatrix:
     def UpdateGhost(self, x):
         """The ghost values of x (CoupledVector::UpdateGhost), as a host array."""
         import torch
-        g = torch.zeros(len(self.couplings.ghost_global),
-                        dtype=torch.float64 if self.dtype == F64 else torch.float32, device=f"cuda:{self.pf.device}")
+        with self.pf.on_stream():
+            g = torch.zeros(len(self.couplings.ghost_global),
+                            dtype=torch.float64 if self.dtype == F64 else torch.float32, device=f"cuda:{self.pf.device}")
         self.pf.check(lib().b200la_coupled_update_ghost(self.pf.h, self.h, x.ptr,
                                                         C.c_void_p(g.data_ptr()) if g.numel() else None),
                       "coupled_update_ghost")
