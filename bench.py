@@ -422,7 +422,8 @@ def run_b200(args, rank, world, local_rank, dist):
         dt = b200.F64 if vbytes == 8 else b200.F32
         xx, yy = pf.vector(np.random.default_rng(1).uniform(-1, 1, n), dt), pf.vector(n, dt)
         import ctypes
-        d = torch.zeros(1, dtype=torch.float64, device="cuda")
+        with pf.on_stream():
+            d = torch.zeros(1, dtype=torch.float64, device="cuda")
         L = b200.lib()
         for _ in range(3):
             L.b200la_spmv_dot(pf.h, A.h, xx.ptr, yy.ptr, ctypes.c_void_p(d.data_ptr()))

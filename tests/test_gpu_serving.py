@@ -45,11 +45,12 @@ def test_q1_assemble_device_bitexact(pf, b200, dim, N, kind, coef):
     kc = np.exp(np.random.default_rng(3).standard_normal(N ** dim)) if coef else None
     beta = np.array([1.0, 0.5, 0.25])
     row_h, col_h, val_h = b200.q1_assemble(dim, N, kind, kc, 1e-2, beta)
-    row = torch.empty(n + 1, dtype=torch.int32, device="cuda")
-    col = torch.empty(nnz, dtype=torch.int32, device="cuda")
-    val = torch.empty(nnz, dtype=torch.float64, device="cuda")
-    rhs = torch.empty(n, dtype=torch.float64, device="cuda")
-    kd = torch.from_numpy(kc).cuda() if coef else None
+    with pf.on_stream():   # ordered with the library's kernels on the platform's stream
+        row = torch.empty(n + 1, dtype=torch.int32, device="cuda")
+        col = torch.empty(nnz, dtype=torch.int32, device="cuda")
+        val = torch.empty(nnz, dtype=torch.float64, device="cuda")
+        rhs = torch.empty(n, dtype=torch.float64, device="cuda")
+        kd = torch.from_numpy(kc).cuda() if coef else None
     L = b200.lib()
     pf.check(L.b200la_q1_assemble_device(pf.h, dim, N, kind, _ptr(kd), 1e-2, beta.ctypes.data, _ptr(row),
                                          _ptr(col), _ptr(val)), "q1_assemble_device")
