@@ -563,11 +563,31 @@ def run_b200(args, rank, world, local_rank, dist):
 
 
 def other_configs(b200, pf, wl):
-    """Time to solution of the two other device configurations: C2 (3-D
+    """Time to solution of the other configurations: C1 (2-D Poisson 256^2,
+    Jacobi-CG to 1e-10, FP64; the reference's own CPU case), C2 (3-D
     Poisson 128^3, 8-colour MC-SGS PCG to 1e-8, FP64) and C4 (2-D
     convection-diffusion 512^2, GMRES(30) + level-scheduled ILU(0) to 1e-9,
     FP64 and mixed: FP32 factors and Arnoldi inside FP64 defect correction)."""
     out = {}
+    # C1
+    row, col, val, b, _ = wl.system(b200, "c1")
+    A1 = b200.CSR_lMatrix.from_csr(pf, row, col, val)
+    cg = b200.CG(pf)
+    cg.SetupOperator(A1)
+    cg.SetupPreconditioner(b200.Preconditioner.Jacobi(pf, A1))
+    cg.InitControl(100000, 0.0, 1e-10, 1e6)
+    bv, x = pf.vector(b), pf.vector(len(b))
+    cg.Solve(bv, x)
+    times = []
+    for _ in range(5):
+        x.Zeros()
+        pf.sync()
+        pf.timer_start()
+        cg.Solve(bv, x)
+        times.append(pf.timer_stop())
+    out["c1_jacobi_cg_fp64"] = {"ms": float(np.median(times)), "iters": cg.iter(), "status": cg.result.status,
+                                "storage": A1.info()["storage"], "n": len(b), "nnz": len(col),
+                                "note": "median of 5 timed solves (the system fits in L2)"}
     # C2
     row, col, val, b, _ = wl.system(b200, "c2")
     t0 = time.perf_counter()

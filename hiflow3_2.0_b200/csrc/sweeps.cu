@@ -321,13 +321,16 @@ struct StageRec {
 template <typename T, int KP>
 __global__ void __launch_bounds__(kLevelThreads) level_sweep_staged_kernel(LevelStagedArgs a)
 {
+    // one thread per row of the largest level (blockDim.x <= kLevelThreads):
+    // idle warps would only lengthen every level's barrier
+    const int NT = blockDim.x;
     extern __shared__ __align__(16) unsigned char s_raw[];
     using Rec = StageRec<T, KP>;
-    Rec *stage = reinterpret_cast<Rec *>(s_raw);                             // [kStages][kLevelThreads]
-    T *ring = reinterpret_cast<T *>(s_raw + sizeof(Rec) * kStages * kLevelThreads);
+    Rec *stage = reinterpret_cast<Rec *>(s_raw);                             // [kStages][NT]
+    T *ring = reinterpret_cast<T *>(s_raw + sizeof(Rec) * kStages * NT);
     int *s_off = reinterpret_cast<int *>(ring + kRingStaged);
     if (gate_closed(a.gate)) return;
-    for (int i = threadIdx.x; i <= a.nlev; i += kLevelThreads) s_off[i] = __ldg(a.off + i);
+    for (int i = threadIdx.x; i <= a.nlev; i += NT) s_off[i] = __ldg(a.off + i);
     __syncthreads();
     const int tid = threadIdx.x, nlev = a.nlev;
     const T *pval = static_cast<const T *>(a.pval);
@@ -342,7 +345,7 @@ __global__ void __launch_bounds__(kLevelThreads) level_sweep_staged_kernel(Level
         if (k < nlev) {
             const int l = level_of(k), rr = s_off[l] + tid;
             if (rr < s_off[l + 1]) {
-                Rec &q = stage[(k % kStages) * kLevelThreads + tid];
+                Rec &q = stage[(k % kStages) * NT + tid];
 #pragma unroll
                 for (int b = 0; b < KP * 4; b += 16) cp_async(reinterpret_cast<char *>(q.col) + b,
                                                               reinterpret_cast<const char *>(a.pcol + (size_t)rr * KP) + b, 16);
@@ -382,11 +385,11 @@ __global__ void __launch_bounds__(kLevelThreads) level_sweep_staged_kernel(Level
         const int l = level_of(k), r0 = s_off[l], r1 = s_off[l + 1];
         const int rr = r0 + tid;
         if (rr < r1) {
-            const Rec &q = stage[(k % kStages) * kLevelThreads + tid];
+            const Rec &q = stage[(k % kStages) * NT + tid];
             solve(rr, q.col, q.val, q.cnt, q.own, need_e1 ? q.e1 : T(0), need_e2 ? q.e2 : T(0), r0, r1);
         }
-        // rows of a level beyond the first kLevelThreads: read directly
-        for (int r2 = rr + kLevelThreads; r2 < r1; r2 += kLevelThreads) {
+        // rows of a level beyond the first NT: read directly
+        for (int r2 = rr + NT; r2 < r1; r2 += NT) {
             int cols[KP];
             T vals[KP];
 #pragma unroll
@@ -421,9 +424,9 @@ __global__ void pack_rows_kernel(int n, int kp, const int *__restrict__ row, con
 }
 
 template <typename T, int KP>
-size_t staged_smem(int nlev)
+size_t staged_smem(int nlev, int NT = kLevelThreads)
 {
-    return sizeof(StageRec<T, KP>) * kStages * kLevelThreads + sizeof(T) * kRingStaged + sizeof(int) * (nlev + 1);
+    return sizeof(StageRec<T, KP>) * kStages * NT + sizeof(T) * kRingStaged + sizeof(int) * (nlev + 1);
 }
 
 }  // namespace
@@ -481,6 +484,7 @@ struct SyncFreePlan {
     int nlev = 0;
     // staged variant: rows of L / U packed into kStagedSlots slots
     int staged = 0;
+    int threads = kLevelThreads;   // the largest level's rows rounded up to a warp (at most kLevelThreads)
     int *pcol[2] = {nullptr, nullptr}, *pcnt[2] = {nullptr, nullptr};
     void *pval[2] = {nullptr, nullptr};
 };
@@ -518,6 +522,9 @@ int syncfree_setup(b200la_ctx *ctx, b200la_precond *P)
     if (cta) {
         SyncFreePlan *plan = new SyncFreePlan();
         plan->nlev = P->nblocks;
+        int widest = 1;
+        for (int l = 0; l < P->nblocks; ++l) widest = std::max(widest, P->block_off[l + 1] - P->block_off[l]);
+        plan->threads = std::min(kLevelThreads, (widest + 31) / 32 * 32);
         cudaError_t e;
         if ((e = cudaMalloc(&plan->lev_off, sizeof(int) * (P->nblocks + 1))) ||
             (e = cudaMemcpy(plan->lev_off, P->block_off.data(), sizeof(int) * (P->nblocks + 1),
@@ -626,12 +633,13 @@ int syncfree_apply(b200la_ctx *ctx, const b200la_precond *P, const void *r, void
             a.pval = plan->pval[dir];
             a.pcnt = plan->pcnt[dir];
             a.backward = dir;
+            const int nt = plan->threads;
             if (P->dtype == B200LA_F64)
                 level_sweep_staged_kernel<double, kStagedSlots>
-                    <<<1, kLevelThreads, staged_smem<double, kStagedSlots>(plan->nlev), ctx->stream>>>(a);
+                    <<<1, nt, staged_smem<double, kStagedSlots>(plan->nlev, nt), ctx->stream>>>(a);
             else
                 level_sweep_staged_kernel<float, kStagedSlots>
-                    <<<1, kLevelThreads, staged_smem<float, kStagedSlots>(plan->nlev), ctx->stream>>>(a);
+                    <<<1, nt, staged_smem<float, kStagedSlots>(plan->nlev, nt), ctx->stream>>>(a);
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) return ctx_fail(ctx, B200LA_ERR_CUDA, "staged level sweep", e);
             ctx->launches += 1;
