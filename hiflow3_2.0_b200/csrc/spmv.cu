@@ -154,12 +154,24 @@ __global__ void __launch_bounds__(kBlock) spmv_direct_kernel(CsrView A, Seg seg,
     const int lane_g = threadIdx.x & (G - 1);
     const uint64_t pol_s = l2_policy(A.l2hint & 1 ? 1 : 0), pol_x = l2_policy(A.l2hint & 2 ? 2 : 0);
     double acc = 0.0;
-    for (int base = seg.r0 + blockIdx.x * rpb; base < seg.r1; base += gridDim.x * rpb) {
+    const int bstep = gridDim.x * rpb;
+    // the row pointers of the group's next row are loaded one row ahead, so
+    // their round trip overlaps this row's value, index and x loads
+    int nj0 = 0, nj1 = 0;
+    if (seg.r0 + blockIdx.x * rpb + grp < seg.r1) {
+        nj0 = __ldg(row + seg.r0 + blockIdx.x * rpb + grp);
+        nj1 = __ldg(row + seg.r0 + blockIdx.x * rpb + grp + 1);
+    }
+    for (int base = seg.r0 + blockIdx.x * rpb; base < seg.r1; base += bstep) {
         const int r = base + grp;
         const bool active = r < seg.r1;
+        const int j0 = nj0, j1 = nj1;
+        if (r + bstep < seg.r1) {
+            nj0 = __ldg(row + r + bstep);
+            nj1 = __ldg(row + r + bstep + 1);
+        }
         T s = T(0);
         if (active) {
-            const int j0 = __ldg(row + r), j1 = __ldg(row + r + 1);
             // 16-byte loads: E values and E column indices per lane per step,
             // the group's windows of E * G elements aligned to their size,
             // elements outside the row masked (the arrays are
