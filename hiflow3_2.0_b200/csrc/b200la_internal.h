@@ -71,7 +71,7 @@ struct b200la_csr {
     int *line_start = nullptr, *line_span = nullptr, *entry_line = nullptr, *entry_lo = nullptr;
     int nlines = 0, span_sum = 0;
     int stage_x = 0;                  // x staged per row tile (B200LA_STAGE_X=1 at creation)
-    int l2hint = 0;                   // L2 priorities on SpMV loads (B200LA_L2HINT bits: 1 stream first, 2 x last)
+    int l2hint = 0;                   // L2 priorities on SpMV loads (bits as in CsrView::l2hint; set at creation)
     // sliced (SELL-32) copy of the values for the dictionary SpMV
     int *sell_off = nullptr;
     void *sell_val = nullptr;

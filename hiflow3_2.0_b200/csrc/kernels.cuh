@@ -136,7 +136,8 @@ struct CsrView {
     const int *line_start, *line_span, *entry_line, *entry_lo;
     int nlines, span_sum;
     int stage_x;     // stage x through shared memory (B200LA_STAGE_X=1)
-    int l2hint;      // bit 0: evict-first matrix stream, bit 1: evict-last gathers (B200LA_L2HINT)
+    int l2hint;      // L2 priorities (B200LA_L2HINT): bit 0 CSR streams evict-first, bit 1 CSR gathers
+                     // evict-last, bit 2 stencil / lattice values evict-first, bit 3 half layout's own rows
     // sliced layout of the dictionary operator (null when absent): chunk c of
     // 32 rows holds its values k-major at sell_val[sell_off[c] + 32 k + lane]
     const int *sell_off;
@@ -190,7 +191,8 @@ struct LatticeDesc {
     int ncol, mx, my, mz;    // colours (4 in 2-D, 8 in 3-D) and node extents (mz = 1 in 2-D)
     int chunks;              // chunks of all colours
     int part;                // 0 strictly lower, 1 strictly upper, 2 whole operator
-    int pad[2];
+    int l2hint;              // the matrix's L2 hint (bit 2: the value stream evict-first)
+    int pad;
     LatticeColour col[kLatMaxColours];
 };
 

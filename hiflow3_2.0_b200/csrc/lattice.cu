@@ -107,7 +107,7 @@ __host__ __device__ __forceinline__ void static_for(F &&f)
 template <typename T, int EPI, int DIM, int PART, int C>
 __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__restrict__ val,
                                               const T *__restrict__ x, int g, int lane, const SpmvOp &op,
-                                              uint64_t pol, double &acc)
+                                              uint64_t pol, uint64_t pol_v, double &acc)
 {
     constexpr SlotTab S = Slots<DIM, C, PART>::tab;
     constexpr int px = C & 1, py = (C >> 1) & 1, pz = (C >> 2) & 1;
@@ -145,7 +145,7 @@ __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__r
     if constexpr (PREALL) {
         static_for<0, S.n>([&](auto kk) {
             constexpr int k = decltype(kk)::value;
-            aall[k] = ld_stream(v + 32 * k, pol);
+            aall[k] = ld_stream(v + 32 * k, pol_v);
         });
         grid_dependency_wait();
     }
@@ -156,7 +156,7 @@ __device__ __forceinline__ void lattice_chunk(const LatticeDesc &d, const T *__r
         static_for<0, cnt>([&](auto jj) {
             constexpr int j = decltype(jj)::value;
             if constexpr (PREALL) a[j] = aall[k0 + j];
-            else a[j] = ld_stream(v + 32 * (k0 + j), pol);
+            else a[j] = ld_stream(v + 32 * (k0 + j), pol_v);
         });
         // x (what earlier colours wrote) only after the previous launch completed
         if constexpr (!PREALL && decltype(gg)::value == 0) grid_dependency_wait();
@@ -196,7 +196,7 @@ __global__ void __launch_bounds__(kBlock) lattice_kernel(const __grid_constant__
     if (gate_closed(op.gate)) return;
     grid_dependents_launch();
     const T *__restrict__ x = static_cast<const T *>(op.x);
-    const uint64_t pol = l2_policy(0);
+    const uint64_t pol = l2_policy(0), pol_v = l2_policy(d.l2hint & 4 ? 1 : 0);
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     const int nw = gridDim.x * (kBlock / 32);
@@ -205,13 +205,13 @@ __global__ void __launch_bounds__(kBlock) lattice_kernel(const __grid_constant__
     double acc = 0.0;
     for (int g = g0 + gw; g < g1; g += nw) {
         if constexpr (CF >= 0) {
-            lattice_chunk<T, EPI, DIM, PART, CF>(d, val, x, g, lane, op, pol, acc);
+            lattice_chunk<T, EPI, DIM, PART, CF>(d, val, x, g, lane, op, pol, pol_v, acc);
         } else {
             int c = c0;
             while (c + 1 < c1 && g >= d.col[c + 1].chunk0) ++c;
             static_for<0, (DIM == 3 ? 8 : 4)>([&](auto cc) {
                 constexpr int C = decltype(cc)::value;
-                if (c == C) lattice_chunk<T, EPI, DIM, PART, C>(d, val, x, g, lane, op, pol, acc);
+                if (c == C) lattice_chunk<T, EPI, DIM, PART, C>(d, val, x, g, lane, op, pol, pol_v, acc);
             });
         }
     }
@@ -481,6 +481,7 @@ int lattice_attach(b200la_ctx *ctx, b200la_csr *A, const b200::host::Csr &Mh, in
     lattice_free(A);
     A->lt_val = dv;
     A->lt = new b200::LatticeDesc(d);
+    A->lt->l2hint = A->l2hint;
     A->bytes += es * v.size();
     return B200LA_OK;
 }

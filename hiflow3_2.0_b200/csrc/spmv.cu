@@ -532,7 +532,9 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
     using V = typename StencilVec<T, W>::type;
     const V *__restrict__ sv = static_cast<const V *>(A.st_val);
     const T *__restrict__ x = static_cast<const T *>(op.x);
-    const uint64_t pol = l2_policy(0);
+    // values: the stream (evict-first in L2 by the matrix's hint, so that x and the
+    // solver's vectors stay resident); gathers: normal
+    const uint64_t pol = l2_policy(0), pol_v = l2_policy(A.l2hint & 4 ? 1 : 0);
     auto gx = [&](int j) -> T { return ld_keep(x + j, pol); };
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
@@ -552,7 +554,7 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
             // FP32: the whole row's values first (G vector loads), then the bands
             T a[G * W];
 #pragma unroll
-            for (int g = 0; g < G; ++g) StencilVec<T, W>::load(v + 32 * g, pol, a + W * g);
+            for (int g = 0; g < G; ++g) StencilVec<T, W>::load(v + 32 * g, pol_v, a + W * g);
 #pragma unroll
             for (int b = 0; b < NB; ++b) {
                 const int d = cen[b];
@@ -574,7 +576,7 @@ __global__ void __launch_bounds__(kBlock) spmv_stencil_kernel(CsrView A, SpmvOp 
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb)
 #pragma unroll
-                    for (int m = 0; m < 3; ++m) StencilVec<T, W>::load(v + 32 * (3 * (b0 + bb) + m), pol, a + 3 * bb + m);
+                    for (int m = 0; m < 3; ++m) StencilVec<T, W>::load(v + 32 * (3 * (b0 + bb) + m), pol_v, a + 3 * bb + m);
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb) {
                     const int d = cen[b0 + bb];
@@ -702,17 +704,17 @@ struct HalfRow<double, NB> {
     }
     // the three values of band b alone (the same loads as values())
     static __device__ __forceinline__ void band(const double *__restrict__ hv, int d, int c, int lane, int b,
-                                                uint64_t pol, double (&a)[3])
+                                                uint64_t pol, uint64_t pol_own, double (&a)[3])
     {
         const int r = (c << 5) + lane;
         const double *own = hv + (size_t)c * H * 32 + lane;
         if (b > U) {
 #pragma unroll
-            for (int m = 0; m < 3; ++m) a[m] = ld_stream(own + 32 * (2 + 3 * (b - U - 1) + m), pol);
+            for (int m = 0; m < 3; ++m) a[m] = ld_stream(own + 32 * (2 + 3 * (b - U - 1) + m), pol_own);
         } else if (b == U) {
             a[0] = at(hv, r - 1, 1, pol);
-            a[1] = ld_stream(own, pol);
-            a[2] = ld_stream(own + 32, pol);
+            a[1] = ld_stream(own, pol_own);
+            a[2] = ld_stream(own + 32, pol_own);
         } else {
             const int q = r + d, p = 2 + 3 * (U - 1 - b);
             a[0] = at(hv, q - 1, p + 2, pol);
@@ -733,7 +735,7 @@ __global__ void __launch_bounds__(kBlock, MINB) spmv_half_kernel(CsrView A, Spmv
     constexpr int U = (NB - 1) / 2;
     const T *__restrict__ x = static_cast<const T *>(op.x);
     const unsigned *__restrict__ mask = A.sh_mask;
-    const uint64_t pol = l2_policy(0);
+    const uint64_t pol = l2_policy(0), pol_own = l2_policy(A.l2hint & 8 ? 1 : 0);
     auto gx = [&](int j) -> T { return ld_keep(x + j, pol); };
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
@@ -758,7 +760,7 @@ __global__ void __launch_bounds__(kBlock, MINB) spmv_half_kernel(CsrView A, Spmv
 #pragma unroll
                 for (int bb = 0; bb < 3; ++bb) {
                     const int b = b0 + bb, d = cen[b];
-                    HalfRow<double, NB>::band(static_cast<const double *>(A.sh_val), d, c, lane, b, pol, a[bb]);
+                    HalfRow<double, NB>::band(static_cast<const double *>(A.sh_val), d, c, lane, b, pol, pol_own, a[bb]);
                     if (ident) {
                         // identity row: its upper slots serve the neighbours; off-diagonals are zero
 #pragma unroll
