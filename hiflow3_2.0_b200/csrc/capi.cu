@@ -617,12 +617,15 @@ int csr_upload(b200la_ctx *ctx, int n_rows, int n_cols, int nnz, const int *row,
     // L2 priorities of the SpMV loads (B200LA_L2HINT overrides): bit 0 CSR-family
     // value / index streams evict-first, bit 1 their x gathers evict-last, bit 2
     // the stencil and lattice value streams evict-first, bit 3 the half
-    // layout's own rows evict-first.  Default bit 2 alone: a structured
-    // layout's stream then leaves x and the solver's vectors resident in L2
-    // (128^3: FP32 stencil SpMV 45.2 -> 41.2 us, mixed solve 34.8 -> 29.7 ms,
-    // MC-SGS apply 138 -> 124 us); the CSR kernels lose with bits 0 and 1
-    // (FP64 CSR CG 71 -> 103 and 88 ms), the half layout gains nothing from bit 3.
-    A->l2hint = 4;
+    // layout's own rows evict-first, bit 4 the half layout's chunk lines
+    // prefetched into L2 before its band groups load them.  Default bits 2
+    // and 4: a structured layout's stream then leaves x and the solver's
+    // vectors resident in L2 (128^3: FP32 stencil SpMV 45.2 -> 41.2 us, mixed
+    // solve 34.8 -> 29.7 ms, MC-SGS apply 138 -> 124 us), and the half
+    // layout's three band groups wait on L2, not DRAM, after the first (FP64
+    // SpMV 59.6 -> 58.9 us).  The CSR kernels lose with bits 0 and 1 (FP64
+    // CSR CG 71 -> 103 and 88 ms); the half layout gains nothing from bit 3.
+    A->l2hint = 4 | 16;
     if (const char *h = std::getenv("B200LA_L2HINT")) A->l2hint = std::atoi(h);
     const int cap = spmv_tile_cap(A->cfg);
     A->h_row.assign(row, row + n_rows + 1);

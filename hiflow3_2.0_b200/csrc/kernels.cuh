@@ -138,6 +138,7 @@ struct CsrView {
     int stage_x;     // stage x through shared memory (B200LA_STAGE_X=1)
     int l2hint;      // L2 priorities (B200LA_L2HINT): bit 0 CSR streams evict-first, bit 1 CSR gathers
                      // evict-last, bit 2 stencil / lattice values evict-first, bit 3 half layout's own rows
+                     // evict-first, bit 4 half layout's chunk lines prefetched into L2
     // sliced layout of the dictionary operator (null when absent): chunk c of
     // 32 rows holds its values k-major at sell_val[sell_off[c] + 32 k + lane]
     const int *sell_off;

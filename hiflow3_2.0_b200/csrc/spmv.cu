@@ -752,6 +752,14 @@ __global__ void __launch_bounds__(kBlock, MINB) spmv_half_kernel(CsrView A, Spmv
         if constexpr (sizeof(T) == 8) {
             // FP64: groups of three bands, their value loads and gathers
             // issued together (register pressure of one group, not of the row)
+            if (A.l2hint & 16) {   // the chunk's own value lines into L2 before the first group's loads
+                constexpr int kLines = HalfRow<double, NB>::H * 32 * 8 / 128;
+                if (lane < kLines) {
+                    const char *q = reinterpret_cast<const char *>(static_cast<const double *>(A.sh_val) +
+                                                                   (size_t)c * HalfRow<double, NB>::H * 32) + 128 * lane;
+                    asm volatile("prefetch.global.L2 [%0];" ::"l"(q));
+                }
+            }
             const bool ident = (__ldg(mask + c) >> lane) & 1u;
             T s = T(0);
 #pragma unroll
