@@ -101,6 +101,17 @@ struct b200la_server {
     unsigned *d_ticket = nullptr;
     int *d_done = nullptr, *h_done = nullptr;
     int *d_tiles = nullptr, *h_tiles = nullptr;
+    // pinned staging of the admission thread's uploads: a copy from pageable
+    // memory is staged by the driver, which may first wait for the copy
+    // stream -- behind the admission kernels that share the GPU with the rounds
+    struct AdmitStage {
+        SysState hs;
+        SysDesc d;
+        unsigned asym;
+    };
+    AdmitStage *h_admit = nullptr;
+    double *h_kc = nullptr;           // a request's cell field
+    size_t h_kc_len = 0;
     cudaGraphExec_t graph = nullptr;
     // kernel shape
     int nw = 8, ctas_per_sm = 4, cpw = 4, iters = 16;
@@ -318,7 +329,17 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
         double *kc = nullptr;
         if (r.q1_kcell) {
             kc = reinterpret_cast<double *>(t);
-            SV(cudaMemcpyAsync(kc, r.q1_kcell, 8 * q1_cells(r.q1_dim, r.q1_N), cudaMemcpyHostToDevice, st));
+            const size_t cells = q1_cells(r.q1_dim, r.q1_N);
+            if (cells > S->h_kc_len) {
+                // the staging buffer grows (the copy stream holds no copy from it: admissions end synchronised)
+                if (S->h_kc) cudaFreeHost(S->h_kc);
+                S->h_kc = nullptr;
+                S->h_kc_len = 0;
+                SV(cudaMallocHost(&S->h_kc, 8 * cells));
+                S->h_kc_len = cells;
+            }
+            std::memcpy(S->h_kc, r.q1_kcell, 8 * cells);
+            SV(cudaMemcpyAsync(kc, S->h_kc, 8 * cells, cudaMemcpyHostToDevice, st));
         }
         SV(b200::launch_q1_assemble(r.q1_dim, r.q1_N, r.q1_kind, kc, r.q1_nu, r.q1_beta, trow, tcol, tval, st));
     }
@@ -337,10 +358,9 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
     SV(b200::srv::launch_build_slot(d, trow, tcol, tval, st));
     if (stencil && d.half) {
         // the half layout needs a_ij == a_ji between rows that are not identity rows
-        unsigned asym = 0;
-        SV(cudaMemcpyAsync(&asym, d.smask + q->nchunks, sizeof asym, cudaMemcpyDeviceToHost, st));
+        SV(cudaMemcpyAsync(&S->h_admit->asym, d.smask + q->nchunks, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
         SV(cudaStreamSynchronize(st));
-        if (asym) {
+        if (S->h_admit->asym) {
             d.half = 0;
             SV(cudaMemsetAsync(const_cast<double *>(d.val64), 0, 8 * (size_t)q->slen, st));
             if (mixed) SV(cudaMemsetAsync(const_cast<float *>(d.val32), 0, 4 * (size_t)q->slen32, st));
@@ -350,7 +370,8 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
     if (r.b) SV(cudaMemcpyAsync(const_cast<double *>(d.b), r.b, 8 * (size_t)n, cudaMemcpyHostToDevice, st));
     else SV(b200::launch_q1_rhs(r.rhs_seed, r.q1_dim, r.q1_N, const_cast<double *>(d.b), st));
     SV(cudaMemsetAsync(vec0, 0, (size_t)(vec1 - vec0), st));
-    SysState hs{};
+    SysState &hs = S->h_admit->hs;   // pinned: the copy below is asynchronous
+    hs = SysState{};
     hs.abstol = r.ctl.abstol;
     hs.reltol = r.ctl.reltol;
     hs.divtol = r.ctl.divtol;
@@ -365,9 +386,10 @@ int admit_slot(b200la_server *S, Req *q, Slot *sl)
     SV(cudaMemsetAsync(d.ticket, 0, sizeof(unsigned) * b200::srv::kTicketWords, st));
     SV(cudaMemsetAsync(d.gcnt, 0, sizeof(unsigned) * (size_t)d.ngroups, st));
     SV(cudaMemsetAsync(d.done, 0, sizeof(int), st));
-    SV(cudaMemcpyAsync(S->d_sys + sl->idx, &d, sizeof d, cudaMemcpyHostToDevice, st));
+    S->h_admit->d = d;
+    SV(cudaMemcpyAsync(S->d_sys + sl->idx, &S->h_admit->d, sizeof d, cudaMemcpyHostToDevice, st));
     SV(cudaFreeAsync(tmp, st));
-    SV(cudaStreamSynchronize(st));
+    SV(cudaStreamSynchronize(st));   // the staging area is reused by the next admission
     sl->desc = d;
     return 0;
 }
@@ -851,6 +873,8 @@ void destroy_server(b200la_server *S)
     cudaFree(S->d_tiles);
     cudaFreeHost(S->h_done);
     cudaFreeHost(S->h_tiles);
+    if (S->h_admit) cudaFreeHost(S->h_admit);
+    if (S->h_kc) cudaFreeHost(S->h_kc);
     if (S->ev_a) cudaEventDestroy(S->ev_a);
     if (S->ev_b) cudaEventDestroy(S->ev_b);
     if (S->ev_fork) cudaEventDestroy(S->ev_fork);
@@ -920,7 +944,8 @@ extern "C" int b200la_serve_start(const b200la_serve_config *cfg, b200la_server 
          cudaMalloc(&S->d_done, sizeof(int) * ms) == cudaSuccess &&
          cudaMalloc(&S->d_tiles, sizeof(int) * kTabWords * kLanes) == cudaSuccess &&
          cudaMallocHost(&S->h_done, sizeof(int) * ms) == cudaSuccess &&
-         cudaMallocHost(&S->h_tiles, sizeof(int) * kTabWords * kLanes) == cudaSuccess;
+         cudaMallocHost(&S->h_tiles, sizeof(int) * kTabWords * kLanes) == cudaSuccess &&
+         cudaMallocHost(&S->h_admit, sizeof(b200la_server::AdmitStage)) == cudaSuccess;
     ok = ok && cudaMemset(S->d_done, 0, sizeof(int) * ms) == cudaSuccess &&
          cudaMemset(S->d_tiles, 0, sizeof(int) * kTabWords * kLanes) == cudaSuccess &&
          cudaMemset(S->d_sys, 0, sizeof(SysDesc) * ms) == cudaSuccess;
