@@ -423,6 +423,8 @@ __global__ void pack_rows_kernel(int n, int kp, const int *__restrict__ row, con
     }
 }
 
+constexpr size_t kStagedSmemCap = 226 * 1024;   // opt-in shared memory per CTA on sm_100 (227 KB), less the static part
+
 template <typename T, int KP>
 size_t staged_smem(int nlev, int NT = kLevelThreads)
 {
@@ -436,12 +438,14 @@ namespace b200 {
 cudaError_t sweeps_configure()
 {
     cudaError_t e;
+    // the largest stage set a plan may use (its CTA size and level count are
+    // checked against kStagedSmemCap at set-up)
     if ((e = cudaFuncSetAttribute(level_sweep_staged_kernel<double, kStagedSlots>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)staged_smem<double, kStagedSlots>(kStagedMaxLevels))) ||
+                                  (int)std::min(staged_smem<double, kStagedSlots>(kStagedMaxLevels), kStagedSmemCap))) ||
         (e = cudaFuncSetAttribute(level_sweep_staged_kernel<float, kStagedSlots>,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)staged_smem<float, kStagedSlots>(kStagedMaxLevels))))
+                                  (int)std::min(staged_smem<float, kStagedSlots>(kStagedMaxLevels), kStagedSmemCap))))
         return e;
     e = cudaFuncSetAttribute(level_sweep_cta_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)(kLevelRing * sizeof(double) + sizeof(int) * (kLevelMaxLevels + 1)));
@@ -512,8 +516,12 @@ int syncfree_setup(b200la_ctx *ctx, b200la_precond *P)
         return m;
     };
     const bool few = P->nblocks > 64 && P->n / std::max(P->nblocks, 1) <= 4 * kLevelThreads;
+    int widest = 1;
+    for (int l = 0; l < P->nblocks; ++l) widest = std::max(widest, P->block_off[l + 1] - P->block_off[l]);
+    const int nt = std::min(kLevelThreads, (widest + 31) / 32 * 32);
     const bool can_stage = P->nblocks <= kStagedMaxLevels && maxlen(P->L) <= kStagedSlots &&
-                           maxlen(P->U) <= kStagedSlots;
+                           maxlen(P->U) <= kStagedSlots &&
+                           staged_smem<double, kStagedSlots>(P->nblocks, nt) <= kStagedSmemCap;
     bool cta = few && P->nblocks <= kLevelMaxLevels, staged = few && can_stage;
     if (const char *sw = std::getenv("B200LA_SWEEP")) {
         staged = std::strcmp(sw, "staged") == 0 && can_stage;
@@ -522,9 +530,7 @@ int syncfree_setup(b200la_ctx *ctx, b200la_precond *P)
     if (cta) {
         SyncFreePlan *plan = new SyncFreePlan();
         plan->nlev = P->nblocks;
-        int widest = 1;
-        for (int l = 0; l < P->nblocks; ++l) widest = std::max(widest, P->block_off[l + 1] - P->block_off[l]);
-        plan->threads = std::min(kLevelThreads, (widest + 31) / 32 * 32);
+        plan->threads = nt;
         cudaError_t e;
         if ((e = cudaMalloc(&plan->lev_off, sizeof(int) * (P->nblocks + 1))) ||
             (e = cudaMemcpy(plan->lev_off, P->block_off.data(), sizeof(int) * (P->nblocks + 1),
