@@ -78,7 +78,11 @@ typedef struct b200la_precond b200la_precond;
  * select `device`, create the platform's stream and reduction scratch. */
 int b200la_create(int device, b200la_ctx **out);
 int b200la_destroy(b200la_ctx *ctx);
-/* Run the context's work on a caller-owned cudaStream_t (NULL: the context's own). */
+/* Run the context's work on a caller-owned cudaStream_t (NULL: the context's own).
+ * Calls without a host result return once their kernels are enqueued on this
+ * stream: a device buffer passed to one may be freed or reused by the caller
+ * only in this stream's order (after b200la_sync, an event recorded on it,
+ * or a stream-ordered free on the same stream). */
 int b200la_set_stream(b200la_ctx *ctx, void *cuda_stream);
 void *b200la_get_stream(b200la_ctx *ctx);
 /* lVector::Sync (src/linear_algebra/lmp/lvector.h:245) */
