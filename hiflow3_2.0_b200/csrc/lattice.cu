@@ -196,7 +196,9 @@ __global__ void __launch_bounds__(kBlock) lattice_kernel(const __grid_constant__
     if (gate_closed(op.gate)) return;
     grid_dependents_launch();
     const T *__restrict__ x = static_cast<const T *>(op.x);
-    const uint64_t pol = l2_policy(0), pol_v = l2_policy(d.l2hint & 4 ? 1 : 0);
+    // gathers evict-last, the value stream evict-first (the matrix's hint):
+    // the gathered vector and the solver's vectors stay in L2 (C2 32.9 -> 32.45 ms)
+    const uint64_t pol = l2_policy(2), pol_v = l2_policy(d.l2hint & 4 ? 1 : 0);
     const int lane = threadIdx.x & 31;
     const int gw = blockIdx.x * (kBlock / 32) + (threadIdx.x >> 5);
     const int nw = gridDim.x * (kBlock / 32);
